@@ -1,0 +1,390 @@
+#!/usr/bin/env python3
+"""Throughput of the MLS-MPM substep engine: particle-substeps per second.
+
+Workload (default `dam_break_2M`): water box x in [4,60), y in [4,41),
+z in [4,124) of a 128^3 grid at RESOLUTION 0.5 (1,989,120 particles, seeded
+sub-cell jitter), a torus obstacle (R 25, r 8, 48x24 segments, 2,304
+triangles) at (80,30,64), PADDING 3, GRAVITY -0.3, DT 0.1, GAMMA 7,
+COMPRESSION 10, SUBSTEPS 4.  One bench step is one frame of the reference's
+Simulation::run loop: SUBSTEPS calls of Engine::step() (keys, stable sort,
+clear, P2G, grid update, G2P) plus the position export.  Inputs are synthetic.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Engine arm (default): `value` is device time (CUDA events on the engine's
+stream) of K frames with the state resident in HBM; `e2e` is the whole job
+through the C ABI with host buffers: upload of the scene from pinned memory
+(mpm_init_particles), then K x (mpm_step + positions read back to pinned
+memory), host wall time.  A second, instrumented pass records CUDA events
+between the stages of every substep for the per-kernel roofline.  Rank 0 at
+N=1 also times the FP32 OpenMP CPU restatement on a bounded sample.
+Under torchrun each rank simulates an independent replica of the scene on its
+own GPU (no collective on the data path; weak scaling), timing is the max over
+ranks.
+
+Reference arm: the reference's own Engine (engine.cu/kernels.cu compiled from
+its sources into oracle/_ref) on the same scene, K frames, device time.  The
+reference implementation of this path is CUDA, so this arm runs on the GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "water-sim-cuda_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-substeps/s"
+UNIT = "particle-substeps/s"
+FALLBACK_HBM_GBS = 6650.0
+SEEDS = {"dam_break_2M": 1235, "dam_break_5M": 1235, "sphere_drop": 1234}
+# Algorithmic bytes per unit (FP32 reference state): per particle and per grid
+# node of each stage, from the hot-path scope table of this project.
+ALGO_BYTES = {"sort": (16, 0), "p2g": (108, 16), "grid": (0, 48), "g2p": (148, 12)}
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20, help="timed frames (each = SUBSTEPS substeps)")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--workload", choices=sorted(SEEDS), default="dam_break_2M")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget (0: skip)")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args(argv)
+
+
+def make_scene(workload: str, rank: int = 0):
+    from mpm_b200 import scenes
+    seed = SEEDS[workload] + 1000 * rank
+    if workload == "sphere_drop":
+        return scenes.sphere_drop(seed)
+    return scenes.dam_break(seed, literal_extent=(workload == "dam_break_5M"))
+
+
+def workload_config(workload, cfg, n, t):
+    return {"workload": workload, "grid": f"{cfg.size_x}x{cfg.size_y}x{cfg.size_z}", "particles": n,
+            "triangles": t, "substeps_per_step": cfg.substeps,
+            "physics": {"padding": cfg.padding, "gravity": cfg.gravity, "dt": cfg.dt, "gamma": cfg.gamma,
+                        "compression": cfg.compression, "resolution": cfg.resolution},
+            "l2": "inputs larger than L2: particle state 96 B x N per buffer (192 MB at 2M) vs 126 MB L2"}
+
+
+# ---------------------------------------------------------------- clocks ----
+_REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+            0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+            0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons via NVML during a timed region."""
+
+    def __init__(self, cuda_index: int):
+        self.samples, self.reasons, self.max_mhz, self.err = [], 0, None, None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            self.nv = pynvml
+            pynvml.nvmlInit()
+            self._h = self._handle(cuda_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # noqa: BLE001 - clocks are reported, not required
+            self.err = f"nvml unavailable: {e}"
+
+    def _handle(self, cuda_index):
+        pynvml = self.nv
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(cuda_index)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:  # noqa: BLE001
+            return pynvml.nvmlDeviceGetHandleByIndex(cuda_index)
+
+    def _reason_bits(self):
+        f = getattr(self.nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            getattr(self.nv, "nvmlDeviceGetCurrentClocksThrottleReasons")
+        return int(f(self._h))
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self._h, self.nv.NVML_CLOCK_SM))
+                self.reasons |= self._reason_bits()
+            except Exception as e:  # noqa: BLE001
+                self.err = str(e)
+            self._stop.wait(0.05)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._h is not None:
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "note": self.err}
+        s = sorted(self.samples)
+        names = [v for k, v in _REASONS.items() if self.reasons & k and k != 0x1]
+        return {"sm_mhz": s[len(s) // 2], "sm_max_mhz": self.max_mhz, "reasons": names, "samples": len(s)}
+
+
+# ------------------------------------------------------------ distributed ----
+class Dist:
+    """Barrier and max-over-ranks for the timing; no data-path collective.
+    backend "nccl" on GPUs (one rank per GPU), "gloo" for CPU tests."""
+
+    def __init__(self, world: int, local: int, backend: str = "nccl"):
+        self.world, self.local, self.backend, self.pg = world, local, backend, None
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            if self.backend == "nccl":
+                self.pg.barrier(device_ids=[self.local])
+            else:
+                self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def load_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)[workload][kernel]["bytes_per_launch"]
+    except Exception:  # noqa: BLE001
+        return None
+
+
+# -------------------------------------------------------------- CPU leg ----
+CPU_SNIPPET = r"""
+import json, os, sys, time
+sys.path.insert(0, os.path.join(sys.argv[1], "water-sim-cuda_b200")); sys.path.insert(0, sys.argv[1])
+import numpy as np
+from bench import make_scene
+from oracle.oracle import Oracle
+cfg, st, tris = make_scene(sys.argv[2], 0)
+o = Oracle(32)
+st = o.init_particles(cfg, st)
+sdf = np.load(sys.argv[4]).astype(np.float32)  # the SDF the engine built
+budget = float(sys.argv[3]); done = 0; t0 = time.perf_counter()
+while True:
+    st = o.substep(cfg, st, sdf)[0]
+    done += 1
+    el = time.perf_counter() - t0
+    if el >= budget or done >= 16:
+        break
+print(json.dumps({"substeps": done, "seconds": el, "n": int(st.shape[1]), "threads": o.threads()}))
+"""
+
+
+def cpu_baseline(workload: str, seconds: float, sdf):
+    """FP32 OpenMP restatement of Engine::step timed on the host cores, in a
+    fresh process (no CUDA in it), on the engine's SDF."""
+    import tempfile
+
+    import numpy as np
+    with tempfile.NamedTemporaryFile(suffix=".npy", delete=False) as f:
+        np.save(f, sdf)
+        sdf_path = f.name
+    try:
+        r = subprocess.run([sys.executable, "-c", CPU_SNIPPET, ROOT, workload, str(seconds), sdf_path],
+                           capture_output=True, text=True, timeout=900)
+    finally:
+        os.unlink(sdf_path)
+    if r.returncode != 0:
+        return {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": "failed: " + r.stderr[-300:]}
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"value": d["n"] * d["substeps"] / d["seconds"], "unit": UNIT, "cores": d["threads"], "kind": "port",
+            "sample": f"{d['substeps']} substeps of the full {d['n']}-particle scene (SDF build excluded), "
+                      f"FP32 OpenMP restatement of Engine::step, {d['seconds']:.1f} s"}
+
+
+# ----------------------------------------------------------- engine arm ----
+def run_engine(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = Dist(world, local)
+    import mpm_b200
+
+    cfg, st, tris = make_scene(args.workload, rank)
+    n, sub = st.shape[1], cfg.substeps
+    eng = mpm_b200.Engine(cfg, device=local)
+    eng.init(st)
+    eng.init_sdf(tris)
+    stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+
+    for _ in range(max(args.warmup, 3)):
+        eng.step_async(sub)
+    eng.synchronize()
+
+    # Timed region: K frames, device time on the engine's stream.
+    launches0 = eng.stats()["kernel_launches"]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            eng.step_async(sub)
+        e1.record(stream)
+        eng.synchronize()
+        torch.cuda.synchronize()
+        dist.barrier()
+    launches = eng.stats()["kernel_launches"] - launches0
+    ms = dist.max(e0.elapsed_time(e1))
+    value = world * n * sub * args.steps / (ms / 1e3)
+
+    # Instrumented repeat: CUDA events between the stages of every substep.
+    eng.set_stage_timing(args.steps * sub)
+    for _ in range(args.steps):
+        eng.step_async(sub)
+    stage_ms, cnt = eng.stage_times()
+    eng.set_stage_timing(0)
+    per_sub = {k: v / max(cnt, 1) for k, v in stage_ms.items()}
+    grid = eng.get_grid()
+    g_dense = cfg.grid_number
+    g_active = int(np.count_nonzero(grid[0] > 0))
+    peak, peak_kind = load_peaks()
+    dom = max(("p2g", "g2p", "grid", "sort"), key=lambda k: per_sub[k])
+    bpp, bpn = ALGO_BYTES[dom]
+    algo = bpp * n + bpn * g_active
+    achieved = algo / (per_sub[dom] / 1e3) / 1e9
+    roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": f"hbm_gbs of {peak_kind}",
+            "traffic": load_traffic(dom, args.workload),
+            "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(per_sub[dom], 5),
+            "units": f"{bpp} B x {n} particles + {bpn} B x {g_active} active nodes (dense grid {g_dense})"}
+
+    # End to end through the C ABI with host buffers (pinned).
+    e2e = None
+    if not args.no_e2e:
+        st_pin = torch.from_numpy(np.ascontiguousarray(st)).pin_memory().numpy()
+        pos_pin = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
+        eng2 = mpm_b200.Engine(cfg, device=local)
+        eng2.init_sdf(tris)
+        eng2.init(st_pin)  # warm the allocation path once
+        eng2.step(sub)
+        dist.barrier()
+        t0 = time.perf_counter()
+        eng2.init(st_pin)
+        for _ in range(args.steps):
+            eng2.step(sub)
+            eng2.get_positions(pos_pin)
+        t1 = time.perf_counter()
+        dist.barrier()
+        e2e_s = dist.max(t1 - t0)
+        e2e = {"value": world * n * sub * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(26 * 4 * n / args.steps), "d2h_bytes_per_step": 12 * n,
+               "timed": "mpm_init_particles(pinned host state) + K x (mpm_step(SUBSTEPS) + "
+                        "mpm_get_positions(pinned)); host wall clock, max over ranks"}
+        eng2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_seconds > 0:
+        cpu = cpu_baseline(args.workload, args.cpu_seconds, eng.get_sdf())
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": dict(workload_config(args.workload, cfg, n, len(tris)), parallelism=f"replicas{world}"),
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+            "clocks": clk.summary(), "stage_ms_per_substep": {k: round(v, 5) for k, v in per_sub.items()},
+            "impl": "engine"}
+    eng.close()
+    dist.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------- reference arm ----
+def run_reference(args, rank, world, local):
+    if rank != 0:
+        return
+    from oracle.oracle import REF_LIB, RefEngine
+    if not os.path.exists(REF_LIB):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_engine.so was not built "
+                          "(the reference sources were absent at build time)"}))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    cfg, st, tris = make_scene(args.workload, 0)
+    n, sub = st.shape[1], cfg.substeps
+    ref = RefEngine()
+    ref.create(cfg, st, tris, f"/tmp/ref_bench_config_{os.getpid()}.txt")
+    ref.step(max(args.warmup, 3) * sub)
+    with ClockSampler(local) as clk:
+        ms = ref.time_steps(args.steps * sub)
+    ref.destroy()
+    value = n * sub * args.steps / (ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": dict(workload_config(args.workload, cfg, n, len(tris)), parallelism="replicas1"),
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": f"{args.steps} frames x {sub} Engine::step() of the reference's own CUDA "
+                                       "engine compiled from its sources for sm_100a; the reference implements "
+                                       "this path only in CUDA, so it runs on the GPU driven by 1 host thread"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world, local)
+    else:
+        run_engine(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

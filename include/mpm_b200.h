@@ -1,0 +1,304 @@
+/*
+ * mpm_b200.h - C ABI of the B200 MLS-MPM substep engine.
+ *
+ * This is the drop-in boundary for the simulation step of water-sim-cuda.
+ * The reference exposes the step as the C++ class `Engine` (engine.h:14-43),
+ * configured through `GameConfigData` (game_configdata.h:15-32) and a
+ * process-global `__constant__ SimConfig d_config` (common.cuh:65-83,
+ * config.cu:3-8).  Each entry point below names the reference member it
+ * replaces.  Differences that a caller can observe are stated beside it.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  `*_host` buffers are host memory (pinned
+ *    or pageable); `*_device` / `d_*` buffers are device memory on the
+ *    engine's device.
+ *  - Every call returns an mpm_status; nothing here exits the process or
+ *    traps the GPU (the reference calls exit(1) on any CUDA or config error,
+ *    engine.cu:21-28, game_configdata.cpp:49,56-61).
+ *  - One engine = one device, one CUDA stream, no process-global state, so
+ *    several engines may live in one process (the reference allows one).
+ *  - An engine is not thread-safe; use one engine per host thread.
+ */
+#ifndef MPM_B200_H
+#define MPM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_ABI_VERSION 1
+
+/* Particle state planes: n floats each, plane-major (SoA), in the order of
+ * `enum ParticleAttr` (common.cuh:12-29).  A state buffer holds 26*n floats,
+ * the layout `VoxelPipeline::process` builds (VoxelPipeline.cpp:5-33). */
+enum {
+    MPM_POS_X = 0, MPM_POS_Y, MPM_POS_Z,
+    MPM_VEL_X, MPM_VEL_Y, MPM_VEL_Z,
+    MPM_C00, MPM_C01, MPM_C02, MPM_C10, MPM_C11, MPM_C12, MPM_C20, MPM_C21, MPM_C22,
+    MPM_F00, MPM_F01, MPM_F02, MPM_F10, MPM_F11, MPM_F12, MPM_F20, MPM_F21, MPM_F22,
+    MPM_VOL, MPM_MASS,
+    MPM_PARTICLE_PLANES /* = 26 */
+};
+
+/* Grid planes: G = size_x*size_y*size_z floats each, node index
+ * z*size_x*size_y + y*size_x + x (common.cuh:110-121, 131-134).  After a
+ * substep the momentum planes hold the updated node velocities, exactly as
+ * the reference's gridUpdate leaves them (kernels.cu:193). */
+enum {
+    MPM_GRID_MASS = 0, MPM_GRID_MOM_X, MPM_GRID_MOM_Y, MPM_GRID_MOM_Z,
+    MPM_GRID_PLANES /* = 4 */
+};
+
+typedef enum mpm_status {
+    MPM_OK = 0,
+    MPM_ERR_INVALID_ARGUMENT = 1,
+    MPM_ERR_BAD_CONFIG = 2,      /* missing key, unparsable value, bad WATER/OBJECT entry */
+    MPM_ERR_IO = 3,              /* config file cannot be opened */
+    MPM_ERR_CUDA = 4,            /* a CUDA runtime call failed; see mpm_last_error */
+    MPM_ERR_OUT_OF_MEMORY = 5,
+    MPM_ERR_NOT_INITIALIZED = 6, /* step/readback before mpm_init_particles */
+    MPM_ERR_NONFINITE_STATE = 7, /* checks on: a particle position/velocity became NaN/Inf */
+    MPM_ERR_OUT_OF_GRID = 8,     /* checks on: a particle left [0,SIZE) on some axis */
+    MPM_ERR_TIMEOUT = 9,         /* a bounded device-side wait gave up */
+    MPM_ERR_UNSUPPORTED = 10,
+    MPM_ERR_NO_DEVICE = 11       /* no CUDA device, or the device is not sm_100 */
+} mpm_status;
+
+/* Simulation parameters: the config.txt keys read by
+ * Simulation::initDeviceParams (Simulation.cpp:56-77) into SimConfig
+ * (common.cuh:65-79).  GRID_SIZE/GRID_NUMBER/GRID_BLOCKS are derived, as in
+ * the reference, and not stored.  sdf_resolution is accepted and ignored:
+ * no reference kernel reads SDF_RESOLUTION, the SDF lives on the simulation
+ * grid. */
+typedef struct mpm_config {
+    int32_t size_x, size_y, size_z; /* SIZE_X/Y/Z (grid nodes per axis) */
+    int32_t padding;                /* PADDING (wall thickness in nodes) */
+    float gravity;                  /* GRAVITY: subtracted from v.y each substep (kernels.cu:155) */
+    float dt;                       /* DT */
+    float gamma;                    /* GAMMA: Tait exponent (kernels.cu:28) */
+    float compression;              /* COMPRESSION: Tait stiffness (kernels.cu:28) */
+    float resolution;               /* RESOLUTION: particle volume = RESOLUTION^3 (kernels.cu:356) */
+    int32_t substeps;               /* SUBSTEPS: substeps per frame (Simulation.cpp:46) */
+    int32_t sdf_resolution;         /* SDF_RESOLUTION: accepted, unused */
+} mpm_config;
+
+#define MPM_PATH_MAX 512
+
+/* One `WATER=` or `OBJECT=` entry, `path;scale;x;y;z` (game_configdata.cpp:35-49,
+ * struct ConfigObject game_configdata.h:7-12). */
+typedef struct mpm_scene_entry {
+    char model_path[MPM_PATH_MAX];
+    float scale;
+    float x, y, z;
+} mpm_scene_entry;
+
+typedef struct mpm_engine mpm_engine;
+
+/* Health bits reported by mpm_get_stats (always recorded) and turned into
+ * step errors by mpm_set_checks. */
+enum {
+    MPM_HEALTH_NONFINITE = 1u << 0,   /* some particle position or velocity is NaN/Inf */
+    MPM_HEALTH_OUT_OF_GRID = 1u << 1  /* some particle position is outside [0,SIZE) */
+};
+
+typedef struct mpm_stats {
+    int64_t substeps;          /* substeps completed since mpm_init_particles */
+    int64_t kernel_launches;   /* kernels this engine launched since creation */
+    int64_t sort_passes;       /* radix passes run since creation */
+    uint32_t health;           /* MPM_HEALTH_* bits seen since init or the last reset */
+    uint32_t reserved;
+} mpm_stats;
+
+/* Stages of one substep, for mpm_substep_partial. */
+enum {
+    MPM_STAGE_SORT = 1,  /* Morton keys + stable sort (engine.cu:92-102) */
+    MPM_STAGE_P2G = 2,   /* + grid clear + particle-to-grid scatter (kernels.cu:6-142, 311-318) */
+    MPM_STAGE_GRID = 3,  /* + grid update (kernels.cu:144-196) */
+    MPM_STAGE_G2P = 4    /* + grid-to-particle gather: a full substep (kernels.cu:199-280) */
+};
+
+/* ------------------------------------------------------------------ */
+/* Library                                                              */
+/* ------------------------------------------------------------------ */
+
+int32_t mpm_abi_version(void);
+const char* mpm_status_string(mpm_status status);
+
+/* ------------------------------------------------------------------ */
+/* Configuration (no GPU needed)                                        */
+/* ------------------------------------------------------------------ */
+
+/* Replaces GameConfigData::setConfigDataFromFile (game_configdata.cpp:22-54)
+ * followed by the getInt/getFloat reads of Simulation::initDeviceParams
+ * (Simulation.cpp:56-77).  Same format: `KEY=value` lines, every space
+ * removed before parsing, blank lines skipped, lines without '=' ignored,
+ * later keys overwrite earlier ones, integer keys parsed like std::stoi
+ * (leading integer prefix, so "0.5" reads as 0), float keys like std::stof.
+ * Repeated WATER=/OBJECT= entries are appended (at most max_* are stored,
+ * n_* counts all).  Where the reference exits, this returns
+ * MPM_ERR_BAD_CONFIG with the reason in err (if err_len > 0):
+ * a required key missing or unparsable, or a WATER/OBJECT value with fewer
+ * than 5 ';'-separated fields.  Any of waters/objects/n_* may be NULL. */
+mpm_status mpm_config_parse_file(const char* path, mpm_config* cfg,
+                                 mpm_scene_entry* waters, int32_t max_waters, int32_t* n_waters,
+                                 mpm_scene_entry* objects, int32_t max_objects, int32_t* n_objects,
+                                 char* err, int32_t err_len);
+
+/* As mpm_config_parse_file, from the text of a config file. */
+mpm_status mpm_config_parse_string(const char* text, mpm_config* cfg,
+                                   mpm_scene_entry* waters, int32_t max_waters, int32_t* n_waters,
+                                   mpm_scene_entry* objects, int32_t max_objects, int32_t* n_objects,
+                                   char* err, int32_t err_len);
+
+/* ------------------------------------------------------------------ */
+/* Engine lifetime                                                      */
+/* ------------------------------------------------------------------ */
+
+/* Replaces `Engine engine;` plus uploadConfigToGPU (config.cu:5-8) and
+ * Engine::initGrid (engine.cu:86-90).  Allocates the grid and SDF on
+ * `device`; the SDF starts at +1e15 everywhere, the value the reference's
+ * makeSDF writes for an empty triangle list (kernels.cu:289,299), so a scene
+ * without OBJECT entries may skip mpm_init_sdf.  Rejects sizes <= 0,
+ * padding < 0, and non-finite floats with MPM_ERR_BAD_CONFIG. */
+mpm_status mpm_create(const mpm_config* cfg, int32_t device, mpm_engine** out);
+
+/* Replaces Engine::~Engine (engine.cu:36-43).  Frees every buffer, including
+ * the SDF and position buffers the reference leaks.  NULL is a no-op. */
+void mpm_destroy(mpm_engine* engine);
+
+/* Replaces Engine::init(int n, float* h_buffer) (engine.cu:45-52, 72-83).
+ * soa26_host holds 26*n floats (layout above).  Unlike the reference, the
+ * buffer is COPIED, not adopted (the reference delete[]s it in ~Engine).
+ * As the reference's initFMatrices does (kernels.cu:349-358), F00/F11/F22
+ * are set to 1, VOL to resolution^3 and MASS to 1; all other planes are
+ * taken from the buffer.  n may be 0 (the reference cannot launch a
+ * zero-block grid and exits).  May be called again to replace the scene. */
+mpm_status mpm_init_particles(mpm_engine* engine, int64_t n, const float* soa26_host);
+
+/* Replaces Engine::initSDF(std::vector<Triangle>) (engine.cu:105-114,
+ * kernels.cu:282-300).  triangles_host holds t triangles of 9 floats
+ * (v0.xyz, v1.xyz, v2.xyz) already placed in grid coordinates, the layout of
+ * `struct Triangle` (common.cuh:123-126).  Each node at integer coordinates
+ * gets sign(winding number > 0.5 ? -1 : +1) * distance to the closest
+ * triangle.  t = 0 gives +1e15 everywhere. */
+mpm_status mpm_init_sdf(mpm_engine* engine, const float* triangles_host, int64_t t);
+
+/* ------------------------------------------------------------------ */
+/* Stepping                                                             */
+/* ------------------------------------------------------------------ */
+
+/* Replaces `for (s < nsub) engine.step();` (Simulation.cpp:46-49,
+ * engine.cu:54-70): nsub MLS-MPM substeps (keys, stable sort, clear, P2G,
+ * grid update, G2P), then the float3 position export (kernels.cu:341-347).
+ * Synchronous: returns after the device finished, like the reference's
+ * per-kernel cudaDeviceSynchronize.  nsub = 0 only refreshes the export. */
+mpm_status mpm_step(mpm_engine* engine, int32_t nsub);
+
+/* As mpm_step but only enqueues the work on the engine's stream. */
+mpm_status mpm_step_async(mpm_engine* engine, int32_t nsub);
+
+/* Waits for the engine's stream and reports any asynchronous error. */
+mpm_status mpm_synchronize(mpm_engine* engine);
+
+/* Runs the stages of one substep up to `upto` (MPM_STAGE_*) and stops, so
+ * that a test can read the grid after P2G or after the grid update.  The
+ * particle state only changes for MPM_STAGE_G2P.  The next mpm_step starts
+ * a fresh substep.  Synchronous.  No counterpart in the reference. */
+mpm_status mpm_substep_partial(mpm_engine* engine, int32_t upto);
+
+/* Health checks: when `flags` holds MPM_HEALTH_* bits, mpm_step returns
+ * MPM_ERR_NONFINITE_STATE / MPM_ERR_OUT_OF_GRID after a step in which the
+ * matching condition appeared (the step itself still completes).  Default 0:
+ * like the reference, the step never fails on state contents. */
+mpm_status mpm_set_checks(mpm_engine* engine, uint32_t flags);
+
+/* ------------------------------------------------------------------ */
+/* Readback                                                             */
+/* ------------------------------------------------------------------ */
+
+/* Replaces Engine::getNumber (engine.h:28). */
+int64_t mpm_num_particles(const mpm_engine* engine);
+
+/* Replaces Engine::getBuffer (engine.h:29) + a device-to-host copy: the
+ * 26*n state in ORIGINAL particle order (the order of mpm_init_particles). */
+mpm_status mpm_get_state(mpm_engine* engine, float* soa26_host);
+
+/* Loads a 26*n state saved by mpm_get_state (checkpoint resume).  n must
+ * equal the engine's particle count.  Unlike mpm_init_particles no plane is
+ * overwritten.  VOL and MASS must each hold one value for all particles, as
+ * every state the reference can produce does (initFMatrices sets them and
+ * no kernel writes them); otherwise MPM_ERR_UNSUPPORTED.  No counterpart in
+ * the reference. */
+mpm_status mpm_set_state(mpm_engine* engine, int64_t n, const float* soa26_host);
+
+/* Replaces Engine::getPositions (engine.h:23): n float3 positions in original
+ * order, as changeFormat writes them (kernels.cu:341-347).  The pointer is
+ * owned by the engine and valid until the next step, init or destroy. */
+const float* mpm_positions_device(mpm_engine* engine);
+
+/* mpm_positions_device + a device-to-host copy of 3*n floats. */
+mpm_status mpm_get_positions(mpm_engine* engine, float* xyz_host);
+
+/* Replaces Engine::getGrid (engine.h:22) + a copy of its 4 planes (4*G
+ * floats, plane order MPM_GRID_*).  After a substep: mass from P2G and the
+ * updated node velocities in the momentum planes. */
+mpm_status mpm_get_grid(mpm_engine* engine, float* grid4_host);
+
+/* Copies the G-float signed distance field (Grid::sdf, common.cuh:114). */
+mpm_status mpm_get_sdf(mpm_engine* engine, float* sdf_host);
+
+/* The Morton keys and sort permutation of the most recent substep, as the
+ * reference's sortParticles leaves them (engine.cu:92-102): keys_host[i] is
+ * setKeys' key of particle i (original order, kernels.cu:361-371) and
+ * perm_host[j] is the original index of the j-th particle in stable
+ * ascending key order (d_values after thrust::sort_by_key).  Either pointer
+ * may be NULL.  Before any substep: keys of the current state, identity. */
+mpm_status mpm_get_sort(mpm_engine* engine, int32_t* keys_host, int32_t* perm_host);
+
+/* Counters and accumulated health bits; reset_health clears the bits. */
+mpm_status mpm_get_stats(mpm_engine* engine, mpm_stats* stats, int32_t reset_health);
+
+/* Per-stage device timing.  With max_substeps > 0 the substep graphs also
+ * record CUDA events between the stages (sort, P2G, grid update, G2P) of the
+ * next max_substeps substeps; 0 turns it off and frees the events.  No
+ * counterpart in the reference (it has no timers). */
+mpm_status mpm_set_stage_timing(mpm_engine* engine, int32_t max_substeps);
+
+/* Sums of the recorded stage durations in milliseconds, ms[0..3] = sort,
+ * P2G, grid update, G2P, over *count substeps, then clears the record.
+ * Synchronizes the engine's stream. */
+mpm_status mpm_get_stage_times(mpm_engine* engine, double* ms, int32_t* count);
+
+/* The engine's cudaStream_t, for callers that order their own work after it. */
+void* mpm_stream(mpm_engine* engine);
+
+/* Text of the engine's last error ("" if none).  Never NULL. */
+const char* mpm_last_error(const mpm_engine* engine);
+
+/* Text of the last error of a call that had no engine to record it on
+ * (mpm_create, mpm_sort_particles_device).  Thread-local.  Never NULL. */
+const char* mpm_global_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* Stand-alone device operators                                         */
+/* ------------------------------------------------------------------ */
+
+/* Replaces Engine::sortParticles (engine.cu:92-102) as a free operator on
+ * caller-owned device buffers: d_keys[i] = Morton key of particle i
+ * (setKeys, kernels.cu:361-371) and d_perm = the stable ascending sort
+ * permutation of those keys (thrust::sequence + thrust::sort_by_key).
+ * Positions are three device arrays of n floats.  Work is enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream); scratch memory is
+ * taken with cudaMallocAsync on that stream and released before return, as
+ * the reference allocates its key buffer each call (engine.cu:95,101).
+ * Returns after enqueueing; synchronize the stream before reading. */
+mpm_status mpm_sort_particles_device(const float* d_pos_x, const float* d_pos_y, const float* d_pos_z,
+                                     int64_t n, int32_t* d_keys, int32_t* d_perm, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPM_B200_H */

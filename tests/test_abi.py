@@ -1,0 +1,62 @@
+"""The C-ABI library loads on a CPU-only host and exports every entry point
+declared in include/*.h; no compute call is made here."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(mpm_\w+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    for must in ("mpm_create", "mpm_destroy", "mpm_init_particles", "mpm_init_sdf", "mpm_step", "mpm_get_state",
+                 "mpm_get_positions", "mpm_positions_device", "mpm_get_grid", "mpm_get_sort",
+                 "mpm_sort_particles_device", "mpm_config_parse_file"):
+        assert must in names
+    assert len(names) >= 25
+
+
+def test_library_exports_every_declared_symbol(mpm):
+    lib = ctypes.CDLL(mpm.LIB_PATH)
+    missing = [n for n in sorted(_declared()) if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_abi_version_and_status_strings(mpm):
+    assert mpm.lib.mpm_abi_version() == 1
+    for code, name in mpm.STATUS.items():
+        assert mpm.lib.mpm_status_string(code).decode() == name
+
+
+def test_create_without_gpu_is_an_error(mpm):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(mpm.MpmError) as ei:
+        mpm.Engine(mpm.Config())
+    assert ei.value.name == "MPM_ERR_NO_DEVICE"
+    assert mpm.lib.mpm_global_last_error()
+
+
+def test_null_engine_calls(mpm):
+    lib = mpm.lib
+    assert lib.mpm_step(None, 1) == 1
+    assert lib.mpm_get_state(None, None) == 1
+    assert lib.mpm_num_particles(None) == 0
+    assert lib.mpm_positions_device(None) is None
+    assert lib.mpm_last_error(None) == b""
+    lib.mpm_destroy(None)
+

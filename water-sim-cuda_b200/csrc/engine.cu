@@ -1,0 +1,687 @@
+// Host engine behind the C ABI (include/mpm_b200.h).
+//
+// Restates the reference's `Engine` (engine.h:14-43, engine.cu:36-114) and
+// the config upload (config.cu:5-8, Simulation.cpp:56-77) with per-engine
+// state: one device, one stream, and a CUDA graph per substep parity.
+//
+// Particle order.  The reference never moves particle data: every substep it
+// sorts (key, 0..n-1) and gathers through the permutation.  Here the state
+// lives in the order of the last sort.  A substep from parity p:
+//   sort keys[p] (keys in ORIGINAL order, values 0..n-1, exactly the
+//       reference's thrust::sequence + sort_by_key) -> sigma[1-p] (the
+//       reference's d_values), rank[1-p] = its inverse, and
+//       gidx[j] = rank[p][sigma[1-p][j]], the slot of the j-th particle in P[p];
+//   P2G reads P[p] through gidx (nearly the identity, so nearly streaming);
+//   grid update;
+//   G2P reads P[p] through gidx and writes P[1-p] at j, i.e. reorders the
+//       state for free, and writes the next key at keys[1-p][sigma[1-p][j]].
+// Readback scatters through sigma back to the original order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "mpm_b200.h"
+
+using mpm::SimParams;
+
+namespace {
+
+thread_local std::string g_global_error;
+
+constexpr int kNoSort = -1;
+enum class GridView { kVelocity, kAccum };
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+struct mpm_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    mpm_config cfg{};
+    SimParams prm{};
+    std::string last_error;
+    uint32_t checks = 0;
+
+    bool initialized = false;
+    int n = 0;
+    long long ld = 0;
+    float* P[2] = {nullptr, nullptr};
+    int32_t* keys[2] = {nullptr, nullptr};
+    int32_t* sigma[2] = {nullptr, nullptr};
+    int32_t* rank[2] = {nullptr, nullptr};
+    int32_t* gidx = nullptr;
+    void* sort_mem = nullptr;
+    mpm::SortScratch sort;
+    float* pos_out = nullptr;
+
+    float4* accum = nullptr;
+    float4* vgrid = nullptr;
+    float* sdf = nullptr;
+    uint32_t* d_flags = nullptr;  // [0] health bits, [1] kernel status bits
+
+    float* staging = nullptr;  // device staging for imports/exports
+    size_t staging_bytes = 0;
+
+    int parity = 0;
+    int sort_src = kNoSort;
+    bool accum_dirty = false;
+    GridView grid_view = GridView::kVelocity;
+
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraph_t graph_src[2] = {nullptr, nullptr};
+    int graph_kernels[2] = {0, 0};
+
+    // Stage timing: kTimingMarks event-record nodes per substep graph, pointed
+    // at a fresh slot of `tev` before each launch (scratch events once full).
+    static constexpr int kTimingMarks = 5;
+    int timing_cap = 0;
+    int timing_used = 0;
+    cudaEvent_t* tev = nullptr;
+    cudaEvent_t tscratch[kTimingMarks] = {};
+    cudaGraphNode_t tnode[2][kTimingMarks] = {};
+
+    int64_t substeps = 0;
+    int64_t kernel_launches = 0;
+    int64_t sort_passes = 0;
+    uint32_t health = 0;
+};
+
+namespace {
+
+mpm_status record(mpm_engine* e, mpm_status s, const std::string& msg) {
+    if (e) e->last_error = msg;
+    else g_global_error = msg;
+    return s;
+}
+
+mpm_status cuda_fail(mpm_engine* e, cudaError_t err, const char* what) {
+    cudaGetLastError();  // clear a non-sticky error
+    std::string msg = std::string("CUDA error in ") + what + ": " + cudaGetErrorName(err) + " (" +
+                      cudaGetErrorString(err) + ")";
+    return record(e, err == cudaErrorMemoryAllocation ? MPM_ERR_OUT_OF_MEMORY : MPM_ERR_CUDA, msg);
+}
+
+#define CK(e, call)                                                  \
+    do {                                                             \
+        cudaError_t err_ = (call);                                   \
+        if (err_ != cudaSuccess) return cuda_fail((e), err_, #call); \
+    } while (0)
+
+template <typename T>
+void free_dev(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+void free_particles(mpm_engine* e) {
+    for (int k = 0; k < 2; ++k) {
+        free_dev(e->P[k]);
+        free_dev(e->keys[k]);
+        free_dev(e->sigma[k]);
+        free_dev(e->rank[k]);
+        if (e->graph[k]) cudaGraphExecDestroy(e->graph[k]);
+        if (e->graph_src[k]) cudaGraphDestroy(e->graph_src[k]);
+        e->graph[k] = nullptr;
+        e->graph_src[k] = nullptr;
+        e->graph_kernels[k] = 0;
+    }
+    free_dev(e->gidx);
+    free_dev(e->sort_mem);
+    free_dev(e->pos_out);
+    e->initialized = false;
+}
+
+mpm_status ensure_staging(mpm_engine* e, size_t bytes) {
+    if (e->staging_bytes >= bytes) return MPM_OK;
+    free_dev(e->staging);
+    e->staging_bytes = 0;
+    CK(e, cudaMalloc(&e->staging, bytes));
+    e->staging_bytes = bytes;
+    return MPM_OK;
+}
+
+mpm_status alloc_particles(mpm_engine* e, int n) {
+    free_particles(e);
+    e->n = n;
+    e->ld = (long long)align_up((size_t)std::max(n, 1), 64);
+    const size_t ibytes = (size_t)e->ld * sizeof(int32_t);
+    for (int k = 0; k < 2; ++k) {
+        CK(e, cudaMalloc(&e->P[k], (size_t)mpm::kStatePlanes * e->ld * sizeof(float)));
+        CK(e, cudaMalloc(&e->keys[k], ibytes));
+        CK(e, cudaMalloc(&e->sigma[k], ibytes));
+        CK(e, cudaMalloc(&e->rank[k], ibytes));
+    }
+    CK(e, cudaMalloc(&e->gidx, ibytes));
+    CK(e, cudaMalloc(&e->sort_mem, mpm::sort_scratch_bytes(std::max(n, 1))));
+    mpm::sort_scratch_carve(e->sort_mem, std::max(n, 1), &e->sort);
+    e->sort.n = n;
+    CK(e, cudaMalloc(&e->pos_out, (size_t)std::max(n, 1) * 3 * sizeof(float)));
+    return MPM_OK;
+}
+
+// Enqueues the stages of one substep from parity `par`, up to `upto`.  With
+// `marks`, records marks[0..4] before the sort and after each stage.
+int enqueue_substep(mpm_engine* e, int par, int upto, const cudaEvent_t* marks = nullptr) {
+    const SimParams& p = e->prm;
+    cudaStream_t st = e->stream;
+    if (marks) cudaEventRecord(marks[0], st);
+    int launches = mpm::launch_radix_sort(e->keys[par], p.n, e->sort, e->sigma[1 - par], e->rank[1 - par],
+                                          e->rank[par], e->gidx, st);
+    if (marks) cudaEventRecord(marks[1], st);
+    if (upto >= MPM_STAGE_P2G) launches += mpm::launch_p2g(p, e->P[par], e->gidx, e->accum, st);
+    if (marks) cudaEventRecord(marks[2], st);
+    if (upto >= MPM_STAGE_GRID) launches += mpm::launch_grid_update(p, e->accum, e->vgrid, e->sdf, st);
+    if (marks) cudaEventRecord(marks[3], st);
+    if (upto >= MPM_STAGE_G2P)
+        launches += mpm::launch_g2p(p, e->P[par], e->P[1 - par], e->gidx, e->sigma[1 - par], e->vgrid, e->sdf,
+                                    e->keys[1 - par], e->d_flags, st);
+    if (marks) cudaEventRecord(marks[4], st);
+    return launches;
+}
+
+mpm_status capture_graphs(mpm_engine* e) {
+    const bool timed = e->timing_cap > 0;
+    for (int par = 0; par < 2; ++par) {
+        if (e->graph[par]) cudaGraphExecDestroy(e->graph[par]);
+        if (e->graph_src[par]) cudaGraphDestroy(e->graph_src[par]);
+        e->graph[par] = nullptr;
+        e->graph_src[par] = nullptr;
+        cudaGraph_t g = nullptr;
+        CK(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        const int launches = enqueue_substep(e, par, MPM_STAGE_G2P, timed ? e->tscratch : nullptr);
+        const cudaError_t launch_err = cudaGetLastError();
+        const cudaError_t end_err = cudaStreamEndCapture(e->stream, &g);
+        if (launch_err != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(e, launch_err, "substep capture");
+        }
+        CK(e, end_err);
+        e->graph_src[par] = g;
+        if (timed) {
+            // Find the event-record nodes by the scratch event each records.
+            size_t count = 0;
+            CK(e, cudaGraphGetNodes(g, nullptr, &count));
+            std::vector<cudaGraphNode_t> nodes(count);
+            CK(e, cudaGraphGetNodes(g, nodes.data(), &count));
+            for (cudaGraphNode_t nd : nodes) {
+                cudaGraphNodeType type;
+                CK(e, cudaGraphNodeGetType(nd, &type));
+                if (type != cudaGraphNodeTypeEventRecord) continue;
+                cudaEvent_t ev;
+                CK(e, cudaGraphEventRecordNodeGetEvent(nd, &ev));
+                for (int k = 0; k < mpm_engine::kTimingMarks; ++k)
+                    if (ev == e->tscratch[k]) e->tnode[par][k] = nd;
+            }
+        }
+        CK(e, cudaGraphInstantiate(&e->graph[par], g, 0));
+        e->graph_kernels[par] = launches;
+    }
+    return MPM_OK;
+}
+
+void free_timing(mpm_engine* e) {
+    if (e->tev) {
+        for (int i = 0; i < e->timing_cap * mpm_engine::kTimingMarks; ++i) cudaEventDestroy(e->tev[i]);
+        delete[] e->tev;
+    }
+    e->tev = nullptr;
+    for (int k = 0; k < mpm_engine::kTimingMarks; ++k) {
+        if (e->tscratch[k]) cudaEventDestroy(e->tscratch[k]);
+        e->tscratch[k] = nullptr;
+    }
+    e->timing_cap = 0;
+    e->timing_used = 0;
+}
+
+mpm_status sync_and_collect(mpm_engine* e) {
+    uint32_t flags[2] = {0, 0};
+    CK(e, cudaMemcpyAsync(flags, e->d_flags, sizeof(flags), cudaMemcpyDeviceToHost, e->stream));
+    CK(e, cudaStreamSynchronize(e->stream));
+    e->health |= flags[0];
+    if (flags[1] & mpm::kStatusTimeout) {
+        CK(e, cudaMemsetAsync(e->d_flags + 1, 0, sizeof(uint32_t), e->stream));
+        return record(e, MPM_ERR_TIMEOUT, "a bounded device-side wait gave up");
+    }
+    return MPM_OK;
+}
+
+mpm_status check_health(mpm_engine* e) {
+    const uint32_t seen = e->health & e->checks;
+    if (seen & MPM_HEALTH_NONFINITE)
+        return record(e, MPM_ERR_NONFINITE_STATE, "a particle position or velocity is not finite");
+    if (seen & MPM_HEALTH_OUT_OF_GRID)
+        return record(e, MPM_ERR_OUT_OF_GRID, "a particle position is outside the grid");
+    return MPM_OK;
+}
+
+bool finite_cfg(const mpm_config* c) {
+    return std::isfinite(c->gravity) && std::isfinite(c->dt) && std::isfinite(c->gamma) &&
+           std::isfinite(c->compression) && std::isfinite(c->resolution);
+}
+
+// Uploads a 26-plane host state and imports it (init_rules: Engine::init).
+mpm_status load_state(mpm_engine* e, const float* soa26_host, bool init_rules) {
+    const int n = e->n;
+    if (n > 0) {
+        const size_t bytes = (size_t)MPM_PARTICLE_PLANES * n * sizeof(float);
+        mpm_status s = ensure_staging(e, bytes);
+        if (s != MPM_OK) return s;
+        CK(e, cudaMemcpyAsync(e->staging, soa26_host, bytes, cudaMemcpyHostToDevice, e->stream));
+        e->kernel_launches += mpm::launch_state_import(e->prm, e->staging, e->P[0], e->sigma[0], e->rank[0],
+                                                       e->keys[0], init_rules, e->stream);
+        CK(e, cudaGetLastError());
+    }
+    e->parity = 0;
+    e->sort_src = kNoSort;
+    CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
+    CK(e, cudaMemsetAsync(e->vgrid, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
+    CK(e, cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(uint32_t), e->stream));
+    e->accum_dirty = false;
+    e->grid_view = GridView::kVelocity;
+    e->health = 0;
+    e->kernel_launches += mpm::launch_positions_export(e->prm, e->P[0], e->sigma[0], e->pos_out, e->stream);
+    CK(e, cudaGetLastError());
+    mpm_status s = capture_graphs(e);
+    if (s != MPM_OK) return s;
+    e->initialized = true;
+    return sync_and_collect(e);
+}
+
+mpm_status enter(mpm_engine* e) {
+    if (!e) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "engine is NULL");
+    e->last_error.clear();
+    CK(e, cudaSetDevice(e->device));
+    return MPM_OK;
+}
+
+mpm_status run_steps(mpm_engine* e, int32_t nsub) {
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (nsub < 0) return record(e, MPM_ERR_INVALID_ARGUMENT, "nsub < 0");
+    if (e->accum_dirty) {
+        CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
+        e->accum_dirty = false;
+    }
+    for (int s = 0; s < nsub; ++s) {
+        if (e->timing_cap > 0) {
+            const int par = e->parity;
+            const bool slot = e->timing_used < e->timing_cap;
+            const cudaEvent_t* evs = slot ? e->tev + (size_t)e->timing_used * mpm_engine::kTimingMarks : e->tscratch;
+            for (int k = 0; k < mpm_engine::kTimingMarks; ++k)
+                CK(e, cudaGraphExecEventRecordNodeSetEvent(e->graph[par], e->tnode[par][k], evs[k]));
+            if (slot) ++e->timing_used;
+        }
+        CK(e, cudaGraphLaunch(e->graph[e->parity], e->stream));
+        e->kernel_launches += e->graph_kernels[e->parity];
+        e->sort_passes += e->n > 0 ? 4 : 0;
+        e->sort_src = e->parity;
+        e->parity ^= 1;
+        ++e->substeps;
+    }
+    if (nsub > 0) e->grid_view = GridView::kVelocity;
+    e->kernel_launches +=
+        mpm::launch_positions_export(e->prm, e->P[e->parity], e->sigma[e->parity], e->pos_out, e->stream);
+    CK(e, cudaGetLastError());
+    return MPM_OK;
+}
+
+}  // namespace
+
+// -------------------------------------------------------------------------
+
+extern "C" int32_t mpm_abi_version(void) { return MPM_ABI_VERSION; }
+
+extern "C" const char* mpm_status_string(mpm_status s) {
+    switch (s) {
+        case MPM_OK: return "MPM_OK";
+        case MPM_ERR_INVALID_ARGUMENT: return "MPM_ERR_INVALID_ARGUMENT";
+        case MPM_ERR_BAD_CONFIG: return "MPM_ERR_BAD_CONFIG";
+        case MPM_ERR_IO: return "MPM_ERR_IO";
+        case MPM_ERR_CUDA: return "MPM_ERR_CUDA";
+        case MPM_ERR_OUT_OF_MEMORY: return "MPM_ERR_OUT_OF_MEMORY";
+        case MPM_ERR_NOT_INITIALIZED: return "MPM_ERR_NOT_INITIALIZED";
+        case MPM_ERR_NONFINITE_STATE: return "MPM_ERR_NONFINITE_STATE";
+        case MPM_ERR_OUT_OF_GRID: return "MPM_ERR_OUT_OF_GRID";
+        case MPM_ERR_TIMEOUT: return "MPM_ERR_TIMEOUT";
+        case MPM_ERR_UNSUPPORTED: return "MPM_ERR_UNSUPPORTED";
+        case MPM_ERR_NO_DEVICE: return "MPM_ERR_NO_DEVICE";
+    }
+    return "MPM_ERR_UNKNOWN";
+}
+
+extern "C" mpm_status mpm_create(const mpm_config* cfg, int32_t device, mpm_engine** out) {
+    g_global_error.clear();
+    if (!cfg || !out) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "cfg and out must be non-NULL");
+    *out = nullptr;
+    if (cfg->size_x <= 0 || cfg->size_y <= 0 || cfg->size_z <= 0)
+        return record(nullptr, MPM_ERR_BAD_CONFIG, "SIZE_X/Y/Z must be positive");
+    const long long g = (long long)cfg->size_x * cfg->size_y * cfg->size_z;
+    if (g > 0x7fffffffLL) return record(nullptr, MPM_ERR_BAD_CONFIG, "grid has more than 2^31-1 nodes");
+    if (!finite_cfg(cfg)) return record(nullptr, MPM_ERR_BAD_CONFIG, "a float parameter is not finite");
+
+    int count = 0;
+    cudaError_t err = cudaGetDeviceCount(&count);
+    if (err != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return record(nullptr, MPM_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(err));
+    }
+    if (device < 0 || device >= count) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "device index out of range");
+    cudaDeviceProp prop;
+    err = cudaGetDeviceProperties(&prop, device);
+    if (err != cudaSuccess) return cuda_fail(nullptr, err, "cudaGetDeviceProperties");
+    if (prop.major != 10 || prop.minor != 0)
+        return record(nullptr, MPM_ERR_NO_DEVICE,
+                      std::string("this library is built for sm_100a (B200); device is ") + prop.name);
+
+    mpm_engine* e = new mpm_engine();
+    e->device = device;
+    e->cfg = *cfg;
+    SimParams& p = e->prm;
+    p.sx = cfg->size_x;
+    p.sy = cfg->size_y;
+    p.sz = cfg->size_z;
+    p.padding = cfg->padding;
+    p.gravity = cfg->gravity;
+    p.dt = cfg->dt;
+    p.gamma = cfg->gamma;
+    p.compression = cfg->compression;
+    p.pvol = cfg->resolution * cfg->resolution * cfg->resolution;  // kernels.cu:356
+    p.pmass = 1.0f;                                                // kernels.cu:357
+    p.n = 0;
+    p.g = (int)g;
+    p.ld = 64;
+
+    auto fail = [&](mpm_status s) {
+        g_global_error = e->last_error;
+        mpm_destroy(e);
+        return s;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(cuda_fail(e, cudaGetLastError(), "cudaSetDevice"));
+    if ((err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(cuda_fail(e, err, "cudaStreamCreate"));
+    if ((err = cudaMalloc(&e->accum, (size_t)g * sizeof(float4))) != cudaSuccess ||
+        (err = cudaMalloc(&e->vgrid, (size_t)g * sizeof(float4))) != cudaSuccess ||
+        (err = cudaMalloc(&e->sdf, (size_t)g * sizeof(float))) != cudaSuccess ||
+        (err = cudaMalloc(&e->d_flags, 2 * sizeof(uint32_t))) != cudaSuccess)
+        return fail(cuda_fail(e, err, "cudaMalloc(grid)"));
+    cudaMemsetAsync(e->accum, 0, (size_t)g * sizeof(float4), e->stream);
+    cudaMemsetAsync(e->vgrid, 0, (size_t)g * sizeof(float4), e->stream);
+    cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(uint32_t), e->stream);
+    // An empty triangle list leaves sqrt(1e30) everywhere (kernels.cu:289,299).
+    e->kernel_launches += mpm::launch_fill(e->sdf, g, sqrtf(1e30f), e->stream);
+    if ((err = cudaGetLastError()) != cudaSuccess) return fail(cuda_fail(e, err, "sdf fill"));
+    if ((err = cudaStreamSynchronize(e->stream)) != cudaSuccess) return fail(cuda_fail(e, err, "create sync"));
+    *out = e;
+    return MPM_OK;
+}
+
+extern "C" void mpm_destroy(mpm_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    free_particles(e);
+    free_timing(e);
+    free_dev(e->accum);
+    free_dev(e->vgrid);
+    free_dev(e->sdf);
+    free_dev(e->d_flags);
+    free_dev(e->staging);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+extern "C" mpm_status mpm_init_particles(mpm_engine* e, int64_t n, const float* soa26_host) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (n < 0 || n > 0x7fffffffLL - 64) return record(e, MPM_ERR_INVALID_ARGUMENT, "n out of range");
+    if (n > 0 && !soa26_host) return record(e, MPM_ERR_INVALID_ARGUMENT, "soa26_host is NULL");
+    if ((s = alloc_particles(e, (int)n)) != MPM_OK) return s;
+    e->prm.n = (int)n;
+    e->prm.ld = e->ld;
+    e->prm.pvol = e->cfg.resolution * e->cfg.resolution * e->cfg.resolution;
+    e->prm.pmass = 1.0f;
+    e->substeps = 0;
+    return load_state(e, soa26_host, true);
+}
+
+extern "C" mpm_status mpm_set_state(mpm_engine* e, int64_t n, const float* soa26_host) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (n != e->n) return record(e, MPM_ERR_INVALID_ARGUMENT, "n differs from the engine's particle count");
+    if (n > 0 && !soa26_host) return record(e, MPM_ERR_INVALID_ARGUMENT, "soa26_host is NULL");
+    if (n > 0) {
+        const float* vol = soa26_host + (size_t)MPM_VOL * n;
+        const float* mass = soa26_host + (size_t)MPM_MASS * n;
+        for (int64_t i = 1; i < n; ++i) {
+            if (std::memcmp(&vol[i], &vol[0], sizeof(float)) != 0 || std::memcmp(&mass[i], &mass[0], sizeof(float)) != 0)
+                return record(e, MPM_ERR_UNSUPPORTED, "VOL and MASS must each be uniform over the particles");
+        }
+        e->prm.pvol = vol[0];
+        e->prm.pmass = mass[0];
+    }
+    return load_state(e, soa26_host, false);
+}
+
+extern "C" mpm_status mpm_init_sdf(mpm_engine* e, const float* tris, int64_t t) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (t < 0 || t > 0x7fffffffLL / 9) return record(e, MPM_ERR_INVALID_ARGUMENT, "triangle count out of range");
+    if (t > 0 && !tris) return record(e, MPM_ERR_INVALID_ARGUMENT, "triangles_host is NULL");
+    if (t == 0) {
+        e->kernel_launches += mpm::launch_fill(e->sdf, e->prm.g, sqrtf(1e30f), e->stream);
+        CK(e, cudaGetLastError());
+        CK(e, cudaStreamSynchronize(e->stream));
+        return MPM_OK;
+    }
+    const size_t bytes = (size_t)t * 9 * sizeof(float);
+    float* d_tris = nullptr;
+    CK(e, cudaMallocAsync(&d_tris, align_up(bytes, 16) + 16, e->stream));
+    cudaError_t err = cudaMemcpyAsync(d_tris, tris, bytes, cudaMemcpyHostToDevice, e->stream);
+    if (err == cudaSuccess) {
+        e->kernel_launches += mpm::launch_sdf_build(e->prm, d_tris, (int)t, e->sdf, e->d_flags + 1, e->stream);
+        err = cudaGetLastError();
+    }
+    cudaFreeAsync(d_tris, e->stream);
+    if (err != cudaSuccess) return cuda_fail(e, err, "sdf build");
+    return sync_and_collect(e);
+}
+
+extern "C" mpm_status mpm_step_async(mpm_engine* e, int32_t nsub) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    return run_steps(e, nsub);
+}
+
+extern "C" mpm_status mpm_synchronize(mpm_engine* e) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if ((s = sync_and_collect(e)) != MPM_OK) return s;
+    return check_health(e);
+}
+
+extern "C" mpm_status mpm_step(mpm_engine* e, int32_t nsub) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if ((s = run_steps(e, nsub)) != MPM_OK) return s;
+    if ((s = sync_and_collect(e)) != MPM_OK) return s;
+    return check_health(e);
+}
+
+extern "C" mpm_status mpm_substep_partial(mpm_engine* e, int32_t upto) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (upto < MPM_STAGE_SORT || upto > MPM_STAGE_G2P) return record(e, MPM_ERR_INVALID_ARGUMENT, "bad stage");
+    if (upto == MPM_STAGE_G2P) return mpm_step(e, 1);
+    if (e->accum_dirty) CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
+    e->kernel_launches += enqueue_substep(e, e->parity, upto);
+    CK(e, cudaGetLastError());
+    e->sort_passes += e->n > 0 ? 4 : 0;
+    e->sort_src = e->parity;
+    if (upto == MPM_STAGE_P2G) {
+        e->accum_dirty = true;
+        e->grid_view = GridView::kAccum;
+    } else if (upto == MPM_STAGE_GRID) {
+        e->accum_dirty = false;
+        e->grid_view = GridView::kVelocity;
+    }
+    return sync_and_collect(e);
+}
+
+extern "C" mpm_status mpm_set_checks(mpm_engine* e, uint32_t flags) {
+    if (!e) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "engine is NULL");
+    e->checks = flags & (MPM_HEALTH_NONFINITE | MPM_HEALTH_OUT_OF_GRID);
+    return MPM_OK;
+}
+
+extern "C" int64_t mpm_num_particles(const mpm_engine* e) { return (e && e->initialized) ? e->n : 0; }
+
+extern "C" mpm_status mpm_get_state(mpm_engine* e, float* out) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (e->n == 0) return MPM_OK;
+    if (!out) return record(e, MPM_ERR_INVALID_ARGUMENT, "soa26_host is NULL");
+    const size_t bytes = (size_t)MPM_PARTICLE_PLANES * e->n * sizeof(float);
+    if ((s = ensure_staging(e, bytes)) != MPM_OK) return s;
+    e->kernel_launches += mpm::launch_state_export(e->prm, e->P[e->parity], e->sigma[e->parity], e->staging, e->stream);
+    CK(e, cudaGetLastError());
+    CK(e, cudaMemcpyAsync(out, e->staging, bytes, cudaMemcpyDeviceToHost, e->stream));
+    CK(e, cudaStreamSynchronize(e->stream));
+    return MPM_OK;
+}
+
+extern "C" const float* mpm_positions_device(mpm_engine* e) {
+    return (e && e->initialized) ? e->pos_out : nullptr;
+}
+
+extern "C" mpm_status mpm_get_positions(mpm_engine* e, float* xyz) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (e->n == 0) return MPM_OK;
+    if (!xyz) return record(e, MPM_ERR_INVALID_ARGUMENT, "xyz_host is NULL");
+    CK(e, cudaMemcpyAsync(xyz, e->pos_out, (size_t)e->n * 3 * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    CK(e, cudaStreamSynchronize(e->stream));
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_get_grid(mpm_engine* e, float* out) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!out) return record(e, MPM_ERR_INVALID_ARGUMENT, "grid4_host is NULL");
+    const size_t bytes = (size_t)MPM_GRID_PLANES * e->prm.g * sizeof(float);
+    if ((s = ensure_staging(e, bytes)) != MPM_OK) return s;
+    const float4* src = e->grid_view == GridView::kAccum ? e->accum : e->vgrid;
+    e->kernel_launches += mpm::launch_grid_export(e->prm, src, e->staging, e->stream);
+    CK(e, cudaGetLastError());
+    CK(e, cudaMemcpyAsync(out, e->staging, bytes, cudaMemcpyDeviceToHost, e->stream));
+    CK(e, cudaStreamSynchronize(e->stream));
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_get_sdf(mpm_engine* e, float* out) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!out) return record(e, MPM_ERR_INVALID_ARGUMENT, "sdf_host is NULL");
+    CK(e, cudaMemcpyAsync(out, e->sdf, (size_t)e->prm.g * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    CK(e, cudaStreamSynchronize(e->stream));
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_get_sort(mpm_engine* e, int32_t* keys_host, int32_t* perm_host) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (e->n == 0) return MPM_OK;
+    const size_t bytes = (size_t)e->n * sizeof(int32_t);
+    const int32_t* k = e->sort_src == kNoSort ? e->keys[e->parity] : e->keys[e->sort_src];
+    const int32_t* q = e->sort_src == kNoSort ? e->sigma[e->parity] : e->sigma[1 - e->sort_src];
+    if (keys_host) CK(e, cudaMemcpyAsync(keys_host, k, bytes, cudaMemcpyDeviceToHost, e->stream));
+    if (perm_host) CK(e, cudaMemcpyAsync(perm_host, q, bytes, cudaMemcpyDeviceToHost, e->stream));
+    CK(e, cudaStreamSynchronize(e->stream));
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_get_stats(mpm_engine* e, mpm_stats* st, int32_t reset_health) {
+    if (!e || !st) return record(e, MPM_ERR_INVALID_ARGUMENT, "engine and stats must be non-NULL");
+    st->substeps = e->substeps;
+    st->kernel_launches = e->kernel_launches;
+    st->sort_passes = e->sort_passes;
+    st->health = e->health;
+    st->reserved = 0;
+    if (reset_health) e->health = 0;
+    return MPM_OK;
+}
+
+extern "C" void* mpm_stream(mpm_engine* e) { return e ? (void*)e->stream : nullptr; }
+
+extern "C" const char* mpm_last_error(const mpm_engine* e) { return e ? e->last_error.c_str() : ""; }
+
+extern "C" const char* mpm_global_last_error(void) { return g_global_error.c_str(); }
+
+extern "C" mpm_status mpm_sort_particles_device(const float* px, const float* py, const float* pz, int64_t n,
+                                                int32_t* d_keys, int32_t* d_perm, void* stream) {
+    g_global_error.clear();
+    if (n < 0 || n > 0x7fffffffLL - 64) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "n out of range");
+    if (n == 0) return MPM_OK;
+    if (!px || !py || !pz || !d_keys || !d_perm)
+        return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "device pointers must be non-NULL");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int ni = (int)n;
+    void* scratch = nullptr;
+    CK(nullptr, cudaMallocAsync(&scratch, mpm::sort_scratch_bytes(ni), st));
+    mpm::SortScratch s;
+    mpm::sort_scratch_carve(scratch, ni, &s);
+    mpm::launch_morton_keys(px, py, pz, ni, d_keys, st);
+    mpm::launch_radix_sort(d_keys, ni, s, d_perm, nullptr, nullptr, nullptr, st);
+    const cudaError_t launch_err = cudaGetLastError();
+    const cudaError_t free_err = cudaFreeAsync(scratch, st);
+    if (launch_err != cudaSuccess) return cuda_fail(nullptr, launch_err, "sort launch");
+    CK(nullptr, free_err);
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_set_stage_timing(mpm_engine* e, int32_t max_substeps) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (max_substeps < 0 || max_substeps > (1 << 20))
+        return record(e, MPM_ERR_INVALID_ARGUMENT, "max_substeps out of range");
+    CK(e, cudaStreamSynchronize(e->stream));
+    free_timing(e);
+    if (max_substeps > 0) {
+        for (int k = 0; k < mpm_engine::kTimingMarks; ++k) CK(e, cudaEventCreate(&e->tscratch[k]));
+        const int total = max_substeps * mpm_engine::kTimingMarks;
+        e->tev = new cudaEvent_t[total]();
+        e->timing_cap = max_substeps;
+        for (int i = 0; i < total; ++i) CK(e, cudaEventCreate(&e->tev[i]));
+    }
+    if (e->initialized) return capture_graphs(e);
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_get_stage_times(mpm_engine* e, double* ms, int32_t* count) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!ms || !count) return record(e, MPM_ERR_INVALID_ARGUMENT, "ms and count must be non-NULL");
+    CK(e, cudaStreamSynchronize(e->stream));
+    for (int k = 0; k < 4; ++k) ms[k] = 0.0;
+    for (int sidx = 0; sidx < e->timing_used; ++sidx) {
+        const cudaEvent_t* ev = e->tev + (size_t)sidx * mpm_engine::kTimingMarks;
+        for (int k = 0; k < 4; ++k) {
+            float t = 0.0f;
+            CK(e, cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+            ms[k] += t;
+        }
+    }
+    *count = e->timing_used;
+    e->timing_used = 0;
+    return MPM_OK;
+}

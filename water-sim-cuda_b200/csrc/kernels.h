@@ -1,0 +1,74 @@
+// Host-side launchers of the engine's CUDA kernels.  Each launcher enqueues
+// its kernels on `st` and returns how many kernel launches it issued, so the
+// engine can count the launches of a step.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_math.cuh"
+
+namespace mpm {
+
+// ---------------------------------------------------------------- sort ----
+// Stable LSD radix sort of 32-bit signed keys, 8-bit digits, 4 passes.
+// Each pass is histogram -> per-digit spine scan -> scatter; no kernel waits
+// on another CTA, so nothing can spin on the GPU.
+struct SortScratch {
+    int32_t* key_a = nullptr;
+    int32_t* val_a = nullptr;
+    int32_t* key_b = nullptr;
+    int32_t* val_b = nullptr;
+    uint32_t* hist = nullptr;    // [256][nb] per-CTA digit counts, scanned in place
+    uint32_t* totals = nullptr;  // [256] digit totals of the pass
+    int n = 0;
+    int nb = 0;       // CTAs per pass
+    int per_cta = 0;  // keys per CTA (multiple of the 2048-key tile)
+};
+
+// Bytes of scratch for sorting n keys (256-byte aligned sub-buffers).
+size_t sort_scratch_bytes(int n);
+// Points the scratch sub-buffers into `base` (sort_scratch_bytes(n) bytes).
+void sort_scratch_carve(void* base, int n, SortScratch* s);
+
+// keys[i] = Morton key of (px[i], py[i], pz[i]) (setKeys, kernels.cu:361-371).
+int launch_morton_keys(const float* px, const float* py, const float* pz, int n, int32_t* keys, cudaStream_t st);
+
+// Sorts `keys` (n signed ints, left unchanged) with values 0..n-1, stable, and
+// writes the permutation sigma[j] = index of the j-th smallest key, the
+// result of thrust::sequence + thrust::sort_by_key (engine.cu:98-99).
+// If rank_out is non-null it also writes rank_out[sigma[j]] = j, and if gidx
+// is non-null gidx[j] = rank_in[sigma[j]] (rank_in null: sigma[j]).
+int launch_radix_sort(const int32_t* keys, int n, const SortScratch& s, int32_t* sigma, int32_t* rank_out,
+                      const int32_t* rank_in, int32_t* gidx, cudaStream_t st);
+
+// ------------------------------------------------------------- substep ----
+// P holds kStatePlanes planes of stride p.ld in the order sigma of the last
+// sort; gidx[j] is the slot in P of the j-th particle of the new order.
+int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, float4* accum, cudaStream_t st);
+int launch_grid_update(const SimParams& p, float4* accum, float4* vgrid, const float* sdf, cudaStream_t st);
+int launch_g2p(const SimParams& p, const float* Pin, float* Pout, const int32_t* gidx, const int32_t* sigma,
+               const float4* vgrid, const float* sdf, int32_t* keys_out, uint32_t* health, cudaStream_t st);
+
+// ------------------------------------------------------ state transfer ----
+// Loads a 26-plane host-layout state (already on the device, stride n) into
+// P (stride p.ld, original order) and resets the order to the identity.
+// init_rules applies initFMatrices (kernels.cu:349-358): F diagonal = 1.
+int launch_state_import(const SimParams& p, const float* soa26, float* P, int32_t* sigma, int32_t* rank,
+                        int32_t* keys, bool init_rules, cudaStream_t st);
+// Writes the 26-plane state in original order: out[k*n + sigma[j]] = P[k][j].
+int launch_state_export(const SimParams& p, const float* P, const int32_t* sigma, float* soa26, cudaStream_t st);
+// Float3 positions in original order (changeFormat, kernels.cu:341-347).
+int launch_positions_export(const SimParams& p, const float* P, const int32_t* sigma, float* xyz, cudaStream_t st);
+// Node float4 (mass, x, y, z) -> 4 planes.
+int launch_grid_export(const SimParams& p, const float4* grid, float* planes4, cudaStream_t st);
+
+// ----------------------------------------------------------------- sdf ----
+// tris: 9*t floats on the device, allocation padded by >= 16 bytes.
+int launch_sdf_build(const SimParams& p, const float* tris, int t, float* sdf, uint32_t* status, cudaStream_t st);
+int launch_fill(float* dst, long long count, float value, cudaStream_t st);
+
+// Device status bits written by kernels with bounded waits.
+enum : uint32_t { kStatusTimeout = 1u << 0 };
+
+}  // namespace mpm

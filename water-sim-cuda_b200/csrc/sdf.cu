@@ -1,0 +1,209 @@
+// Signed distance field of the obstacle triangles on the simulation grid
+// (makeSDF, kernels.cu:282-300; Engine::initSDF, engine.cu:105-114).
+//
+// One thread per node at integer coordinates.  Every CTA streams the whole
+// triangle list through shared memory in tiles of 256 triangles: one thread
+// issues a bulk async copy (cp.async.bulk, the 1-D TMA path) of the next tile
+// into the second buffer while the CTA evaluates the current one, and
+// completion is tracked by an mbarrier.  Each wait gives up after a fixed
+// time, records kStatusTimeout and drains the copies still in flight before
+// the CTA returns, so a lost completion cannot hang the device.
+//
+// Per node-triangle pair the kernel adds the signed solid angle
+// (Van Oosterom & Strackee, 1983) and keeps the minimum squared distance to
+// the triangle (closest point by Voronoi regions, Ericson, "Real-Time
+// Collision Detection" 5.1.5), in triangle order like the reference.  The
+// node is inside when the winding number, the solid-angle sum divided by
+// 4 * 3.1415 (the reference's constant, kernels.cu:298), exceeds 0.5.
+#include "kernels.h"
+
+namespace mpm {
+namespace {
+
+constexpr int kSdfThreads = 256;
+constexpr int kTriTile = 256;                 // triangles per stage
+constexpr int kTriFloats = 9;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per wait
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void proxy_fence_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for phase `parity` of `bar`; false after kWaitNs.
+__device__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (globaltimer_ns() - t0 > kWaitNs) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    return ax * bx + ay * by + az * bz;
+}
+
+// Signed solid angle of triangle (a, b, c) seen from the origin, the vertices
+// already relative to the node (calculateSolidAngle, common.cuh:310-323).
+__device__ __forceinline__ float solid_angle(float ax, float ay, float az, float bx, float by, float bz, float cx,
+                                             float cy, float cz) {
+    const float la = norm3df(ax, ay, az), lb = norm3df(bx, by, bz), lc = norm3df(cx, cy, cz);
+    const float det = ax * (by * cz - bz * cy) + ay * (bz * cx - bx * cz) + az * (bx * cy - by * cx);
+    const float div = la * lb * lc + dot3(ax, ay, az, bx, by, bz) * lc + dot3(ax, ay, az, cx, cy, cz) * lb +
+                      dot3(bx, by, bz, cx, cy, cz) * la;
+    return 2.0f * atan2f(det, div);
+}
+
+// Squared distance from P to triangle (a, b, c) (pointTriangleDistanceSq,
+// common.cuh:325-378).
+__device__ __forceinline__ float tri_dist2(float px, float py, float pz, const float* t) {
+    const float ax = t[0], ay = t[1], az = t[2];
+    const float abx = t[3] - ax, aby = t[4] - ay, abz = t[5] - az;
+    const float acx = t[6] - ax, acy = t[7] - ay, acz = t[8] - az;
+    const float apx = px - ax, apy = py - ay, apz = pz - az;
+    const float d1 = dot3(abx, aby, abz, apx, apy, apz), d2 = dot3(acx, acy, acz, apx, apy, apz);
+    if (d1 <= 0.0f && d2 <= 0.0f) return dot3(apx, apy, apz, apx, apy, apz);
+    const float bpx = px - t[3], bpy = py - t[4], bpz = pz - t[5];
+    const float d3 = dot3(abx, aby, abz, bpx, bpy, bpz), d4 = dot3(acx, acy, acz, bpx, bpy, bpz);
+    if (d3 >= 0.0f && d4 <= d3) return dot3(bpx, bpy, bpz, bpx, bpy, bpz);
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+        const float v = d1 / (d1 - d3);
+        const float qx = px - (ax + v * abx), qy = py - (ay + v * aby), qz = pz - (az + v * abz);
+        return dot3(qx, qy, qz, qx, qy, qz);
+    }
+    const float cpx = px - t[6], cpy = py - t[7], cpz = pz - t[8];
+    const float d5 = dot3(abx, aby, abz, cpx, cpy, cpz), d6 = dot3(acx, acy, acz, cpx, cpy, cpz);
+    if (d6 >= 0.0f && d5 <= d6) return dot3(cpx, cpy, cpz, cpx, cpy, cpz);
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+        const float w = d2 / (d2 - d6);
+        const float qx = px - (ax + w * acx), qy = py - (ay + w * acy), qz = pz - (az + w * acz);
+        return dot3(qx, qy, qz, qx, qy, qz);
+    }
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+        const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        const float qx = px - (t[3] + w * (t[6] - t[3])), qy = py - (t[4] + w * (t[7] - t[4])),
+                    qz = pz - (t[5] + w * (t[8] - t[5]));
+        return dot3(qx, qy, qz, qx, qy, qz);
+    }
+    const float denom = 1.0f / (va + vb + vc);
+    const float v = vb * denom, w = vc * denom;
+    const float qx = px - (ax + abx * v + acx * w), qy = py - (ay + aby * v + acy * w),
+                qz = pz - (az + abz * v + acz * w);
+    return dot3(qx, qy, qz, qx, qy, qz);
+}
+
+__global__ void __launch_bounds__(kSdfThreads) sdf_build_kernel(SimParams p, const float* __restrict__ tris,
+                                                                int t_count, float* __restrict__ sdf,
+                                                                uint32_t* __restrict__ status) {
+    __shared__ __align__(128) float s_tri[2][kTriTile * kTriFloats];
+    __shared__ __align__(8) uint64_t s_bar[2];
+
+    const int node = blockIdx.x * kSdfThreads + threadIdx.x;
+    const int x = node % p.sx, y = (node / p.sx) % p.sy, z = node / (p.sx * p.sy);
+    const float px = x * 1.0f, py = y * 1.0f, pz = z * 1.0f;
+    const int ntiles = (t_count + kTriTile - 1) / kTriTile;
+
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+
+    auto issue = [&](int tile) {
+        const int b = tile & 1;
+        const int cnt = min(kTriTile, t_count - tile * kTriTile);
+        const uint32_t bytes = (uint32_t)((cnt * kTriFloats * 4 + 15) & ~15);
+        proxy_fence_shared();
+        mbar_expect_tx(&s_bar[b], bytes);
+        bulk_copy_g2s(s_tri[b], tris + (size_t)tile * kTriTile * kTriFloats, bytes, &s_bar[b]);
+    };
+
+    if (threadIdx.x == 0 && ntiles > 0) issue(0);
+    float wsum = 0.0f, dmin2 = 1e30f;
+    bool aborted = false;
+    int tile = 0;
+    for (; tile < ntiles; ++tile) {
+        const int b = tile & 1;
+        if (threadIdx.x == 0 && tile + 1 < ntiles) issue(tile + 1);
+        const bool ok = mbar_wait_bounded(&s_bar[b], (uint32_t)((tile >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            aborted = true;
+            break;
+        }
+        const int cnt = min(kTriTile, t_count - tile * kTriTile);
+        const float* st = s_tri[b];
+        for (int k = 0; k < cnt; ++k) {
+            const float* tr = st + k * kTriFloats;
+            wsum += solid_angle(tr[0] - px, tr[1] - py, tr[2] - pz, tr[3] - px, tr[4] - py, tr[5] - pz,
+                                tr[6] - px, tr[7] - py, tr[8] - pz);
+            const float d2 = tri_dist2(px, py, pz, tr);
+            if (d2 < dmin2) dmin2 = d2;
+        }
+        __syncthreads();
+    }
+    if (aborted) {
+        // Drain: the copy of `tile` and possibly `tile + 1` may still land.
+        if (threadIdx.x == 0) {
+            atomicOr(status, kStatusTimeout);
+            mbar_wait_bounded(&s_bar[tile & 1], (uint32_t)((tile >> 1) & 1));
+            if (tile + 1 < ntiles) mbar_wait_bounded(&s_bar[(tile + 1) & 1], (uint32_t)(((tile + 1) >> 1) & 1));
+        }
+        __syncthreads();
+        return;
+    }
+    if (node < p.g) {
+        const float wn = wsum / (4.0f * 3.1415f);
+        sdf[node] = (wn > 0.5f ? -1.0f : 1.0f) * sqrtf(dmin2);
+    }
+}
+
+}  // namespace
+
+int launch_sdf_build(const SimParams& p, const float* tris, int t, float* sdf, uint32_t* status, cudaStream_t st) {
+    if (p.g <= 0) return 0;
+    sdf_build_kernel<<<(p.g + kSdfThreads - 1) / kSdfThreads, kSdfThreads, 0, st>>>(p, tris, t, sdf, status);
+    return 1;
+}
+
+}  // namespace mpm

@@ -1,0 +1,322 @@
+"""Python mirror of the B200 MLS-MPM engine's C ABI (include/mpm_b200.h).
+
+The class `Engine` mirrors the reference's C++ `Engine` (engine.h:14-43):
+`init(n, buffer)`, `step()`, `init_sdf(triangles)`, `get_buffer()`,
+`get_positions()`, `get_grid()`, `get_number()`, and `sort_particles()`;
+`parse_config_file` mirrors GameConfigData (game_configdata.cpp:22-90).
+Every call goes through libmpm_b200.so.  There is no CPU fallback: importing
+this module without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libmpm_b200.so")
+
+PARTICLE_PLANES = 26
+GRID_PLANES = 4
+POS_X, VEL_X, C00, F00, VOL, MASS = 0, 3, 6, 15, 24, 25
+STAGE_SORT, STAGE_P2G, STAGE_GRID, STAGE_G2P = 1, 2, 3, 4
+HEALTH_NONFINITE, HEALTH_OUT_OF_GRID = 1, 2
+
+STATUS = {
+    0: "MPM_OK", 1: "MPM_ERR_INVALID_ARGUMENT", 2: "MPM_ERR_BAD_CONFIG", 3: "MPM_ERR_IO",
+    4: "MPM_ERR_CUDA", 5: "MPM_ERR_OUT_OF_MEMORY", 6: "MPM_ERR_NOT_INITIALIZED",
+    7: "MPM_ERR_NONFINITE_STATE", 8: "MPM_ERR_OUT_OF_GRID", 9: "MPM_ERR_TIMEOUT",
+    10: "MPM_ERR_UNSUPPORTED", 11: "MPM_ERR_NO_DEVICE",
+}
+
+
+class MpmError(RuntimeError):
+    """A non-zero mpm_status, with the library's message."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.name = STATUS.get(status, f"status {status}")
+        super().__init__(f"{self.name}: {message}")
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("size_x", ctypes.c_int32), ("size_y", ctypes.c_int32), ("size_z", ctypes.c_int32),
+        ("padding", ctypes.c_int32), ("gravity", ctypes.c_float), ("dt", ctypes.c_float),
+        ("gamma", ctypes.c_float), ("compression", ctypes.c_float), ("resolution", ctypes.c_float),
+        ("substeps", ctypes.c_int32), ("sdf_resolution", ctypes.c_int32),
+    ]
+
+
+class _SceneEntry(ctypes.Structure):
+    _fields_ = [("model_path", ctypes.c_char * 512), ("scale", ctypes.c_float),
+                ("x", ctypes.c_float), ("y", ctypes.c_float), ("z", ctypes.c_float)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("substeps", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
+                ("sort_passes", ctypes.c_int64), ("health", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+@dataclass
+class SceneEntry:
+    """A WATER= or OBJECT= line: `path;scale;x;y;z` (struct ConfigObject)."""
+    model_path: str
+    scale: float
+    x: float
+    y: float
+    z: float
+
+
+@dataclass
+class Config:
+    """The config.txt keys of SimConfig (common.cuh:65-79)."""
+    size_x: int = 128
+    size_y: int = 128
+    size_z: int = 128
+    padding: int = 2
+    gravity: float = 9.81
+    dt: float = 0.01
+    gamma: float = -2.0
+    compression: float = 200.0
+    resolution: float = 1.0
+    substeps: int = 10
+    sdf_resolution: int = 256
+    waters: list = field(default_factory=list)
+    objects: list = field(default_factory=list)
+
+    @property
+    def grid_number(self) -> int:
+        return self.size_x * self.size_y * self.size_z
+
+    def to_c(self) -> _Config:
+        return _Config(self.size_x, self.size_y, self.size_z, self.padding, self.gravity, self.dt,
+                       self.gamma, self.compression, self.resolution, self.substeps, self.sdf_resolution)
+
+    def to_text(self) -> str:
+        """config.txt text with float values that read back bit-identically."""
+        f = lambda v: repr(float(np.float32(v)))
+        lines = [f"SIZE_X={self.size_x}", f"SIZE_Y={self.size_y}", f"SIZE_Z={self.size_z}",
+                 f"PADDING={self.padding}", f"GRAVITY={f(self.gravity)}", f"DT={f(self.dt)}",
+                 f"GAMMA={f(self.gamma)}", f"COMPRESSION={f(self.compression)}",
+                 f"RESOLUTION={f(self.resolution)}", f"SUBSTEPS={self.substeps}",
+                 f"SDF_RESOLUTION={self.sdf_resolution}"]
+        for tag, entries in (("WATER", self.waters), ("OBJECT", self.objects)):
+            for e in entries:
+                lines.append(f"{tag}={e.model_path};{f(e.scale)};{f(e.x)};{f(e.y)};{f(e.z)}")
+        return "\n".join(lines) + "\n"
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C water-sim-cuda_b200` "
+                           "(or __graft_entry__.build())")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, I32, I64, U32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32
+    sigs = {
+        "mpm_abi_version": (I32, []),
+        "mpm_status_string": (ctypes.c_char_p, [I32]),
+        "mpm_config_parse_file": (I32, [ctypes.c_char_p, P, P, I32, P, P, I32, P, ctypes.c_char_p, I32]),
+        "mpm_config_parse_string": (I32, [ctypes.c_char_p, P, P, I32, P, P, I32, P, ctypes.c_char_p, I32]),
+        "mpm_create": (I32, [P, I32, P]),
+        "mpm_destroy": (None, [P]),
+        "mpm_init_particles": (I32, [P, I64, P]),
+        "mpm_init_sdf": (I32, [P, P, I64]),
+        "mpm_step": (I32, [P, I32]),
+        "mpm_step_async": (I32, [P, I32]),
+        "mpm_synchronize": (I32, [P]),
+        "mpm_substep_partial": (I32, [P, I32]),
+        "mpm_set_checks": (I32, [P, U32]),
+        "mpm_num_particles": (I64, [P]),
+        "mpm_get_state": (I32, [P, P]),
+        "mpm_set_state": (I32, [P, I64, P]),
+        "mpm_positions_device": (P, [P]),
+        "mpm_get_positions": (I32, [P, P]),
+        "mpm_get_grid": (I32, [P, P]),
+        "mpm_get_sdf": (I32, [P, P]),
+        "mpm_get_sort": (I32, [P, P, P]),
+        "mpm_get_stats": (I32, [P, P, I32]),
+        "mpm_set_stage_timing": (I32, [P, I32]),
+        "mpm_get_stage_times": (I32, [P, P, P]),
+        "mpm_stream": (P, [P]),
+        "mpm_last_error": (ctypes.c_char_p, [P]),
+        "mpm_global_last_error": (ctypes.c_char_p, []),
+        "mpm_sort_particles_device": (I32, [P, P, P, I64, P, P, P]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _parse(fn, arg, max_entries=64) -> Config:
+    c = _Config()
+    waters = (_SceneEntry * max_entries)()
+    objects = (_SceneEntry * max_entries)()
+    nw, no = ctypes.c_int32(0), ctypes.c_int32(0)
+    err = ctypes.create_string_buffer(1024)
+    st = fn(arg, ctypes.byref(c), waters, max_entries, ctypes.byref(nw), objects, max_entries,
+            ctypes.byref(no), err, len(err))
+    if st != 0:
+        raise MpmError(st, err.value.decode(errors="replace"))
+    cfg = Config(c.size_x, c.size_y, c.size_z, c.padding, c.gravity, c.dt, c.gamma, c.compression,
+                 c.resolution, c.substeps, c.sdf_resolution)
+    conv = lambda e: SceneEntry(e.model_path.decode(errors="replace"), e.scale, e.x, e.y, e.z)
+    cfg.waters = [conv(waters[i]) for i in range(min(nw.value, max_entries))]
+    cfg.objects = [conv(objects[i]) for i in range(min(no.value, max_entries))]
+    return cfg
+
+
+def parse_config_file(path: str) -> Config:
+    """GameConfigData::setConfigDataFromFile + the key reads of initDeviceParams."""
+    return _parse(lib.mpm_config_parse_file, path.encode())
+
+
+def parse_config_string(text: str) -> Config:
+    return _parse(lib.mpm_config_parse_string, text.encode())
+
+
+class Engine:
+    """One simulation on one GPU (the reference's `Engine`, engine.h:14-43)."""
+
+    def __init__(self, cfg: Config, device: int = 0):
+        self.cfg = cfg
+        handle = ctypes.c_void_p()
+        c = cfg.to_c()
+        st = lib.mpm_create(ctypes.byref(c), device, ctypes.byref(handle))
+        if st != 0:
+            raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
+        self._h = handle
+        self.n = 0
+
+    def _check(self, st: int):
+        if st != 0:
+            raise MpmError(st, lib.mpm_last_error(self._h).decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.mpm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- Engine::init / initSDF -------------------------------------------------
+    def init(self, state26: np.ndarray):
+        """Engine::init(n, buffer): state26 is (26, n) or flat 26*n float32 (copied)."""
+        a = np.ascontiguousarray(state26, dtype=np.float32).reshape(-1)
+        if a.size % PARTICLE_PLANES:
+            raise ValueError("state size is not a multiple of 26")
+        n = a.size // PARTICLE_PLANES
+        self._check(lib.mpm_init_particles(self._h, n, _ptr(a)))
+        self.n = n
+
+    def init_sdf(self, triangles: np.ndarray):
+        """Engine::initSDF(triangles): (t, 9) or (t, 3, 3) float32 in grid coordinates."""
+        t = np.ascontiguousarray(triangles, dtype=np.float32).reshape(-1)
+        if t.size % 9:
+            raise ValueError("triangle array size is not a multiple of 9")
+        self._check(lib.mpm_init_sdf(self._h, t.size // 9, _ptr(t) if t.size else None))
+
+    def set_state(self, state26: np.ndarray):
+        a = np.ascontiguousarray(state26, dtype=np.float32).reshape(-1)
+        self._check(lib.mpm_set_state(self._h, a.size // PARTICLE_PLANES, _ptr(a)))
+
+    # -- stepping -----------------------------------------------------------------
+    def step(self, nsub: int = 1):
+        """nsub calls of Engine::step() (one substep each), synchronous."""
+        self._check(lib.mpm_step(self._h, int(nsub)))
+
+    def step_async(self, nsub: int = 1):
+        self._check(lib.mpm_step_async(self._h, int(nsub)))
+
+    def synchronize(self):
+        self._check(lib.mpm_synchronize(self._h))
+
+    def substep_partial(self, upto: int):
+        self._check(lib.mpm_substep_partial(self._h, int(upto)))
+
+    def set_checks(self, flags: int):
+        self._check(lib.mpm_set_checks(self._h, int(flags)))
+
+    # -- readback -----------------------------------------------------------------
+    def get_number(self) -> int:
+        return int(lib.mpm_num_particles(self._h))
+
+    def get_buffer(self) -> np.ndarray:
+        """Engine::getBuffer() copied to the host: (26, n) float32, original order."""
+        out = np.empty((PARTICLE_PLANES, self.n), np.float32)
+        self._check(lib.mpm_get_state(self._h, _ptr(out)))
+        return out
+
+    def get_positions(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Engine::getPositions() copied to the host: (n, 3) float32."""
+        if out is None:
+            out = np.empty((self.n, 3), np.float32)
+        self._check(lib.mpm_get_positions(self._h, _ptr(out)))
+        return out
+
+    def positions_device_ptr(self) -> int:
+        return int(lib.mpm_positions_device(self._h) or 0)
+
+    def get_grid(self) -> np.ndarray:
+        """Engine::getGrid() planes copied to the host: (4, G) float32."""
+        out = np.empty((GRID_PLANES, self.cfg.grid_number), np.float32)
+        self._check(lib.mpm_get_grid(self._h, _ptr(out)))
+        return out
+
+    def get_sdf(self) -> np.ndarray:
+        out = np.empty(self.cfg.grid_number, np.float32)
+        self._check(lib.mpm_get_sdf(self._h, _ptr(out)))
+        return out
+
+    def get_sort(self):
+        """(keys, perm) of the last substep's sortParticles (engine.cu:92-102)."""
+        keys = np.empty(self.n, np.int32)
+        perm = np.empty(self.n, np.int32)
+        self._check(lib.mpm_get_sort(self._h, _ptr(keys), _ptr(perm)))
+        return keys, perm
+
+    def stats(self, reset_health: bool = False) -> dict:
+        s = _Stats()
+        self._check(lib.mpm_get_stats(self._h, ctypes.byref(s), int(reset_health)))
+        return {"substeps": s.substeps, "kernel_launches": s.kernel_launches,
+                "sort_passes": s.sort_passes, "health": s.health}
+
+    def stream(self) -> int:
+        return int(lib.mpm_stream(self._h) or 0)
+
+    def set_stage_timing(self, max_substeps: int):
+        """Record CUDA events between the stages of the next max_substeps substeps."""
+        self._check(lib.mpm_set_stage_timing(self._h, int(max_substeps)))
+
+    def stage_times(self):
+        """({'sort','p2g','grid','g2p'}: summed ms, substeps recorded); clears the record."""
+        ms = (ctypes.c_double * 4)()
+        cnt = ctypes.c_int32(0)
+        self._check(lib.mpm_get_stage_times(self._h, ms, ctypes.byref(cnt)))
+        return dict(zip(("sort", "p2g", "grid", "g2p"), list(ms))), cnt.value
+
+
+def sort_particles_device(px: int, py: int, pz: int, n: int, keys: int, perm: int, stream: int = 0):
+    """Engine::sortParticles on caller-owned device buffers (raw device pointers)."""
+    st = lib.mpm_sort_particles_device(px, py, pz, n, keys, perm, stream or None)
+    if st != 0:
+        raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
