@@ -480,17 +480,20 @@ extern "C" mpm_status mpm_init_sdf(mpm_engine* e, const float* tris, int64_t t) 
         CK(e, cudaStreamSynchronize(e->stream));
         return MPM_OK;
     }
+    // cudaMalloc: 256-byte aligned, as the kernel's 16-byte bulk copies need;
+    // 16 spare bytes cover the last tile's copy rounded up to 16 bytes.
     const size_t bytes = (size_t)t * 9 * sizeof(float);
     float* d_tris = nullptr;
-    CK(e, cudaMallocAsync(&d_tris, align_up(bytes, 16) + 16, e->stream));
-    cudaError_t err = cudaMemcpyAsync(d_tris, tris, bytes, cudaMemcpyHostToDevice, e->stream);
+    CK(e, cudaMalloc(&d_tris, align_up(bytes, 16) + 16));
+    cudaError_t err = cudaMemsetAsync(d_tris, 0, align_up(bytes, 16) + 16, e->stream);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(d_tris, tris, bytes, cudaMemcpyHostToDevice, e->stream);
     if (err == cudaSuccess) {
         e->kernel_launches += mpm::launch_sdf_build(e->prm, d_tris, (int)t, e->sdf, e->d_flags + 1, e->stream);
         err = cudaGetLastError();
     }
-    cudaFreeAsync(d_tris, e->stream);
-    if (err != cudaSuccess) return cuda_fail(e, err, "sdf build");
-    return sync_and_collect(e);
+    const mpm_status s2 = err != cudaSuccess ? cuda_fail(e, err, "sdf build") : sync_and_collect(e);
+    cudaFree(d_tris);
+    return s2;
 }
 
 extern "C" mpm_status mpm_step_async(mpm_engine* e, int32_t nsub) {
