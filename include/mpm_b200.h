@@ -202,10 +202,13 @@ mpm_status mpm_step_async(mpm_engine* engine, int32_t nsub);
 /* Waits for the engine's stream and reports any asynchronous error. */
 mpm_status mpm_synchronize(mpm_engine* engine);
 
-/* Runs the stages of one substep up to `upto` (MPM_STAGE_*) and stops, so
- * that a test can read the grid after P2G or after the grid update.  The
- * particle state only changes for MPM_STAGE_G2P.  The next mpm_step starts
- * a fresh substep.  Synchronous.  No counterpart in the reference. */
+/* Runs one substep stage by stage, so that a test can read the grid after
+ * P2G or after the grid update: continues the substep in progress with the
+ * stages after the last one run, up to `upto` (MPM_STAGE_*), or starts a new
+ * substep when none is in progress or `upto` is not past the last stage run.
+ * MPM_STAGE_G2P completes the substep exactly as mpm_step(engine, 1) would.
+ * Particles only change at MPM_STAGE_G2P; mpm_step discards an unfinished
+ * substep.  Synchronous.  No counterpart in the reference. */
 mpm_status mpm_substep_partial(mpm_engine* engine, int32_t upto);
 
 /* Health checks: when `flags` holds MPM_HEALTH_* bits, mpm_step returns

@@ -60,3 +60,26 @@ def test_null_engine_calls(mpm):
     assert lib.mpm_last_error(None) == b""
     lib.mpm_destroy(None)
 
+
+
+def test_wrapper_marshalling_against_null_engine(mpm):
+    """Every Engine method marshals its arguments (ctypes) and reaches the
+    library, which rejects the NULL engine with MPM_ERR_INVALID_ARGUMENT."""
+    import numpy as np
+    e = mpm.Engine.__new__(mpm.Engine)
+    e._h = None
+    e.cfg = mpm.Config(size_x=8, size_y=8, size_z=8)
+    e.n = 4
+    st = np.zeros((26, 4), np.float32)
+    calls = [lambda: e.init(st), lambda: e.init_sdf(np.zeros((2, 9), np.float32)), lambda: e.set_state(st),
+             lambda: e.step(1), lambda: e.step_async(1), e.synchronize, lambda: e.substep_partial(2),
+             lambda: e.set_checks(1), e.get_buffer, e.get_positions, e.get_grid, e.get_sdf, e.get_sort, e.stats,
+             lambda: e.set_stage_timing(2), e.stage_times]
+    for call in calls:
+        with pytest.raises(mpm.MpmError) as ei:
+            call()
+        assert ei.value.name == "MPM_ERR_INVALID_ARGUMENT"
+    assert e.get_number() == 0 and e.positions_device_ptr() == 0 and e.stream() == 0
+    with pytest.raises(mpm.MpmError):
+        mpm.sort_particles_device(0, 0, 0, 5, 0, 0, 0)
+    assert mpm.lib.mpm_sort_particles_device(None, None, None, 0, None, None, None) == 0

@@ -82,8 +82,9 @@ def test_stage_g2p(gpu_ok, mpm, oracle64):
         eng.substep_partial(mpm.STAGE_GRID)
         vgrid = eng.get_grid()
         sdf = eng.get_sdf()
-        eng.step(1)  # a full substep redoes sort/P2G/update identically up to atomic order
+        eng.substep_partial(mpm.STAGE_G2P)  # completes this substep on the same grid
         got = eng.get_buffer()
+        assert eng.stats()["substeps"] == 1
     st0 = oracle64.init_particles(cfg, st)
     want = oracle64.g2p(cfg, st0, None, vgrid.astype(np.float64), sdf.astype(np.float64))
     assert_state_close(got, want, st0, rtol=RTOL)

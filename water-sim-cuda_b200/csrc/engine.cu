@@ -71,6 +71,7 @@ struct mpm_engine {
 
     int parity = 0;
     int sort_src = kNoSort;
+    int partial_stage = 0;  // last MPM_STAGE_* run by mpm_substep_partial, 0 = none
     bool accum_dirty = false;
     GridView grid_view = GridView::kVelocity;
 
@@ -166,23 +167,30 @@ mpm_status alloc_particles(mpm_engine* e, int n) {
     return MPM_OK;
 }
 
-// Enqueues the stages of one substep from parity `par`, up to `upto`.  With
-// `marks`, records marks[0..4] before the sort and after each stage.
-int enqueue_substep(mpm_engine* e, int par, int upto, const cudaEvent_t* marks = nullptr) {
+// Enqueues stages `from`..`upto` (MPM_STAGE_*) of one substep from parity
+// `par`.  With `marks` (only while capturing a graph), records marks[0..4]
+// as event-record nodes before the sort and after each stage.
+int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_t* marks = nullptr) {
     const SimParams& p = e->prm;
     cudaStream_t st = e->stream;
-    if (marks) cudaEventRecord(marks[0], st);
-    int launches = mpm::launch_radix_sort(e->keys[par], p.n, e->sort, e->sigma[1 - par], e->rank[1 - par],
-                                          e->rank[par], e->gidx, st);
-    if (marks) cudaEventRecord(marks[1], st);
-    if (upto >= MPM_STAGE_P2G) launches += mpm::launch_p2g(p, e->P[par], e->gidx, e->accum, st);
-    if (marks) cudaEventRecord(marks[2], st);
-    if (upto >= MPM_STAGE_GRID) launches += mpm::launch_grid_update(p, e->accum, e->vgrid, e->sdf, st);
-    if (marks) cudaEventRecord(marks[3], st);
-    if (upto >= MPM_STAGE_G2P)
+    auto mark = [&](int k) {
+        if (marks) cudaEventRecordWithFlags(marks[k], st, cudaEventRecordExternal);
+    };
+    int launches = 0;
+    mark(0);
+    if (from <= MPM_STAGE_SORT && upto >= MPM_STAGE_SORT)
+        launches += mpm::launch_radix_sort(e->keys[par], p.n, e->sort, e->sigma[1 - par], e->rank[1 - par],
+                                           e->rank[par], e->gidx, st);
+    mark(1);
+    if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G) launches += mpm::launch_p2g(p, e->P[par], e->gidx, e->accum, st);
+    mark(2);
+    if (from <= MPM_STAGE_GRID && upto >= MPM_STAGE_GRID)
+        launches += mpm::launch_grid_update(p, e->accum, e->vgrid, e->sdf, st);
+    mark(3);
+    if (from <= MPM_STAGE_G2P && upto >= MPM_STAGE_G2P)
         launches += mpm::launch_g2p(p, e->P[par], e->P[1 - par], e->gidx, e->sigma[1 - par], e->vgrid, e->sdf,
                                     e->keys[1 - par], e->d_flags, st);
-    if (marks) cudaEventRecord(marks[4], st);
+    mark(4);
     return launches;
 }
 
@@ -195,7 +203,7 @@ mpm_status capture_graphs(mpm_engine* e) {
         e->graph_src[par] = nullptr;
         cudaGraph_t g = nullptr;
         CK(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-        const int launches = enqueue_substep(e, par, MPM_STAGE_G2P, timed ? e->tscratch : nullptr);
+        const int launches = enqueue_substep(e, par, MPM_STAGE_SORT, MPM_STAGE_G2P, timed ? e->tscratch : nullptr);
         const cudaError_t launch_err = cudaGetLastError();
         const cudaError_t end_err = cudaStreamEndCapture(e->stream, &g);
         if (launch_err != cudaSuccess) {
@@ -205,6 +213,7 @@ mpm_status capture_graphs(mpm_engine* e) {
         CK(e, end_err);
         e->graph_src[par] = g;
         if (timed) {
+            for (int k = 0; k < mpm_engine::kTimingMarks; ++k) e->tnode[par][k] = nullptr;
             // Find the event-record nodes by the scratch event each records.
             size_t count = 0;
             CK(e, cudaGraphGetNodes(g, nullptr, &count));
@@ -219,6 +228,8 @@ mpm_status capture_graphs(mpm_engine* e) {
                 for (int k = 0; k < mpm_engine::kTimingMarks; ++k)
                     if (ev == e->tscratch[k]) e->tnode[par][k] = nd;
             }
+            for (int k = 0; k < mpm_engine::kTimingMarks; ++k)
+                if (!e->tnode[par][k]) return record(e, MPM_ERR_CUDA, "stage-timing event node missing from the graph");
         }
         CK(e, cudaGraphInstantiate(&e->graph[par], g, 0));
         e->graph_kernels[par] = launches;
@@ -280,6 +291,7 @@ mpm_status load_state(mpm_engine* e, const float* soa26_host, bool init_rules) {
     }
     e->parity = 0;
     e->sort_src = kNoSort;
+    e->partial_stage = 0;
     CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
     CK(e, cudaMemsetAsync(e->vgrid, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
     CK(e, cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(uint32_t), e->stream));
@@ -304,6 +316,7 @@ mpm_status enter(mpm_engine* e) {
 mpm_status run_steps(mpm_engine* e, int32_t nsub) {
     if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
     if (nsub < 0) return record(e, MPM_ERR_INVALID_ARGUMENT, "nsub < 0");
+    e->partial_stage = 0;  // a partial substep in progress is discarded (it changed no particle)
     if (e->accum_dirty) {
         CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
         e->accum_dirty = false;
@@ -522,20 +535,37 @@ extern "C" mpm_status mpm_substep_partial(mpm_engine* e, int32_t upto) {
     if (s != MPM_OK) return s;
     if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
     if (upto < MPM_STAGE_SORT || upto > MPM_STAGE_G2P) return record(e, MPM_ERR_INVALID_ARGUMENT, "bad stage");
-    if (upto == MPM_STAGE_G2P) return mpm_step(e, 1);
-    if (e->accum_dirty) CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
-    e->kernel_launches += enqueue_substep(e, e->parity, upto);
+    // Continue the substep in progress, or start a new one.
+    int from = e->partial_stage + 1;
+    if (upto <= e->partial_stage) from = MPM_STAGE_SORT;
+    if (from == MPM_STAGE_SORT && e->accum_dirty) {
+        CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
+        e->accum_dirty = false;
+    }
+    e->kernel_launches += enqueue_substep(e, e->parity, from, upto);
     CK(e, cudaGetLastError());
-    e->sort_passes += e->n > 0 ? 4 : 0;
-    e->sort_src = e->parity;
+    if (from == MPM_STAGE_SORT) {
+        e->sort_passes += e->n > 0 ? 4 : 0;
+        e->sort_src = e->parity;
+    }
+    e->partial_stage = upto;
     if (upto == MPM_STAGE_P2G) {
         e->accum_dirty = true;
         e->grid_view = GridView::kAccum;
-    } else if (upto == MPM_STAGE_GRID) {
+    } else if (upto >= MPM_STAGE_GRID && from <= MPM_STAGE_GRID) {
         e->accum_dirty = false;
         e->grid_view = GridView::kVelocity;
     }
-    return sync_and_collect(e);
+    if (upto == MPM_STAGE_G2P) {
+        e->partial_stage = 0;
+        e->parity ^= 1;
+        ++e->substeps;
+        e->kernel_launches +=
+            mpm::launch_positions_export(e->prm, e->P[e->parity], e->sigma[e->parity], e->pos_out, e->stream);
+        CK(e, cudaGetLastError());
+    }
+    if ((s = sync_and_collect(e)) != MPM_OK) return s;
+    return upto == MPM_STAGE_G2P ? check_health(e) : MPM_OK;
 }
 
 extern "C" mpm_status mpm_set_checks(mpm_engine* e, uint32_t flags) {

@@ -233,7 +233,7 @@ class Engine:
         t = np.ascontiguousarray(triangles, dtype=np.float32).reshape(-1)
         if t.size % 9:
             raise ValueError("triangle array size is not a multiple of 9")
-        self._check(lib.mpm_init_sdf(self._h, t.size // 9, _ptr(t) if t.size else None))
+        self._check(lib.mpm_init_sdf(self._h, _ptr(t) if t.size else None, t.size // 9))
 
     def set_state(self, state26: np.ndarray):
         a = np.ascontiguousarray(state26, dtype=np.float32).reshape(-1)
