@@ -300,6 +300,35 @@ const char* mpm_global_last_error(void);
 mpm_status mpm_sort_particles_device(const float* d_pos_x, const float* d_pos_y, const float* d_pos_z,
                                      int64_t n, int32_t* d_keys, int32_t* d_perm, void* stream);
 
+/* Largest n mpm_sort_particles_device_static accepts. */
+#define MPM_SORT_STATIC_MAX_PARTICLES (1 << 20)
+
+/* mpm_sort_particles_device for callers that cannot allocate device memory:
+ * the same keys and permutation, bit for bit, with no cudaMalloc, cudaFree or
+ * other allocating call.  It has no counterpart in the reference, which
+ * allocates its key buffer on every sort (engine.cu:95,101).
+ * Who needs it: hosts whose device memory belongs to another allocator (a
+ * game engine's or framework's pool that reserved it up front), real-time
+ * frame loops that must not block on an allocator or on the device-wide
+ * synchronisation of cudaFree, and stacks without stream-ordered
+ * allocation.
+ * How: the sort scratch is one fixed array in device memory, about
+ * 16 MiB + 1 MiB, that every device which loads this library holds until the
+ * process exits.  n above MPM_SORT_STATIC_MAX_PARTICLES is rejected with
+ * MPM_ERR_INVALID_ARGUMENT (mpm_global_last_error says why); use
+ * mpm_sort_particles_device for larger inputs.
+ * Runs on the calling thread's current device; `stream` must belong to it.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) and caches it, so make that first call before any
+ * stream capture begins.
+ * All calls on a device share the one array and nothing clears it between
+ * calls (no part of it needs to start at zero).  Calls that overlap on the
+ * GPU, on different streams or from different threads, race on it and give
+ * wrong results: order them on one stream or serialise them.
+ * Returns after enqueueing; synchronize the stream before reading. */
+mpm_status mpm_sort_particles_device_static(const float* d_pos_x, const float* d_pos_y, const float* d_pos_z,
+                                            int64_t n, int32_t* d_keys, int32_t* d_perm, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -660,6 +660,10 @@ extern "C" const char* mpm_last_error(const mpm_engine* e) { return e ? e->last_
 
 extern "C" const char* mpm_global_last_error(void) { return g_global_error.c_str(); }
 
+// Lets the free operators of other translation units report through
+// mpm_global_last_error.
+void mpm::set_global_error(const std::string& msg) { g_global_error = msg; }
+
 extern "C" mpm_status mpm_sort_particles_device(const float* px, const float* py, const float* pz, int64_t n,
                                                 int32_t* d_keys, int32_t* d_perm, void* stream) {
     g_global_error.clear();

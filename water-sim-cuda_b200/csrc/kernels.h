@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "device_math.cuh"
 
 namespace mpm {
@@ -70,5 +72,8 @@ int launch_fill(float* dst, long long count, float value, cudaStream_t st);
 
 // Device status bits written by kernels with bounded waits.
 enum : uint32_t { kStatusTimeout = 1u << 0 };
+
+// Sets the thread's mpm_global_last_error text (engine.cu).
+void set_global_error(const std::string& msg);
 
 }  // namespace mpm

@@ -23,6 +23,7 @@ GRID_PLANES = 4
 POS_X, VEL_X, C00, F00, VOL, MASS = 0, 3, 6, 15, 24, 25
 STAGE_SORT, STAGE_P2G, STAGE_GRID, STAGE_G2P = 1, 2, 3, 4
 HEALTH_NONFINITE, HEALTH_OUT_OF_GRID = 1, 2
+SORT_STATIC_MAX_PARTICLES = 1 << 20  # MPM_SORT_STATIC_MAX_PARTICLES
 
 STATUS = {
     0: "MPM_OK", 1: "MPM_ERR_INVALID_ARGUMENT", 2: "MPM_ERR_BAD_CONFIG", 3: "MPM_ERR_IO",
@@ -145,6 +146,7 @@ def _load() -> ctypes.CDLL:
         "mpm_last_error": (ctypes.c_char_p, [P]),
         "mpm_global_last_error": (ctypes.c_char_p, []),
         "mpm_sort_particles_device": (I32, [P, P, P, I64, P, P, P]),
+        "mpm_sort_particles_device_static": (I32, [P, P, P, I64, P, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -318,5 +320,14 @@ class Engine:
 def sort_particles_device(px: int, py: int, pz: int, n: int, keys: int, perm: int, stream: int = 0):
     """Engine::sortParticles on caller-owned device buffers (raw device pointers)."""
     st = lib.mpm_sort_particles_device(px, py, pz, n, keys, perm, stream or None)
+    if st != 0:
+        raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
+
+
+def sort_particles_device_static(px: int, py: int, pz: int, n: int, keys: int, perm: int, stream: int = 0):
+    """sort_particles_device without any device allocation: the scratch is a
+    fixed array inside the library (n <= SORT_STATIC_MAX_PARTICLES).  For hosts
+    that cannot allocate device memory; calls that overlap on the GPU race."""
+    st = lib.mpm_sort_particles_device_static(px, py, pz, n, keys, perm, stream or None)
     if st != 0:
         raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
