@@ -11,17 +11,27 @@
 
 namespace mpm {
 
-// Particle planes kept on the device.  VOL and MASS are not stored per
-// particle: Engine::init's initFMatrices sets every particle to
-// VOL = RESOLUTION^3 and MASS = 1 (kernels.cu:349-358) and no kernel writes
-// them again, so they are two scalars in SimParams.
-enum StatePlane : int {
-    kPX = 0, kPY = 1, kPZ = 2,
-    kVX = 3, kVY = 4, kVZ = 5,
-    kC0 = 6,   // C00..C22 row-major, planes 6..14
-    kF0 = 15,  // F00..F22 row-major, planes 15..23
-    kStatePlanes = 24
+// Particle state on the device, particle-major: 24 floats (96 bytes, six
+// 16-byte vectors) per particle, position and F first so that G2P reads its
+// inputs as three vectors.  VOL and MASS are not stored per particle:
+// Engine::init's initFMatrices sets every particle to VOL = RESOLUTION^3 and
+// MASS = 1 (kernels.cu:349-358) and no kernel writes them again, so they are
+// two scalars in SimParams.
+enum ParticleField : int {
+    kAPos = 0,   // x, y, z
+    kAF = 3,     // F00..F22 row-major
+    kAVel = 12,  // vx, vy, vz
+    kAC = 15,    // C00..C22 row-major
+    kAFloats = 24
 };
+
+// Particles are binned by their stencil base cell b = stencil_base(pos)
+// (the cell whose 3x3x3 node stencil they scatter to).  A particle reaches
+// the grid only if b lies in [-2, SIZE-1] on every axis; bins are blocks of
+// kBinX x kBinY x kBinZ base cells over that shifted range (u = b + 2).  Bin
+// `nb` collects the particles that reach no node.
+constexpr int kBinX = 8, kBinY = 4, kBinZ = 4;
+constexpr int kBinCells = kBinX * kBinY * kBinZ;  // 128
 
 struct SimParams {
     int sx, sy, sz;       // SIZE_X/Y/Z
@@ -30,7 +40,8 @@ struct SimParams {
     float pvol, pmass;    // per-particle volume and mass
     int n;                // particles
     int g;                // grid nodes sx*sy*sz
-    long long ld;         // plane stride of the particle state (floats)
+    int nbx, nby, nbz;    // bin blocks per axis: ceil((SIZE+2) / kBin*)
+    int nb;               // bin blocks; bin nb holds the particles that reach no node
 };
 
 // Node index z*SX*SY + y*SX + x (getGridIdx, common.cuh:131-134).
@@ -84,6 +95,22 @@ __device__ __forceinline__ int32_t morton_key(float px, float py, float pz) {
     const uint32_t y = __float2uint_rz(fmaxf(0.0f, py));
     const uint32_t z = __float2uint_rz(fmaxf(0.0f, pz));
     return (int32_t)((spread_bits3(z) << 2) | (spread_bits3(y) << 1) | spread_bits3(x));
+}
+
+// Cell of a particle at (x, y, z): bin * kBinCells + the index of its stencil
+// base cell inside the bin (x fastest), and its bin.  A particle none of
+// whose 27 stencil nodes is in the grid (isInBounds, common.cuh:212-218)
+// goes to the single cell of the overflow bin nb.
+__device__ __forceinline__ int cell_of(const SimParams& p, float x, float y, float z, int* bin) {
+    const int bx = stencil_base(x), by = stencil_base(y), bz = stencil_base(z);
+    if (bx < -2 || by < -2 || bz < -2 || bx > p.sx - 1 || by > p.sy - 1 || bz > p.sz - 1) {
+        *bin = p.nb;
+        return p.nb * kBinCells;
+    }
+    const int ux = bx + 2, uy = by + 2, uz = bz + 2;
+    const int b = ((uz / kBinZ) * p.nby + uy / kBinY) * p.nbx + ux / kBinX;
+    *bin = b;
+    return b * kBinCells + ((uz % kBinZ) * kBinY + uy % kBinY) * kBinX + ux % kBinX;
 }
 
 __device__ __forceinline__ float det3(const float* A) {

@@ -5,17 +5,23 @@
 // state: one device, one stream, and a CUDA graph per substep parity.
 //
 // Particle order.  The reference never moves particle data: every substep it
-// sorts (key, 0..n-1) and gathers through the permutation.  Here the state
-// lives in the order of the last sort.  A substep from parity p:
-//   sort keys[p] (keys in ORIGINAL order, values 0..n-1, exactly the
-//       reference's thrust::sequence + sort_by_key) -> sigma[1-p] (the
-//       reference's d_values), rank[1-p] = its inverse, and
-//       gidx[j] = rank[p][sigma[1-p][j]], the slot of the j-th particle in P[p];
-//   P2G reads P[p] through gidx (nearly the identity, so nearly streaming);
+// sorts (Morton key, 0..n-1) and gathers through the permutation, so that
+// the particles of a CTA are likely to share its shared-memory tile.  Here
+// the particles are ordered by stencil base cell, grouped in bins of
+// 8 x 4 x 4 cells, which is what the P2G kernel needs: all particles of a
+// cell scatter to the same 27 nodes.  A substep from parity p, state P[p]
+// filed into counter set p:
+//   bin order: bin and cell starts from set p, gidx[new slot] = old slot;
+//   P2G: one warp per listed bin, lane = cell, reading P[p] through gidx;
 //   grid update;
-//   G2P reads P[p] through gidx and writes P[1-p] at j, i.e. reorders the
-//       state for free, and writes the next key at keys[1-p][sigma[1-p][j]].
-// Readback scatters through sigma back to the original order.
+//   G2P reads P[p] through gidx and writes P[1-p] at the new slot, i.e. the
+//       state is regrouped for free, carries sigma (slot -> original index)
+//       along and files every particle into set 1-p for the next substep.
+// The reference's keys and sort permutation of a substep are a function of
+// the state the substep started from, which stays intact in P[p] until the
+// next substep; mpm_get_sort recomputes them from it with the bit-exact key
+// kernel and radix sort of sort.cu.  Readback scatters through sigma back to
+// the original order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -51,12 +57,13 @@ struct mpm_engine {
 
     bool initialized = false;
     int n = 0;
-    long long ld = 0;
-    float* P[2] = {nullptr, nullptr};
-    int32_t* keys[2] = {nullptr, nullptr};
-    int32_t* sigma[2] = {nullptr, nullptr};
-    int32_t* rank[2] = {nullptr, nullptr};
-    int32_t* gidx = nullptr;
+    float* P[2] = {nullptr, nullptr};        // particle-major state, 24 floats per particle
+    int32_t* sigma[2] = {nullptr, nullptr};  // slot -> original index
+    int32_t* gidx = nullptr;                 // new slot -> old slot of the current binning
+    int32_t* pcell = nullptr;                // cell of each slot of P[parity]
+    int32_t* prank = nullptr;                // rank within its cell
+    int32_t* ref_keys = nullptr;             // mpm_get_sort: keys in original order
+    int32_t* ref_perm = nullptr;             // mpm_get_sort: stable sort permutation
     void* sort_mem = nullptr;
     mpm::SortScratch sort;
     float* pos_out = nullptr;
@@ -64,6 +71,14 @@ struct mpm_engine {
     float4* accum = nullptr;
     float4* vgrid = nullptr;
     float* sdf = nullptr;
+    // Binning: two counter sets (cell counts, bin counts, bin lists) in one
+    // allocation, the bin and cell starts of the current order, and ctl =
+    // {list length of set 0, of set 1, P2G work counter}.
+    void* bins_mem = nullptr;
+    mpm::BinSet bins[2] = {};
+    int32_t* bstart = nullptr;
+    int32_t* cstart = nullptr;
+    uint32_t* ctl = nullptr;
     uint32_t* d_flags = nullptr;  // [0] health bits, [1] kernel status bits
 
     float* staging = nullptr;  // device staging for imports/exports
@@ -124,9 +139,7 @@ void free_dev(T*& p) {
 void free_particles(mpm_engine* e) {
     for (int k = 0; k < 2; ++k) {
         free_dev(e->P[k]);
-        free_dev(e->keys[k]);
         free_dev(e->sigma[k]);
-        free_dev(e->rank[k]);
         if (e->graph[k]) cudaGraphExecDestroy(e->graph[k]);
         if (e->graph_src[k]) cudaGraphDestroy(e->graph_src[k]);
         e->graph[k] = nullptr;
@@ -134,6 +147,10 @@ void free_particles(mpm_engine* e) {
         e->graph_kernels[k] = 0;
     }
     free_dev(e->gidx);
+    free_dev(e->pcell);
+    free_dev(e->prank);
+    free_dev(e->ref_keys);
+    free_dev(e->ref_perm);
     free_dev(e->sort_mem);
     free_dev(e->pos_out);
     e->initialized = false;
@@ -151,20 +168,40 @@ mpm_status ensure_staging(mpm_engine* e, size_t bytes) {
 mpm_status alloc_particles(mpm_engine* e, int n) {
     free_particles(e);
     e->n = n;
-    e->ld = (long long)align_up((size_t)std::max(n, 1), 64);
-    const size_t ibytes = (size_t)e->ld * sizeof(int32_t);
+    const size_t cap = (size_t)std::max(n, 1);
+    const size_t ibytes = cap * sizeof(int32_t);
     for (int k = 0; k < 2; ++k) {
-        CK(e, cudaMalloc(&e->P[k], (size_t)mpm::kStatePlanes * e->ld * sizeof(float)));
-        CK(e, cudaMalloc(&e->keys[k], ibytes));
+        CK(e, cudaMalloc(&e->P[k], cap * mpm::kAFloats * sizeof(float)));
         CK(e, cudaMalloc(&e->sigma[k], ibytes));
-        CK(e, cudaMalloc(&e->rank[k], ibytes));
     }
     CK(e, cudaMalloc(&e->gidx, ibytes));
+    CK(e, cudaMalloc(&e->pcell, ibytes));
+    CK(e, cudaMalloc(&e->prank, ibytes));
+    CK(e, cudaMalloc(&e->ref_keys, ibytes));
+    CK(e, cudaMalloc(&e->ref_perm, ibytes));
     CK(e, cudaMalloc(&e->sort_mem, mpm::sort_scratch_bytes(std::max(n, 1))));
     mpm::sort_scratch_carve(e->sort_mem, std::max(n, 1), &e->sort);
     e->sort.n = n;
     CK(e, cudaMalloc(&e->pos_out, (size_t)std::max(n, 1) * 3 * sizeof(float)));
     return MPM_OK;
+}
+
+// Bytes of the two counter sets: per set (nb + 1) * kBinCells cell counts,
+// nb + 1 bin counts and nb + 1 list entries, rounded up to 256 bytes so that
+// the second set's cell counts stay 16-byte aligned for vector access.
+size_t bins_set_words(const SimParams& p) { return align_up((size_t)(p.nb + 1) * (mpm::kBinCells + 2), 64); }
+size_t bins_bytes(const SimParams& p) { return 2 * bins_set_words(p) * sizeof(uint32_t); }
+
+void carve_bins(mpm_engine* e) {
+    const SimParams& p = e->prm;
+    uint32_t* base = static_cast<uint32_t*>(e->bins_mem);
+    for (int k = 0; k < 2; ++k) {
+        uint32_t* s = base + k * bins_set_words(p);  // cell counts first: 16-byte aligned
+        e->bins[k].ccount = s;
+        e->bins[k].bcount = s + (size_t)(p.nb + 1) * mpm::kBinCells;
+        e->bins[k].blist = reinterpret_cast<int32_t*>(e->bins[k].bcount + (p.nb + 1));
+        e->bins[k].nlist = e->ctl + k;
+    }
 }
 
 // Enqueues stages `from`..`upto` (MPM_STAGE_*) of one substep from parity
@@ -177,19 +214,21 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
         if (marks) cudaEventRecordWithFlags(marks[k], st, cudaEventRecordExternal);
     };
     int launches = 0;
+    uint32_t* work = e->ctl + 2;
     mark(0);
     if (from <= MPM_STAGE_SORT && upto >= MPM_STAGE_SORT)
-        launches += mpm::launch_radix_sort(e->keys[par], p.n, e->sort, e->sigma[1 - par], e->rank[1 - par],
-                                           e->rank[par], e->gidx, st);
+        launches += mpm::launch_bin_order(p, e->bins[par], e->bins[1 - par], e->bstart, e->cstart, e->pcell, e->prank,
+                                          e->gidx, work, st);
     mark(1);
-    if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G) launches += mpm::launch_p2g(p, e->P[par], e->gidx, e->accum, st);
+    if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
+        launches += mpm::launch_p2g(p, e->P[par], e->gidx, e->bstart, e->cstart, e->bins[par], work, e->accum, st);
     mark(2);
     if (from <= MPM_STAGE_GRID && upto >= MPM_STAGE_GRID)
         launches += mpm::launch_grid_update(p, e->accum, e->vgrid, e->sdf, st);
     mark(3);
     if (from <= MPM_STAGE_G2P && upto >= MPM_STAGE_G2P)
-        launches += mpm::launch_g2p(p, e->P[par], e->P[1 - par], e->gidx, e->sigma[1 - par], e->vgrid, e->sdf,
-                                    e->keys[1 - par], e->d_flags, st);
+        launches += mpm::launch_g2p(p, e->P[par], e->P[1 - par], e->gidx, e->sigma[par], e->sigma[1 - par], e->vgrid,
+                                    e->sdf, e->pcell, e->prank, e->bins[1 - par], e->d_flags, st);
     mark(4);
     return launches;
 }
@@ -285,10 +324,14 @@ mpm_status load_state(mpm_engine* e, const float* soa26_host, bool init_rules) {
         mpm_status s = ensure_staging(e, bytes);
         if (s != MPM_OK) return s;
         CK(e, cudaMemcpyAsync(e->staging, soa26_host, bytes, cudaMemcpyHostToDevice, e->stream));
-        e->kernel_launches += mpm::launch_state_import(e->prm, e->staging, e->P[0], e->sigma[0], e->rank[0],
-                                                       e->keys[0], init_rules, e->stream);
+        e->kernel_launches += mpm::launch_state_import(e->prm, e->staging, e->P[0], e->sigma[0], init_rules, e->stream);
         CK(e, cudaGetLastError());
     }
+    // Both counter sets empty, then the imported particles filed into set 0.
+    CK(e, cudaMemsetAsync(e->bins_mem, 0, bins_bytes(e->prm), e->stream));
+    CK(e, cudaMemsetAsync(e->ctl, 0, 4 * sizeof(uint32_t), e->stream));
+    e->kernel_launches += mpm::launch_bin_count(e->prm, e->P[0], e->pcell, e->prank, e->bins[0], e->stream);
+    CK(e, cudaGetLastError());
     e->parity = 0;
     e->sort_src = kNoSort;
     e->partial_stage = 0;
@@ -332,7 +375,6 @@ mpm_status run_steps(mpm_engine* e, int32_t nsub) {
         }
         CK(e, cudaGraphLaunch(e->graph[e->parity], e->stream));
         e->kernel_launches += e->graph_kernels[e->parity];
-        e->sort_passes += e->n > 0 ? 4 : 0;
         e->sort_src = e->parity;
         e->parity ^= 1;
         ++e->substeps;
@@ -408,7 +450,12 @@ extern "C" mpm_status mpm_create(const mpm_config* cfg, int32_t device, mpm_engi
     p.pmass = 1.0f;                                                // kernels.cu:357
     p.n = 0;
     p.g = (int)g;
-    p.ld = 64;
+    p.nbx = (cfg->size_x + 2 + mpm::kBinX - 1) / mpm::kBinX;
+    p.nby = (cfg->size_y + 2 + mpm::kBinY - 1) / mpm::kBinY;
+    p.nbz = (cfg->size_z + 2 + mpm::kBinZ - 1) / mpm::kBinZ;
+    if ((long long)p.nbx * p.nby * p.nbz >= 0x7fffffffLL / mpm::kBinCells - 1)
+        return record(nullptr, MPM_ERR_BAD_CONFIG, "grid too large for the cell index");
+    p.nb = p.nbx * p.nby * p.nbz;
 
     auto fail = [&](mpm_status s) {
         g_global_error = e->last_error;
@@ -421,8 +468,13 @@ extern "C" mpm_status mpm_create(const mpm_config* cfg, int32_t device, mpm_engi
     if ((err = cudaMalloc(&e->accum, (size_t)g * sizeof(float4))) != cudaSuccess ||
         (err = cudaMalloc(&e->vgrid, (size_t)g * sizeof(float4))) != cudaSuccess ||
         (err = cudaMalloc(&e->sdf, (size_t)g * sizeof(float))) != cudaSuccess ||
-        (err = cudaMalloc(&e->d_flags, 2 * sizeof(uint32_t))) != cudaSuccess)
+        (err = cudaMalloc(&e->d_flags, 2 * sizeof(uint32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->bins_mem, bins_bytes(p))) != cudaSuccess ||
+        (err = cudaMalloc(&e->bstart, (size_t)(p.nb + 2) * sizeof(int32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->cstart, (size_t)(p.nb + 1) * mpm::kBinCells * sizeof(int32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->ctl, 4 * sizeof(uint32_t))) != cudaSuccess)
         return fail(cuda_fail(e, err, "cudaMalloc(grid)"));
+    carve_bins(e);
     cudaMemsetAsync(e->accum, 0, (size_t)g * sizeof(float4), e->stream);
     cudaMemsetAsync(e->vgrid, 0, (size_t)g * sizeof(float4), e->stream);
     cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(uint32_t), e->stream);
@@ -443,6 +495,10 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->accum);
     free_dev(e->vgrid);
     free_dev(e->sdf);
+    free_dev(e->bins_mem);
+    free_dev(e->bstart);
+    free_dev(e->cstart);
+    free_dev(e->ctl);
     free_dev(e->d_flags);
     free_dev(e->staging);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -456,7 +512,6 @@ extern "C" mpm_status mpm_init_particles(mpm_engine* e, int64_t n, const float* 
     if (n > 0 && !soa26_host) return record(e, MPM_ERR_INVALID_ARGUMENT, "soa26_host is NULL");
     if ((s = alloc_particles(e, (int)n)) != MPM_OK) return s;
     e->prm.n = (int)n;
-    e->prm.ld = e->ld;
     e->prm.pvol = e->cfg.resolution * e->cfg.resolution * e->cfg.resolution;
     e->prm.pmass = 1.0f;
     e->substeps = 0;
@@ -544,10 +599,7 @@ extern "C" mpm_status mpm_substep_partial(mpm_engine* e, int32_t upto) {
     }
     e->kernel_launches += enqueue_substep(e, e->parity, from, upto);
     CK(e, cudaGetLastError());
-    if (from == MPM_STAGE_SORT) {
-        e->sort_passes += e->n > 0 ? 4 : 0;
-        e->sort_src = e->parity;
-    }
+    if (from == MPM_STAGE_SORT) e->sort_src = e->parity;
     e->partial_stage = upto;
     if (upto == MPM_STAGE_P2G) {
         e->accum_dirty = true;
@@ -635,10 +687,20 @@ extern "C" mpm_status mpm_get_sort(mpm_engine* e, int32_t* keys_host, int32_t* p
     if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
     if (e->n == 0) return MPM_OK;
     const size_t bytes = (size_t)e->n * sizeof(int32_t);
-    const int32_t* k = e->sort_src == kNoSort ? e->keys[e->parity] : e->keys[e->sort_src];
-    const int32_t* q = e->sort_src == kNoSort ? e->sigma[e->parity] : e->sigma[1 - e->sort_src];
-    if (keys_host) CK(e, cudaMemcpyAsync(keys_host, k, bytes, cudaMemcpyDeviceToHost, e->stream));
-    if (perm_host) CK(e, cudaMemcpyAsync(perm_host, q, bytes, cudaMemcpyDeviceToHost, e->stream));
+    // The state the most recent substep started from (intact until the next
+    // substep), or the current state before any substep.
+    const int src = e->sort_src == kNoSort ? e->parity : e->sort_src;
+    e->kernel_launches += mpm::launch_reference_keys(e->prm, e->P[src], e->sigma[src], e->ref_keys, e->stream);
+    if (e->sort_src == kNoSort) {
+        e->kernel_launches += mpm::launch_identity(e->ref_perm, e->n, e->stream);
+    } else {
+        e->kernel_launches += mpm::launch_radix_sort(e->ref_keys, e->n, e->sort, e->ref_perm, nullptr, nullptr,
+                                                     nullptr, e->stream);
+        e->sort_passes += 4;
+    }
+    CK(e, cudaGetLastError());
+    if (keys_host) CK(e, cudaMemcpyAsync(keys_host, e->ref_keys, bytes, cudaMemcpyDeviceToHost, e->stream));
+    if (perm_host) CK(e, cudaMemcpyAsync(perm_host, e->ref_perm, bytes, cudaMemcpyDeviceToHost, e->stream));
     CK(e, cudaStreamSynchronize(e->stream));
     return MPM_OK;
 }

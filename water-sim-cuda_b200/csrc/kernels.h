@@ -45,20 +45,48 @@ int launch_radix_sort(const int32_t* keys, int n, const SortScratch& s, int32_t*
                       const int32_t* rank_in, int32_t* gidx, cudaStream_t st);
 
 // ------------------------------------------------------------- substep ----
-// P holds kStatePlanes planes of stride p.ld in the order sigma of the last
-// sort; gidx[j] is the slot in P of the j-th particle of the new order.
-int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, float4* accum, cudaStream_t st);
+// P is the particle-major state (device_math.cuh), ordered by cell of the
+// binning that produced it.  pcell[j]/prank[j] are the cell of slot j and its
+// rank among the cell's particles.  A counter set holds, for the cells
+// (nb + 1) * kBinCells of the grid, their particle counts, the bin counts
+// (nb + 1), and the list of bins that hold particles (nb + 1 entries + its
+// length).  Two sets alternate: a substep orders the particles by one and
+// its G2P fills the other, which that substep clears first.
+struct BinSet {
+    uint32_t* ccount;
+    uint32_t* bcount;
+    int32_t* blist;
+    uint32_t* nlist;
+};
+
+// Files the particles of P in slot order into an empty set (after an import).
+int launch_bin_count(const SimParams& p, const float* P, int32_t* pcell, int32_t* prank, const BinSet& set,
+                     cudaStream_t st);
+// Order by cell from set `cur`: bstart (nb + 2 bin starts), cstart (first slot
+// of every cell of a listed bin), gidx[new slot] = old slot; clears `other`
+// and the P2G work counter.
+int launch_bin_order(const SimParams& p, const BinSet& cur, const BinSet& other, int32_t* bstart, int32_t* cstart,
+                     const int32_t* pcell, const int32_t* prank, int32_t* gidx, uint32_t* work, cudaStream_t st);
+// P2G over the bins listed in `cur`; gidx maps slots of the new order to P.
+int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, const int32_t* bstart, const int32_t* cstart,
+               const BinSet& cur, uint32_t* work, float4* accum, cudaStream_t st);
 int launch_grid_update(const SimParams& p, float4* accum, float4* vgrid, const float* sdf, cudaStream_t st);
-int launch_g2p(const SimParams& p, const float* Pin, float* Pout, const int32_t* gidx, const int32_t* sigma,
-               const float4* vgrid, const float* sdf, int32_t* keys_out, uint32_t* health, cudaStream_t st);
+// G2P: slot j of Pout = particle gidx[j] of Pin advanced one substep;
+// sig_out[j] = sig_in[gidx[j]]; files slot j into `next`.
+int launch_g2p(const SimParams& p, const float* Pin, float* Pout, const int32_t* gidx, const int32_t* sig_in,
+               int32_t* sig_out, const float4* vgrid, const float* sdf, int32_t* pcell, int32_t* prank,
+               const BinSet& next, uint32_t* health, cudaStream_t st);
 
 // ------------------------------------------------------ state transfer ----
 // Loads a 26-plane host-layout state (already on the device, stride n) into
-// P (stride p.ld, original order) and resets the order to the identity.
-// init_rules applies initFMatrices (kernels.cu:349-358): F diagonal = 1.
-int launch_state_import(const SimParams& p, const float* soa26, float* P, int32_t* sigma, int32_t* rank,
-                        int32_t* keys, bool init_rules, cudaStream_t st);
-// Writes the 26-plane state in original order: out[k*n + sigma[j]] = P[k][j].
+// P (original order) and sets sigma to the identity.  init_rules applies
+// initFMatrices (kernels.cu:349-358): F diagonal = 1.
+int launch_state_import(const SimParams& p, const float* soa26, float* P, int32_t* sigma, bool init_rules,
+                        cudaStream_t st);
+// keys[sigma[j]] = setKeys' Morton key of slot j of P (original order).
+int launch_reference_keys(const SimParams& p, const float* P, const int32_t* sigma, int32_t* keys, cudaStream_t st);
+// Writes the 26-plane state in original order: plane k of particle sigma[j]
+// from slot j of P (VOL and MASS from the scalars).
 int launch_state_export(const SimParams& p, const float* P, const int32_t* sigma, float* soa26, cudaStream_t st);
 // Float3 positions in original order (changeFormat, kernels.cu:341-347).
 int launch_positions_export(const SimParams& p, const float* P, const int32_t* sigma, float* xyz, cudaStream_t st);
@@ -69,6 +97,8 @@ int launch_grid_export(const SimParams& p, const float4* grid, float* planes4, c
 // tris: 9*t floats on the device, allocation padded by >= 16 bytes.
 int launch_sdf_build(const SimParams& p, const float* tris, int t, float* sdf, uint32_t* status, cudaStream_t st);
 int launch_fill(float* dst, long long count, float value, cudaStream_t st);
+// dst[i] = i for i < n.
+int launch_identity(int32_t* dst, int n, cudaStream_t st);
 
 // Device status bits written by kernels with bounded waits.
 enum : uint32_t { kStatusTimeout = 1u << 0 };

@@ -1,9 +1,16 @@
-// One MLS-MPM substep on the device: P2G scatter, grid update, G2P gather,
-// plus the kernels that move state across the boundary.
+// One MLS-MPM substep on the device: particle binning, P2G scatter, grid
+// update, G2P gather, plus the kernels that move state across the boundary.
 //
 // Layout (HBM):
-//  - particle state: 24 float planes (pos, vel, C, F) of stride ld, kept in
-//    the Morton order of the last sort, so every particle kernel streams it;
+//  - particle state: particle-major, 24 floats per particle (device_math.cuh),
+//    double-buffered, ordered by cell of the last binning so that the
+//    particles of one stencil base cell are contiguous;
+//  - cells: every stencil base cell of the grid, numbered bin * kBinCells +
+//    the cell's index in its bin (kBinX x kBinY x kBinZ cells).  Two counter
+//    sets alternate: the substep from parity p orders the particles by set p
+//    (filled by the previous G2P or by an import) and its G2P files every
+//    particle into set 1-p (cell count, bin count, and the list of bins that
+//    received particles);
 //  - grid: one float4 per node, (mass, x, y, z).  `accum` receives the P2G
 //    sums with 16-byte vector reductions (red.global.add.v4.f32); the grid
 //    update turns it into `vgrid` (mass, velocity) and leaves `accum` zero
@@ -17,145 +24,433 @@
 namespace mpm {
 namespace {
 
-constexpr int kP2GThreads = 256;
-constexpr int kTileCap = 2048;  // nodes of the per-CTA shared tile (32 KB)
-
 __device__ __forceinline__ void red_add_v4(float4* addr, float a, float b, float c, float d) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
                  : "memory");
 }
 
-// P2G (p2GTransferScatter, kernels.cu:6-142).  One thread per particle of the
-// sorted order.  The CTA's particles are contiguous in Morton order, so the
-// in-grid nodes of their 3x3x3 stencils fit a small box; the CTA accumulates
-// into that box in shared memory and flushes each touched node once with a
-// vector reduction.  A CTA whose box exceeds kTileCap nodes (its particles
-// straddle a high-level Morton boundary) reduces straight to global memory.
-// Unlike the reference, no tile partial sum is dropped (it drops tile cells
-// whose partial mass is <= 1e-9, kernels.cu:132).
-__global__ void __launch_bounds__(kP2GThreads) p2g_kernel(SimParams p, const float* __restrict__ P,
-                                                          const int32_t* __restrict__ gidx,
-                                                          float4* __restrict__ accum) {
-    __shared__ float s_m[kTileCap], s_x[kTileCap], s_y[kTileCap], s_z[kTileCap];
-    __shared__ int s_part[6][kP2GThreads / 32];
-    __shared__ int s_box[6];
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
 
-    const int i = blockIdx.x * kP2GThreads + threadIdx.x;
-    const bool valid = i < p.n;
-    float pos[3] = {0.f, 0.f, 0.f}, vel[3] = {0.f, 0.f, 0.f}, C[9], F[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) C[k] = F[k] = 0.f;
-    if (valid) {
-        const float* q = P + __ldg(gidx + i);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) pos[k] = __ldg(q + (kPX + k) * p.ld);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) vel[k] = __ldg(q + (kVX + k) * p.ld);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) C[k] = __ldg(q + (kC0 + k) * p.ld);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) F[k] = __ldg(q + (kF0 + k) * p.ld);
-    }
-    const int bx = stencil_base(pos[0]), by = stencil_base(pos[1]), bz = stencil_base(pos[2]);
-    // In-grid part of the stencil; 64-bit so saturated bases cannot overflow.
-    const int lox = (int)max((long long)bx, 0LL), hix = (int)min((long long)bx + 2, (long long)p.sx - 1);
-    const int loy = (int)max((long long)by, 0LL), hiy = (int)min((long long)by + 2, (long long)p.sy - 1);
-    const int loz = (int)max((long long)bz, 0LL), hiz = (int)min((long long)bz + 2, (long long)p.sz - 1);
-    const bool contributes = valid && lox <= hix && loy <= hiy && loz <= hiz;
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
-    // CTA box of all contributing stencils.
-    int box[6] = {contributes ? lox : INT_MAX, contributes ? loy : INT_MAX, contributes ? loz : INT_MAX,
-                  contributes ? hix : INT_MIN, contributes ? hiy : INT_MIN, contributes ? hiz : INT_MIN};
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) box[k] = __reduce_min_sync(0xffffffffu, box[k]);
-#pragma unroll
-    for (int k = 3; k < 6; ++k) box[k] = __reduce_max_sync(0xffffffffu, box[k]);
-    if (lane == 0) {
-#pragma unroll
-        for (int k = 0; k < 6; ++k) s_part[k][warp] = box[k];
+// Files this lane's particle under `cell` (bin `bin`) of a counter set and
+// returns its rank among the cell's particles: one atomic per distinct cell
+// and per distinct bin of the warp; the first particle of a bin appends the
+// bin to the set's list.  Every lane of the warp must call it; lanes with
+// cell < 0 take part without counting.
+__device__ __forceinline__ int file_particle(int cell, int bin, const BinSet& set) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t peers = __match_any_sync(0xffffffffu, cell);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (cell >= 0 && lane == leader) base = atomicAdd(set.ccount + cell, (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const uint32_t bpeers = __match_any_sync(0xffffffffu, bin);
+    if (bin >= 0 && lane == __ffs(bpeers) - 1) {
+        if (atomicAdd(set.bcount + bin, (uint32_t)__popc(bpeers)) == 0u) set.blist[atomicAdd(set.nlist, 1u)] = bin;
     }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        const int k = threadIdx.x;
-        int v = s_part[k][0];
-        for (int w = 1; w < kP2GThreads / 32; ++w) v = k < 3 ? min(v, s_part[k][w]) : max(v, s_part[k][w]);
-        s_box[k] = v;
-    }
-    __syncthreads();
-    const int ox = s_box[0], oy = s_box[1], oz = s_box[2];
-    if (ox > s_box[3]) return;  // no particle of this CTA touches the grid (uniform)
-    const int dx = s_box[3] - ox + 1, dy = s_box[4] - oy + 1, dz = s_box[5] - oz + 1;
-    const long long vol = (long long)dx * dy * dz;
-    const bool use_tile = vol <= kTileCap;
-    if (use_tile) {
-        for (int q = threadIdx.x; q < vol; q += kP2GThreads) s_m[q] = s_x[q] = s_y[q] = s_z[q] = 0.f;
-    }
-    __syncthreads();
+    return (int)base + __popc(peers & lanemask_lt());
+}
 
-    if (contributes) {
-        // Tait pressure from the clamped det F and the APIC + stress affine
-        // matrix C' = C + (4 DT V p / m) I (kernels.cu:26-35).
-        float J = det3(F);
-        J = fmaxf(0.9f, fminf(J, 1.1f));
-        float pressure = p.compression * (powf(J, p.gamma) - 1.0f);
-        if (pressure < 0.0f) pressure = 0.0f;
-        const float volume = p.pvol * J;
-        const float multi = 4.0f * p.dt * volume * pressure / p.pmass;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) C[k] += multi * ((k % 4 == 0) ? 1.0f : 0.0f);
+// ------------------------------------------------------------------ P2G ----
+// P2G (p2GTransferScatter, kernels.cu:6-142).  Persistent CTAs of four warps
+// take the bins that hold particles from a work counter.  Warp w walks z-layer
+// w of the bin (8 x 4 base cells), one lane per cell: all particles of a cell
+// scatter to the same 27 nodes, so the lane sums them in registers, reading
+// them through a ring of kRing particles fetched ahead with 16-byte cp.async
+// copies (the gather through gidx costs no registers).  The lane then adds
+// its 27 sums to the warp's footprint, the layer's 10 x 6 x 3 nodes: the 32
+// cells of a layer are distinct, so for one stencil offset the 32 nodes
+// differ and a plain read-add-write per offset is race-free.  A bin with
+// fewer than kSparseBin particles (spray, thin sheets) would leave most lanes
+// idle; there each thread takes one particle and adds to the footprint of
+// the particle's layer with shared atomics.  The four footprints, which
+// overlap in z, are summed into the bin's 10 x 6 x 6 nodes and sent to global
+// memory with one vector reduction per touched node.  Unlike the reference,
+// no partial sum is dropped (it drops shared-tile cells whose partial mass is
+// <= 1e-9, kernels.cu:132).
+constexpr int kP2GThreads = 32 * kBinZ;  // one warp per z-layer of a bin
+constexpr int kP2GBlocksPerSM = 3;
+constexpr int kRing = 2;
+constexpr int kGidxStage = 256;  // gather indices of a layer staged in shared memory
+constexpr int kSparseBin = 96;   // bins with fewer particles take one thread per particle
+constexpr int kTX = kBinX + 2, kTY = kBinY + 2;
+constexpr int kFootNodes = kTX * kTY * 3;             // 180: one layer's stencil footprint
+constexpr int kTileNodes = kTX * kTY * (kBinZ + 2);  // 360: the bin's nodes
+static_assert(kBinX * kBinY == 32, "one warp covers one z-layer of a bin");
 
-        float wx[3], wy[3], wz[3];
+// Spline weights of nodes 0, 1, 2 of one axis at fractional offset f = pos -
+// base, times m.  For f in [0.5, 1.5) (every particle at pos >= 0.5) the
+// branch of bspline_weight is known per node and the same roundings are
+// written out; otherwise the general form.
+__device__ __forceinline__ void axis_weights(float f, float m, float* w) {
+    if (f >= 0.5f && f < 1.5f) {
+        const float t0 = __fsub_rn(1.5f, f);
+        const float x1 = __fsub_rn(f, 1.0f);
+        const float t2 = __fsub_rn(1.5f, __fsub_rn(2.0f, f));
+        w[0] = m * __fmul_rn(__fmul_rn(t0, t0), 0.5f);
+        w[1] = m * __fsub_rn(0.75f, __fmul_rn(x1, x1));
+        w[2] = m * __fmul_rn(__fmul_rn(t2, t2), 0.5f);
+    } else {
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            wx[a] = bspline_weight(pos[0] - (float)(bx + a));
-            wy[a] = bspline_weight(pos[1] - (float)(by + a));
-            wz[a] = bspline_weight(pos[2] - (float)(bz + a));
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const int z = bz + c;
-            if ((unsigned)z >= (unsigned)p.sz) continue;
-            const float dzv = -(pos[2] - (float)z);
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const int y = by + b;
-                if ((unsigned)y >= (unsigned)p.sy) continue;
-                const float dyv = -(pos[1] - (float)y);
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    const int x = bx + a;
-                    if ((unsigned)x >= (unsigned)p.sx) continue;
-                    const float dxv = -(pos[0] - (float)x);
-                    const float w = wx[a] * wy[b] * wz[c];
-                    const float wm = p.pmass * w;
-                    const float mx = wm * (vel[0] + (C[0] * dxv + C[1] * dyv + C[2] * dzv));
-                    const float my = wm * (vel[1] + (C[3] * dxv + C[4] * dyv + C[5] * dzv));
-                    const float mz = wm * (vel[2] + (C[6] * dxv + C[7] * dyv + C[8] * dzv));
-                    if (use_tile) {
-                        const int l = ((z - oz) * dy + (y - oy)) * dx + (x - ox);
-                        atomicAdd(&s_m[l], wm);
-                        atomicAdd(&s_x[l], mx);
-                        atomicAdd(&s_y[l], my);
-                        atomicAdd(&s_z[l], mz);
-                    } else {
-                        red_add_v4(accum + node_index(p, x, y, z), wm, mx, my, mz);
-                    }
-                }
-            }
-        }
-    }
-    if (!use_tile) return;  // uniform
-    __syncthreads();
-    for (int q = threadIdx.x; q < vol; q += kP2GThreads) {
-        const float m = s_m[q];
-        if (m != 0.0f) {
-            const int lx = q % dx, ly = (q / dx) % dy, lz = q / (dx * dy);
-            red_add_v4(accum + node_index(p, ox + lx, oy + ly, oz + lz), m, s_x[q], s_y[q], s_z[q]);
-        }
+        for (int a = 0; a < 3; ++a) w[a] = m * bspline_weight(f - (float)a);
     }
 }
 
+// Per-particle part of P2G from the particle's 96-byte record: the spline
+// weights (mass folded into wx) and the affine momentum at stencil node
+// (0,0,0), u = v - C' f, with C' the stress-augmented affine matrix.  Node
+// o of the stencil then gets w_o (u + C' o).
+struct P2GParticle {
+    float wx[3], wy[3], wz[3];
+    float u0, u1, u2;
+    float C[9];
+    int bx, by, bz;  // stencil base cell
+};
+
+__device__ __forceinline__ P2GParticle p2g_particle(const SimParams& p, float4 q0, float4 q1, float4 q2, float4 q3,
+                                                    float4 q4, float4 q5) {
+    P2GParticle r;
+    const float px = q0.x, py = q0.y, pz = q0.z;
+    const float F[9] = {q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
+    float* C = r.C;
+    C[0] = q3.w;
+    C[1] = q4.x;
+    C[2] = q4.y;
+    C[3] = q4.z;
+    C[4] = q4.w;
+    C[5] = q5.x;
+    C[6] = q5.y;
+    C[7] = q5.z;
+    C[8] = q5.w;
+    // Tait pressure from the clamped det F and the APIC + stress affine
+    // matrix C' = C + (4 DT V p / m) I (kernels.cu:20-35).
+    float J = det3(F);
+    J = fmaxf(0.9f, fminf(J, 1.1f));
+    float pressure = p.compression * (powf(J, p.gamma) - 1.0f);
+    if (pressure < 0.0f) pressure = 0.0f;
+    const float multi = 4.0f * p.dt * (p.pvol * J) * pressure / p.pmass;
+    C[0] += multi;
+    C[4] += multi;
+    C[8] += multi;
+    // f = pos - base is exact for |pos| < 2^24, so f - o equals the
+    // reference's pos - (base + o) bit for bit.
+    r.bx = stencil_base(px);
+    r.by = stencil_base(py);
+    r.bz = stencil_base(pz);
+    const float fx = px - (float)r.bx, fy = py - (float)r.by, fz = pz - (float)r.bz;
+    axis_weights(fx, p.pmass, r.wx);
+    axis_weights(fy, 1.0f, r.wy);
+    axis_weights(fz, 1.0f, r.wz);
+    r.u0 = q3.x - (C[0] * fx + C[1] * fy + C[2] * fz);
+    r.u1 = q3.y - (C[3] * fx + C[4] * fy + C[5] * fz);
+    r.u2 = q3.z - (C[6] * fx + C[7] * fy + C[8] * fz);
+    return r;
+}
+
+// The 27 contributions w_o (u + C' o) of one particle, o = (a, b, c), handed
+// to emit(k, a, b, c, m, mx, my, mz) in order k = (c * 3 + b) * 3 + a.
+template <typename Emit>
+__device__ __forceinline__ void p2g_stencil(const P2GParticle& r, Emit emit) {
+    float tz0 = r.u0, tz1 = r.u1, tz2 = r.u2;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float ty0 = tz0, ty1 = tz1, ty2 = tz2;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const float wyz = r.wy[b] * r.wz[c];
+            float t0 = ty0, t1 = ty1, t2 = ty2;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const float w = r.wx[a] * wyz;
+                emit((c * 3 + b) * 3 + a, a, b, c, w, w * t0, w * t1, w * t2);
+                t0 += r.C[0];
+                t1 += r.C[3];
+                t2 += r.C[6];
+            }
+            ty0 += r.C[1];
+            ty1 += r.C[4];
+            ty2 += r.C[7];
+        }
+        tz0 += r.C[2];
+        tz1 += r.C[5];
+        tz2 += r.C[8];
+    }
+}
+
+__global__ void __launch_bounds__(kP2GThreads, kP2GBlocksPerSM) p2g_kernel(
+    SimParams p, const float* __restrict__ P, const int32_t* __restrict__ gidx, const int32_t* __restrict__ bstart,
+    const int32_t* __restrict__ cstart, BinSet set, uint32_t* __restrict__ work, float4* __restrict__ accum) {
+    __shared__ __align__(16) float4 s_ring[kBinZ][kRing][6][32];
+    __shared__ float4 s_foot[kBinZ][kFootNodes];
+    __shared__ int32_t s_gidx[kBinZ][kGidxStage];
+    __shared__ int s_item;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int lx = lane % kBinX, ly = lane / kBinX;
+    const int nbins = (int)*reinterpret_cast<volatile uint32_t*>(set.nlist);
+    float4* foot = &s_foot[0][0];
+    for (int q = t; q < kBinZ * kFootNodes; q += kP2GThreads) foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (;;) {
+        if (t == 0) s_item = (int)atomicAdd(work, 1u);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= nbins) return;
+        const int bin = __ldg(set.blist + item);
+        if (bin >= p.nb) continue;  // the overflow bin reaches no node
+        const int bxi = bin % p.nbx, byi = (bin / p.nbx) % p.nby, bzi = bin / (p.nbx * p.nby);
+        // Node origin of the bin = base cell of its cell (0,0,0).
+        const int ox = bxi * kBinX - 2, oy = byi * kBinY - 2, oz = bzi * kBinZ - 2;
+        const int b0 = __ldg(bstart + bin), bn = __ldg(bstart + bin + 1) - b0;
+        if (bn < kSparseBin) {
+            for (int i = t; i < bn; i += kP2GThreads) {
+                const float4* q = reinterpret_cast<const float4*>(P + (size_t)__ldg(gidx + b0 + i) * kAFloats);
+                const P2GParticle r = p2g_particle(p, __ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3), __ldg(q + 4),
+                                                   __ldg(q + 5));
+                const int tx = r.bx - ox, ty = r.by - oy, tz = r.bz - oz;
+                if ((unsigned)tx < (unsigned)kBinX && (unsigned)ty < (unsigned)kBinY && (unsigned)tz < (unsigned)kBinZ) {
+                    float4* f = s_foot[tz];
+                    p2g_stencil(r, [&](int, int a, int b, int c, float m, float mx, float my, float mz) {
+                        float4* d = &f[(c * kTY + ty + b) * kTX + tx + a];
+                        atomicAdd(&d->x, m);
+                        atomicAdd(&d->y, mx);
+                        atomicAdd(&d->z, my);
+                        atomicAdd(&d->w, mz);
+                    });
+                } else {
+                    // Not filed under this bin (cannot happen while the binning
+                    // matches the state): straight to global memory.
+                    p2g_stencil(r, [&](int, int a, int b, int c, float m, float mx, float my, float mz) {
+                        const long long x = (long long)r.bx + a, y = (long long)r.by + b, z = (long long)r.bz + c;
+                        if (x >= 0 && y >= 0 && z >= 0 && x < p.sx && y < p.sy && z < p.sz)
+                            red_add_v4(accum + node_index(p, (int)x, (int)y, (int)z), m, mx, my, mz);
+                    });
+                }
+            }
+        } else {
+            // Layer `warp`: the cells of a layer are consecutive, so its
+            // particles are slots [l0, l1) of the new order.
+            const int cell = bin * kBinCells + warp * 32 + lane;
+            const int cs = __ldg(cstart + cell);
+            const int cnt = (int)__ldg(set.ccount + cell);
+            const int l0 = __shfl_sync(0xffffffffu, cs, 0);
+            const int l1 = __shfl_sync(0xffffffffu, cs + cnt, 31);
+            int maxc = cnt;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
+            if (maxc > 0) {
+                const bool staged = l1 - l0 <= kGidxStage;
+                if (staged)
+                    for (int q = lane; q < l1 - l0; q += 32) s_gidx[warp][q] = __ldg(gidx + l0 + q);
+                __syncwarp();
+                auto src_of = [&](int s) -> const float4* {
+                    const int g = staged ? s_gidx[warp][cs - l0 + s] : __ldg(gidx + cs + s);
+                    return reinterpret_cast<const float4*>(P + (size_t)g * kAFloats);
+                };
+                float4(*ring)[6][32] = s_ring[warp];
+#pragma unroll
+                for (int d = 0; d < kRing - 1; ++d) {
+                    if (d < cnt) {
+                        const float4* src = src_of(d);
+#pragma unroll
+                        for (int v = 0; v < 6; ++v) cp_async16(&ring[d][v][lane], src + v);
+                    }
+                    cp_async_commit();
+                }
+                float am[27], ax[27], ay[27], az[27];
+#pragma unroll
+                for (int k = 0; k < 27; ++k) am[k] = ax[k] = ay[k] = az[k] = 0.f;
+                for (int s = 0; s < maxc; ++s) {
+                    const int pf = s + kRing - 1;
+                    if (pf < cnt) {
+                        const float4* src = src_of(pf);
+#pragma unroll
+                        for (int v = 0; v < 6; ++v) cp_async16(&ring[pf % kRing][v][lane], src + v);
+                    }
+                    cp_async_commit();
+                    cp_async_wait<kRing - 1>();
+                    __syncwarp();
+                    if (s < cnt) {
+                        const int sl = s % kRing;
+                        const P2GParticle r = p2g_particle(p, ring[sl][0][lane], ring[sl][1][lane], ring[sl][2][lane],
+                                                           ring[sl][3][lane], ring[sl][4][lane], ring[sl][5][lane]);
+                        p2g_stencil(r, [&](int k, int, int, int, float m, float mx, float my, float mz) {
+                            am[k] += m;
+                            ax[k] += mx;
+                            ay[k] += my;
+                            az[k] += mz;
+                        });
+                    }
+                    __syncwarp();
+                }
+                cp_async_wait<0>();
+                float4* f = s_foot[warp];
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b)
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            const int k = (c * 3 + b) * 3 + a;
+                            float4* d = &f[(c * kTY + ly + b) * kTX + lx + a];
+                            __syncwarp();
+                            float4 v = *d;
+                            v.x += am[k];
+                            v.y += ax[k];
+                            v.z += ay[k];
+                            v.w += az[k];
+                            *d = v;
+                        }
+            }
+        }
+        __syncthreads();
+        // Footprint of layer w covers nodes z = w .. w + 2 of the bin.
+        for (int q = t; q < kTileNodes; q += kP2GThreads) {
+            const int x = q % kTX, y = (q / kTX) % kTY, z = q / (kTX * kTY);
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int w = 0; w < kBinZ; ++w) {
+                const int zz = z - w;
+                if (zz < 0 || zz > 2) continue;
+                const float4 u = s_foot[w][(zz * kTY + y) * kTX + x];
+                v.x += u.x;
+                v.y += u.y;
+                v.z += u.z;
+                v.w += u.w;
+            }
+            const int gx = ox + x, gy = oy + y, gz = oz + z;
+            if (node_in_grid(p, gx, gy, gz) && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))  // NaN counts
+                red_add_v4(accum + node_index(p, gx, gy, gz), v.x, v.y, v.z, v.w);
+        }
+        __syncthreads();
+        for (int q = t; q < kBinZ * kFootNodes; q += kP2GThreads) foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// -------------------------------------------------------------- binning ----
+// Files the particles of an imported state (slot order) into a counter set.
+__global__ void __launch_bounds__(256) bin_count_kernel(SimParams p, const float* __restrict__ P,
+                                                        int32_t* __restrict__ pcell, int32_t* __restrict__ prank,
+                                                        BinSet set) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = j < p.n;
+    int cell = -1, bin = -1;
+    if (valid) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(P + (size_t)j * kAFloats));
+        cell = cell_of(p, q.x, q.y, q.z, &bin);
+    }
+    const int r = file_particle(cell, bin, set);
+    if (valid) {
+        pcell[j] = cell;
+        prank[j] = r;
+    }
+}
+
+// bstart[i] = sum of bcount[0..i) over nbins = nb + 1 bins, bstart[nbins] =
+// n.  Also zeroes the bin counters of the other set and the P2G work
+// counter.  One CTA.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(const uint32_t* __restrict__ bcount,
+                                                                uint32_t* __restrict__ bclear,
+                                                                int32_t* __restrict__ bstart, int nbins,
+                                                                uint32_t* __restrict__ work) {
+    __shared__ int s_warp[kScanThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int per = (nbins + kScanThreads - 1) / kScanThreads;
+    const int lo = min(t * per, nbins), hi = min(lo + per, nbins);
+    int sum = 0;
+    for (int i = lo; i < hi; ++i) sum += (int)bcount[i];
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int w = s_warp[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        s_warp[lane] = w;
+    }
+    __syncthreads();
+    int run = incl - sum + (warp > 0 ? s_warp[warp - 1] : 0);
+    for (int i = lo; i < hi; ++i) {
+        const int c = (int)bcount[i];
+        bstart[i] = run;
+        run += c;
+        bclear[i] = 0u;
+    }
+    if (t == kScanThreads - 1) {
+        bstart[nbins] = s_warp[31];
+        *work = 0u;
+    }
+}
+
+// One warp per listed bin: cstart of its 128 cells = bstart[bin] + the
+// exclusive scan of their counts.  Then clears the cell counters of the
+// other set for the bins on that set's list (the cells it last filled).
+__global__ void __launch_bounds__(128) cell_scan_kernel(BinSet set, const int32_t* __restrict__ bstart,
+                                                        int32_t* __restrict__ cstart, BinSet clear) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int nlist = (int)*set.nlist;
+    for (int item = gw; item < nlist; item += nw) {
+        const int bin = set.blist[item];
+        const uint4 c = *reinterpret_cast<const uint4*>(set.ccount + (size_t)bin * kBinCells + lane * 4);
+        const int sum = (int)(c.x + c.y + c.z + c.w);
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int e0 = bstart[bin] + incl - sum;
+        int4 st;
+        st.x = e0;
+        st.y = e0 + (int)c.x;
+        st.z = st.y + (int)c.y;
+        st.w = st.z + (int)c.z;
+        *reinterpret_cast<int4*>(cstart + (size_t)bin * kBinCells + lane * 4) = st;
+    }
+    const int nclear = (int)*clear.nlist;
+    for (int item = gw; item < nclear; item += nw) {
+        const int bin = clear.blist[item];
+        *reinterpret_cast<uint4*>(clear.ccount + (size_t)bin * kBinCells + lane * 4) = make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
+// gidx[cstart[cell[j]] + rank[j]] = j: the order by cell.  Thread 0 resets
+// the other set's list, which cell_scan_kernel has just cleared.
+__global__ void __launch_bounds__(256) bin_scatter_kernel(int n, const int32_t* __restrict__ pcell,
+                                                          const int32_t* __restrict__ prank,
+                                                          const int32_t* __restrict__ cstart,
+                                                          int32_t* __restrict__ gidx, uint32_t* __restrict__ clear_nlist) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j == 0) *clear_nlist = 0u;
+    if (j >= n) return;
+    gidx[__ldg(cstart + __ldg(pcell + j)) + __ldg(prank + j)] = j;
+}
+
+// ---------------------------------------------------------- grid update ----
 // Grid update (gridUpdate, kernels.cu:144-196): v = p/m, gravity, SDF
 // projection where sdf < 0, PADDING walls.  Writes (mass, v) to vgrid and
 // zeroes accum for the next P2G.  The wall tests use the reference's
@@ -195,23 +490,25 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SimParams p, float4* _
     if (a.x != 0.f || a.y != 0.f || a.z != 0.f || a.w != 0.f) accum[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
+// ------------------------------------------------------------------ G2P ----
 // G2P (g2PTransfer, kernels.cu:199-280).  Thread j reads the particle at
-// slot gidx[j] of the old order and writes slot j of the new order, so the
-// state ends up in the order of this substep's sort.  The key of the new
-// position is written at the particle's original index for the next sort.
+// slot gidx[j] of the old state and writes slot j of the new one, so the
+// state ends up ordered by cell.  It also files the new position into the
+// counter set of the next substep.
 __global__ void __launch_bounds__(256) g2p_kernel(SimParams p, const float* __restrict__ Pin,
                                                   float* __restrict__ Pout, const int32_t* __restrict__ gidx,
-                                                  const int32_t* __restrict__ sigma,
+                                                  const int32_t* __restrict__ sig_in, int32_t* __restrict__ sig_out,
                                                   const float4* __restrict__ vgrid, const float* __restrict__ sdf,
-                                                  int32_t* __restrict__ keys_out, uint32_t* __restrict__ health) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= p.n) return;
-    const float* q = Pin + __ldg(gidx + j);
-    float pos[3], F[9];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) pos[k] = __ldg(q + (kPX + k) * p.ld);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) F[k] = __ldg(q + (kF0 + k) * p.ld);
+                                                  int32_t* __restrict__ pcell, int32_t* __restrict__ prank, BinSet next,
+                                                  uint32_t* __restrict__ health) {
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = jj < p.n;
+    const int j = valid ? jj : p.n - 1;  // idle lanes redo the last particle and store nothing
+    const int src = __ldg(gidx + j);
+    const float4* q = reinterpret_cast<const float4*>(Pin + (size_t)src * kAFloats);
+    const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+    const float pos[3] = {q0.x, q0.y, q0.z};
+    const float F[9] = {q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
 
     const int bx = stencil_base(pos[0]), by = stencil_base(pos[1]), bz = stencil_base(pos[2]);
     float wx[3], wy[3], wz[3];
@@ -288,17 +585,20 @@ __global__ void __launch_bounds__(256) g2p_kernel(SimParams p, const float* __re
             tv[2] -= nrm.z * vdn;
         }
     }
-    float* o = Pout + j;
-    o[kPX * p.ld] = nx;
-    o[kPY * p.ld] = ny;
-    o[kPZ * p.ld] = nz;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o[(kVX + k) * p.ld] = tv[k];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) o[(kC0 + k) * p.ld] = tc[k];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) o[(kF0 + k) * p.ld] = NF[k];
-    keys_out[__ldg(sigma + j)] = morton_key(nx, ny, nz);
+    int bin = -1, cell = -1;
+    if (valid) cell = cell_of(p, nx, ny, nz, &bin);
+    const int rank = file_particle(cell, bin, next);
+    if (!valid) return;
+    float4* o = reinterpret_cast<float4*>(Pout + (size_t)j * kAFloats);
+    o[0] = make_float4(nx, ny, nz, NF[0]);
+    o[1] = make_float4(NF[1], NF[2], NF[3], NF[4]);
+    o[2] = make_float4(NF[5], NF[6], NF[7], NF[8]);
+    o[3] = make_float4(tv[0], tv[1], tv[2], tc[0]);
+    o[4] = make_float4(tc[1], tc[2], tc[3], tc[4]);
+    o[5] = make_float4(tc[5], tc[6], tc[7], tc[8]);
+    sig_out[j] = __ldg(sig_in + src);
+    pcell[j] = cell;
+    prank[j] = rank;
 
     uint32_t flags = 0;
     if (!(isfinite(nx) && isfinite(ny) && isfinite(nz) && isfinite(tv[0]) && isfinite(tv[1]) && isfinite(tv[2])))
@@ -308,22 +608,40 @@ __global__ void __launch_bounds__(256) g2p_kernel(SimParams p, const float* __re
     if (flags) atomicOr(health, flags);
 }
 
+// ------------------------------------------------------- state transfer ----
+// Field of the device state that holds host plane k (MPM_POS_X.., 0..23).
+__device__ __forceinline__ int field_of_plane(int k) {
+    if (k < 3) return kAPos + k;
+    if (k < 6) return kAVel + (k - 3);
+    if (k < 15) return kAC + (k - 6);
+    return kAF + (k - 15);
+}
+
 __global__ void __launch_bounds__(256) state_import_kernel(SimParams p, const float* __restrict__ in,
                                                            float* __restrict__ P, int32_t* __restrict__ sigma,
-                                                           int32_t* __restrict__ rank, int32_t* __restrict__ keys,
                                                            bool init_rules) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const long long n = p.n;
+    float v[kAFloats];
 #pragma unroll
-    for (int k = 0; k < kStatePlanes; ++k) {
-        float v = __ldg(in + k * n + i);
-        if (init_rules && (k == kF0 || k == kF0 + 4 || k == kF0 + 8)) v = 1.0f;
-        P[k * p.ld + i] = v;
-    }
+    for (int k = 0; k < kAFloats; ++k) v[field_of_plane(k)] = __ldg(in + k * n + i);
+    if (init_rules) v[kAF + 0] = v[kAF + 4] = v[kAF + 8] = 1.0f;
+    float4* o = reinterpret_cast<float4*>(P + (size_t)i * kAFloats);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
     sigma[i] = i;
-    rank[i] = i;
-    keys[i] = morton_key(__ldg(in + kPX * n + i), __ldg(in + kPY * n + i), __ldg(in + kPZ * n + i));
+}
+
+// keys[sigma[j]] = setKeys' Morton key of the particle in slot j
+// (kernels.cu:361-371): the keys in original particle order.
+__global__ void __launch_bounds__(256) reference_keys_kernel(SimParams p, const float* __restrict__ P,
+                                                             const int32_t* __restrict__ sigma,
+                                                             int32_t* __restrict__ keys) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= p.n) return;
+    const float4 q = __ldg(reinterpret_cast<const float4*>(P + (size_t)j * kAFloats));
+    keys[__ldg(sigma + j)] = morton_key(q.x, q.y, q.z);
 }
 
 __global__ void __launch_bounds__(256) state_export_kernel(SimParams p, const float* __restrict__ P,
@@ -333,8 +651,18 @@ __global__ void __launch_bounds__(256) state_export_kernel(SimParams p, const fl
     if (j >= p.n) return;
     const long long n = p.n;
     const int o = __ldg(sigma + j);
+    const float4* q = reinterpret_cast<const float4*>(P + (size_t)j * kAFloats);
+    float v[kAFloats];
 #pragma unroll
-    for (int k = 0; k < kStatePlanes; ++k) out[k * n + o] = __ldg(P + k * p.ld + j);
+    for (int k = 0; k < 6; ++k) {
+        const float4 t = __ldg(q + k);
+        v[4 * k] = t.x;
+        v[4 * k + 1] = t.y;
+        v[4 * k + 2] = t.z;
+        v[4 * k + 3] = t.w;
+    }
+#pragma unroll
+    for (int k = 0; k < kAFloats; ++k) out[k * n + o] = v[field_of_plane(k)];
     out[24 * n + o] = p.pvol;
     out[25 * n + o] = p.pmass;
 }
@@ -345,9 +673,10 @@ __global__ void __launch_bounds__(256) positions_export_kernel(SimParams p, cons
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= p.n) return;
     const long long o = __ldg(sigma + j);
-    xyz[3 * o + 0] = __ldg(P + kPX * p.ld + j);
-    xyz[3 * o + 1] = __ldg(P + kPY * p.ld + j);
-    xyz[3 * o + 2] = __ldg(P + kPZ * p.ld + j);
+    const float4 q = __ldg(reinterpret_cast<const float4*>(P + (size_t)j * kAFloats));
+    xyz[3 * o + 0] = q.x;
+    xyz[3 * o + 1] = q.y;
+    xyz[3 * o + 2] = q.z;
 }
 
 __global__ void __launch_bounds__(256) grid_export_kernel(SimParams p, const float4* __restrict__ grid,
@@ -362,6 +691,11 @@ __global__ void __launch_bounds__(256) grid_export_kernel(SimParams p, const flo
     planes[3 * g + i] = v.w;
 }
 
+__global__ void __launch_bounds__(256) identity_kernel(int32_t* __restrict__ dst, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = i;
+}
+
 __global__ void __launch_bounds__(256) fill_kernel(float* __restrict__ dst, long long count, float value) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
          i += (long long)gridDim.x * blockDim.x)
@@ -372,9 +706,28 @@ inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, float4* accum, cudaStream_t st) {
+int launch_bin_count(const SimParams& p, const float* P, int32_t* pcell, int32_t* prank, const BinSet& set,
+                     cudaStream_t st) {
     if (p.n <= 0) return 0;
-    p2g_kernel<<<blocks_for(p.n, kP2GThreads), kP2GThreads, 0, st>>>(p, P, gidx, accum);
+    bin_count_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p, P, pcell, prank, set);
+    return 1;
+}
+
+int launch_bin_order(const SimParams& p, const BinSet& cur, const BinSet& other, int32_t* bstart, int32_t* cstart,
+                     const int32_t* pcell, const int32_t* prank, int32_t* gidx, uint32_t* work, cudaStream_t st) {
+    if (p.n <= 0) return 0;
+    bin_scan_kernel<<<1, kScanThreads, 0, st>>>(cur.bcount, other.bcount, bstart, p.nb + 1, work);
+    const int ctas = std::max(1, std::min(blocks_for((long long)(p.nb + 1) * 32, 128), 148 * 8));
+    cell_scan_kernel<<<ctas, 128, 0, st>>>(cur, bstart, cstart, other);
+    bin_scatter_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p.n, pcell, prank, cstart, gidx, other.nlist);
+    return 3;
+}
+
+int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, const int32_t* bstart, const int32_t* cstart,
+               const BinSet& cur, uint32_t* work, float4* accum, cudaStream_t st) {
+    if (p.n <= 0 || p.nb <= 0) return 0;
+    const int ctas = std::min(p.nb + 1, 148 * kP2GBlocksPerSM);
+    p2g_kernel<<<ctas, kP2GThreads, 0, st>>>(p, P, gidx, bstart, cstart, cur, work, accum);
     return 1;
 }
 
@@ -383,17 +736,25 @@ int launch_grid_update(const SimParams& p, float4* accum, float4* vgrid, const f
     return 1;
 }
 
-int launch_g2p(const SimParams& p, const float* Pin, float* Pout, const int32_t* gidx, const int32_t* sigma,
-               const float4* vgrid, const float* sdf, int32_t* keys_out, uint32_t* health, cudaStream_t st) {
+int launch_g2p(const SimParams& p, const float* Pin, float* Pout, const int32_t* gidx, const int32_t* sig_in,
+               int32_t* sig_out, const float4* vgrid, const float* sdf, int32_t* pcell, int32_t* prank,
+               const BinSet& next, uint32_t* health, cudaStream_t st) {
     if (p.n <= 0) return 0;
-    g2p_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p, Pin, Pout, gidx, sigma, vgrid, sdf, keys_out, health);
+    g2p_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, prank,
+                                                     next, health);
     return 1;
 }
 
-int launch_state_import(const SimParams& p, const float* soa26, float* P, int32_t* sigma, int32_t* rank,
-                        int32_t* keys, bool init_rules, cudaStream_t st) {
+int launch_state_import(const SimParams& p, const float* soa26, float* P, int32_t* sigma, bool init_rules,
+                        cudaStream_t st) {
     if (p.n <= 0) return 0;
-    state_import_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p, soa26, P, sigma, rank, keys, init_rules);
+    state_import_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p, soa26, P, sigma, init_rules);
+    return 1;
+}
+
+int launch_reference_keys(const SimParams& p, const float* P, const int32_t* sigma, int32_t* keys, cudaStream_t st) {
+    if (p.n <= 0) return 0;
+    reference_keys_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p, P, sigma, keys);
     return 1;
 }
 
@@ -411,6 +772,12 @@ int launch_positions_export(const SimParams& p, const float* P, const int32_t* s
 
 int launch_grid_export(const SimParams& p, const float4* grid, float* planes4, cudaStream_t st) {
     grid_export_kernel<<<blocks_for(p.g, 256), 256, 0, st>>>(p, grid, planes4);
+    return 1;
+}
+
+int launch_identity(int32_t* dst, int n, cudaStream_t st) {
+    if (n <= 0) return 0;
+    identity_kernel<<<blocks_for(n, 256), 256, 0, st>>>(dst, n);
     return 1;
 }
 
