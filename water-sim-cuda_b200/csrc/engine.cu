@@ -221,7 +221,8 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
                                           e->gidx, work, st);
     mark(1);
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
-        launches += mpm::launch_p2g(p, e->P[par], e->gidx, e->bstart, e->cstart, e->bins[par], work, e->accum, st);
+        launches += mpm::launch_p2g(p, e->P[par], e->gidx, e->cstart, e->bins[par], work, e->accum, e->d_flags + 1,
+                                    st);
     mark(2);
     if (from <= MPM_STAGE_GRID && upto >= MPM_STAGE_GRID)
         launches += mpm::launch_grid_update(p, e->accum, e->vgrid, e->sdf, st);
@@ -295,8 +296,10 @@ mpm_status sync_and_collect(mpm_engine* e) {
     CK(e, cudaMemcpyAsync(flags, e->d_flags, sizeof(flags), cudaMemcpyDeviceToHost, e->stream));
     CK(e, cudaStreamSynchronize(e->stream));
     e->health |= flags[0];
-    if (flags[1] & mpm::kStatusTimeout) {
+    if (flags[1] & (mpm::kStatusTimeout | mpm::kStatusBinning)) {
         CK(e, cudaMemsetAsync(e->d_flags + 1, 0, sizeof(uint32_t), e->stream));
+        if (flags[1] & mpm::kStatusBinning)
+            return record(e, MPM_ERR_CUDA, "internal error: a particle was not in the cell it was filed under");
         return record(e, MPM_ERR_TIMEOUT, "a bounded device-side wait gave up");
     }
     return MPM_OK;

@@ -68,8 +68,8 @@ int launch_bin_count(const SimParams& p, const float* P, int32_t* pcell, int32_t
 int launch_bin_order(const SimParams& p, const BinSet& cur, const BinSet& other, int32_t* bstart, int32_t* cstart,
                      const int32_t* pcell, const int32_t* prank, int32_t* gidx, uint32_t* work, cudaStream_t st);
 // P2G over the bins listed in `cur`; gidx maps slots of the new order to P.
-int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, const int32_t* bstart, const int32_t* cstart,
-               const BinSet& cur, uint32_t* work, float4* accum, cudaStream_t st);
+int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, const int32_t* cstart, const BinSet& cur,
+               uint32_t* work, float4* accum, uint32_t* status, cudaStream_t st);
 int launch_grid_update(const SimParams& p, float4* accum, float4* vgrid, const float* sdf, cudaStream_t st);
 // G2P: slot j of Pout = particle gidx[j] of Pin advanced one substep;
 // sig_out[j] = sig_in[gidx[j]]; files slot j into `next`.
@@ -101,7 +101,10 @@ int launch_fill(float* dst, long long count, float value, cudaStream_t st);
 int launch_identity(int32_t* dst, int n, cudaStream_t st);
 
 // Device status bits written by kernels with bounded waits.
-enum : uint32_t { kStatusTimeout = 1u << 0 };
+enum : uint32_t {
+    kStatusTimeout = 1u << 0,  // a bounded wait gave up
+    kStatusBinning = 1u << 1   // P2G met a particle outside the cell it was filed under
+};
 
 // Sets the thread's mpm_global_last_error text (engine.cu).
 void set_global_error(const std::string& msg);

@@ -66,30 +66,28 @@ __device__ __forceinline__ int file_particle(int cell, int bin, const BinSet& se
 }
 
 // ------------------------------------------------------------------ P2G ----
-// P2G (p2GTransferScatter, kernels.cu:6-142).  Persistent CTAs of four warps
-// take the bins that hold particles from a work counter.  Warp w walks z-layer
-// w of the bin (8 x 4 base cells), one lane per cell: all particles of a cell
-// scatter to the same 27 nodes, so the lane sums them in registers, reading
-// them through a ring of kRing particles fetched ahead with 16-byte cp.async
-// copies (the gather through gidx costs no registers).  The lane then adds
-// its 27 sums to the warp's footprint, the layer's 10 x 6 x 3 nodes: the 32
-// cells of a layer are distinct, so for one stencil offset the 32 nodes
-// differ and a plain read-add-write per offset is race-free.  A bin with
-// fewer than kSparseBin particles (spray, thin sheets) would leave most lanes
-// idle; there each thread takes one particle and adds to the footprint of
-// the particle's layer with shared atomics.  The four footprints, which
-// overlap in z, are summed into the bin's 10 x 6 x 6 nodes and sent to global
-// memory with one vector reduction per touched node.  Unlike the reference,
-// no partial sum is dropped (it drops shared-tile cells whose partial mass is
-// <= 1e-9, kernels.cu:132).
-constexpr int kP2GThreads = 32 * kBinZ;  // one warp per z-layer of a bin
-constexpr int kP2GBlocksPerSM = 3;
+// P2G (p2GTransferScatter, kernels.cu:6-142).  Persistent single-warp CTAs
+// take work items from a counter; an item is one z-layer (8 x 4 base cells)
+// of a bin that holds particles.  The cells of a layer are consecutive in the
+// particle order, so its particles are one slot range.  Lane = cell: all
+// particles of a cell scatter to the same 27 nodes, so the lane sums them in
+// registers, reading them through a ring of kRing particles fetched ahead with
+// 16-byte cp.async copies (the gather through gidx costs no registers).  The
+// lane then adds its 27 sums to the warp's footprint, the layer's 10 x 6 x 3
+// nodes in shared memory: the 32 cells of a layer are distinct, so for one
+// stencil offset the 32 nodes differ and a plain read-add-write per offset is
+// race-free.  A lane sums at most kCellCap particles of its cell; the rest of
+// a crowded cell (this Tait law resists only expansion, so compressed fluid
+// piles up) is shared by all 32 lanes and reduced across the warp.  The
+// footprint goes to global memory with one vector reduction per touched
+// node.  Unlike the reference, no partial sum is dropped (it drops
+// shared-tile cells whose partial mass is <= 1e-9, kernels.cu:132).
+constexpr int kP2GWarpsPerSM = 12;
 constexpr int kRing = 2;
-constexpr int kGidxStage = 256;  // gather indices of a layer staged in shared memory
-constexpr int kSparseBin = 96;   // bins with fewer particles take one thread per particle
+constexpr int kGidxStage = 256;   // gather indices of a layer staged in shared memory
+constexpr int kCellCap = 12;      // particles of a cell its own lane sums; the rest: whole warp
 constexpr int kTX = kBinX + 2, kTY = kBinY + 2;
-constexpr int kFootNodes = kTX * kTY * 3;             // 180: one layer's stencil footprint
-constexpr int kTileNodes = kTX * kTY * (kBinZ + 2);  // 360: the bin's nodes
+constexpr int kFootNodes = kTX * kTY * 3;  // 180: one layer's stencil footprint
 static_assert(kBinX * kBinY == 32, "one warp covers one z-layer of a bin");
 
 // Spline weights of nodes 0, 1, 2 of one axis at fractional offset f = pos -
@@ -191,102 +189,84 @@ __device__ __forceinline__ void p2g_stencil(const P2GParticle& r, Emit emit) {
     }
 }
 
-__global__ void __launch_bounds__(kP2GThreads, kP2GBlocksPerSM) p2g_kernel(
-    SimParams p, const float* __restrict__ P, const int32_t* __restrict__ gidx, const int32_t* __restrict__ bstart,
-    const int32_t* __restrict__ cstart, BinSet set, uint32_t* __restrict__ work, float4* __restrict__ accum) {
-    __shared__ __align__(16) float4 s_ring[kBinZ][kRing][6][32];
-    __shared__ float4 s_foot[kBinZ][kFootNodes];
-    __shared__ int32_t s_gidx[kBinZ][kGidxStage];
-    __shared__ int s_item;
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int lx = lane % kBinX, ly = lane / kBinX;
-    const int nbins = (int)*reinterpret_cast<volatile uint32_t*>(set.nlist);
-    float4* foot = &s_foot[0][0];
-    for (int q = t; q < kBinZ * kFootNodes; q += kP2GThreads) foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+__global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SimParams p, const float* __restrict__ P,
+                                                                  const int32_t* __restrict__ gidx,
+                                                                  const int32_t* __restrict__ cstart, BinSet set,
+                                                                  uint32_t* __restrict__ work,
+                                                                  float4* __restrict__ accum,
+                                                                  uint32_t* __restrict__ status) {
+    __shared__ __align__(16) float4 s_ring[kRing][6][32];
+    __shared__ float4 s_foot[kFootNodes];
+    __shared__ int32_t s_gidx[kGidxStage];
+    const int lane = threadIdx.x;
+    const int nitems = (int)*reinterpret_cast<volatile uint32_t*>(set.nlist) * kBinZ;
+    for (int q = lane; q < kFootNodes; q += 32) s_foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (;;) {
-        if (t == 0) s_item = (int)atomicAdd(work, 1u);
-        __syncthreads();
-        const int item = s_item;
-        __syncthreads();
-        if (item >= nbins) return;
-        const int bin = __ldg(set.blist + item);
+        int item = 0;
+        if (lane == 0) item = (int)atomicAdd(work, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= nitems) return;
+        const int bin = __ldg(set.blist + item / kBinZ), layer = item % kBinZ;
         if (bin >= p.nb) continue;  // the overflow bin reaches no node
         const int bxi = bin % p.nbx, byi = (bin / p.nbx) % p.nby, bzi = bin / (p.nbx * p.nby);
-        // Node origin of the bin = base cell of its cell (0,0,0).
-        const int ox = bxi * kBinX - 2, oy = byi * kBinY - 2, oz = bzi * kBinZ - 2;
-        const int b0 = __ldg(bstart + bin), bn = __ldg(bstart + bin + 1) - b0;
-        if (bn < kSparseBin) {
-            for (int i = t; i < bn; i += kP2GThreads) {
-                const float4* q = reinterpret_cast<const float4*>(P + (size_t)__ldg(gidx + b0 + i) * kAFloats);
-                const P2GParticle r = p2g_particle(p, __ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3), __ldg(q + 4),
-                                                   __ldg(q + 5));
-                const int tx = r.bx - ox, ty = r.by - oy, tz = r.bz - oz;
-                if ((unsigned)tx < (unsigned)kBinX && (unsigned)ty < (unsigned)kBinY && (unsigned)tz < (unsigned)kBinZ) {
-                    float4* f = s_foot[tz];
-                    p2g_stencil(r, [&](int, int a, int b, int c, float m, float mx, float my, float mz) {
-                        float4* d = &f[(c * kTY + ty + b) * kTX + tx + a];
-                        atomicAdd(&d->x, m);
-                        atomicAdd(&d->y, mx);
-                        atomicAdd(&d->z, my);
-                        atomicAdd(&d->w, mz);
-                    });
-                } else {
-                    // Not filed under this bin (cannot happen while the binning
-                    // matches the state): straight to global memory.
-                    p2g_stencil(r, [&](int, int a, int b, int c, float m, float mx, float my, float mz) {
-                        const long long x = (long long)r.bx + a, y = (long long)r.by + b, z = (long long)r.bz + c;
-                        if (x >= 0 && y >= 0 && z >= 0 && x < p.sx && y < p.sy && z < p.sz)
-                            red_add_v4(accum + node_index(p, (int)x, (int)y, (int)z), m, mx, my, mz);
-                    });
-                }
-            }
-        } else {
-            // Layer `warp`: the cells of a layer are consecutive, so its
-            // particles are slots [l0, l1) of the new order.
-            const int cell = bin * kBinCells + warp * 32 + lane;
-            const int cs = __ldg(cstart + cell);
-            const int cnt = (int)__ldg(set.ccount + cell);
-            const int l0 = __shfl_sync(0xffffffffu, cs, 0);
-            const int l1 = __shfl_sync(0xffffffffu, cs + cnt, 31);
+        // Node origin of the footprint = base cell of lane 0 of this layer.
+        const int ox = bxi * kBinX - 2, oy = byi * kBinY - 2, oz = bzi * kBinZ - 2 + layer;
+        const int cell = bin * kBinCells + layer * 32 + lane;
+        const int cs = __ldg(cstart + cell);
+        const int full = (int)__ldg(set.ccount + cell);
+        const int l0 = __shfl_sync(0xffffffffu, cs, 0);
+        const int l1 = __shfl_sync(0xffffffffu, cs + full, 31);
+        if (l1 == l0) continue;
+        const bool staged = l1 - l0 <= kGidxStage;
+        if (staged)
+            for (int q = lane; q < l1 - l0; q += 32) s_gidx[q] = __ldg(gidx + l0 + q);
+        __syncwarp();
+        // Pass 0: each lane its own cell's first kCellCap particles (slots
+        // cs + s).  Pass k > 0: the k-th crowded cell's further particles,
+        // slot hcs + kCellCap + lane + 32 s, for every lane.  One loop body
+        // serves both; only the flush differs.
+        uint32_t crowded = __ballot_sync(0xffffffffu, full > kCellCap);
+        int first = cs, step = 1, cnt = min(full, kCellCap), target = lane;
+        for (;;) {
+            float am[27], ax[27], ay[27], az[27];
             int maxc = cnt;
 #pragma unroll
             for (int o = 16; o; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
-            if (maxc > 0) {
-                const bool staged = l1 - l0 <= kGidxStage;
-                if (staged)
-                    for (int q = lane; q < l1 - l0; q += 32) s_gidx[warp][q] = __ldg(gidx + l0 + q);
-                __syncwarp();
-                auto src_of = [&](int s) -> const float4* {
-                    const int g = staged ? s_gidx[warp][cs - l0 + s] : __ldg(gidx + cs + s);
-                    return reinterpret_cast<const float4*>(P + (size_t)g * kAFloats);
-                };
-                float4(*ring)[6][32] = s_ring[warp];
+            auto src_of = [&](int s) -> const float4* {
+                const int slot = first + s * step;
+                const int g = staged ? s_gidx[slot - l0] : __ldg(gidx + slot);
+                return reinterpret_cast<const float4*>(P + (size_t)g * kAFloats);
+            };
 #pragma unroll
-                for (int d = 0; d < kRing - 1; ++d) {
-                    if (d < cnt) {
-                        const float4* src = src_of(d);
+            for (int k = 0; k < 27; ++k) am[k] = ax[k] = ay[k] = az[k] = 0.f;
 #pragma unroll
-                        for (int v = 0; v < 6; ++v) cp_async16(&ring[d][v][lane], src + v);
-                    }
-                    cp_async_commit();
+            for (int d = 0; d < kRing - 1; ++d) {
+                if (d < cnt) {
+                    const float4* src = src_of(d);
+#pragma unroll
+                    for (int v = 0; v < 6; ++v) cp_async16(&s_ring[d][v][lane], src + v);
                 }
-                float am[27], ax[27], ay[27], az[27];
+                cp_async_commit();
+            }
+            for (int s = 0; s < maxc; ++s) {
+                const int pf = s + kRing - 1;
+                if (pf < cnt) {
+                    const float4* src = src_of(pf);
 #pragma unroll
-                for (int k = 0; k < 27; ++k) am[k] = ax[k] = ay[k] = az[k] = 0.f;
-                for (int s = 0; s < maxc; ++s) {
-                    const int pf = s + kRing - 1;
-                    if (pf < cnt) {
-                        const float4* src = src_of(pf);
-#pragma unroll
-                        for (int v = 0; v < 6; ++v) cp_async16(&ring[pf % kRing][v][lane], src + v);
-                    }
-                    cp_async_commit();
-                    cp_async_wait<kRing - 1>();
-                    __syncwarp();
-                    if (s < cnt) {
-                        const int sl = s % kRing;
-                        const P2GParticle r = p2g_particle(p, ring[sl][0][lane], ring[sl][1][lane], ring[sl][2][lane],
-                                                           ring[sl][3][lane], ring[sl][4][lane], ring[sl][5][lane]);
+                    for (int v = 0; v < 6; ++v) cp_async16(&s_ring[pf % kRing][v][lane], src + v);
+                }
+                cp_async_commit();
+                cp_async_wait<kRing - 1>();
+                __syncwarp();
+                if (s < cnt) {
+                    const int sl = s % kRing;
+                    const P2GParticle r = p2g_particle(p, s_ring[sl][0][lane], s_ring[sl][1][lane], s_ring[sl][2][lane],
+                                                       s_ring[sl][3][lane], s_ring[sl][4][lane], s_ring[sl][5][lane]);
+                    // Filed under a cell of this layer by construction; a
+                    // mismatch is recorded, never scattered to a wrong node.
+                    if (r.bx - ox != target % kBinX || r.by - oy != target / kBinX || r.bz != oz) {
+                        atomicOr(status, kStatusBinning);
+                    } else {
                         p2g_stencil(r, [&](int k, int, int, int, float m, float mx, float my, float mz) {
                             am[k] += m;
                             ax[k] += mx;
@@ -294,10 +274,13 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GBlocksPerSM) p2g_kernel(
                             az[k] += mz;
                         });
                     }
-                    __syncwarp();
                 }
-                cp_async_wait<0>();
-                float4* f = s_foot[warp];
+                __syncwarp();
+            }
+            cp_async_wait<0>();
+            if (step == 1) {
+                // One lane per cell: distinct nodes for each stencil offset.
+                const int tx = lane % kBinX, ty = lane / kBinX;
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -305,7 +288,7 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GBlocksPerSM) p2g_kernel(
 #pragma unroll
                         for (int a = 0; a < 3; ++a) {
                             const int k = (c * 3 + b) * 3 + a;
-                            float4* d = &f[(c * kTY + ly + b) * kTX + lx + a];
+                            float4* d = &s_foot[(c * kTY + ty + b) * kTX + tx + a];
                             __syncwarp();
                             float4 v = *d;
                             v.x += am[k];
@@ -314,29 +297,59 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GBlocksPerSM) p2g_kernel(
                             v.w += az[k];
                             *d = v;
                         }
-            }
-        }
-        __syncthreads();
-        // Footprint of layer w covers nodes z = w .. w + 2 of the bin.
-        for (int q = t; q < kTileNodes; q += kP2GThreads) {
-            const int x = q % kTX, y = (q / kTX) % kTY, z = q / (kTX * kTY);
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                // A crowded cell's pass: reduce-scatter the 32 lanes' partial
+                // sums (27 nodes x 4, padded to 128 values) by halving them at
+                // each shuffle step, so that lane l ends with node l's totals.
+                float v[128];
 #pragma unroll
-            for (int w = 0; w < kBinZ; ++w) {
-                const int zz = z - w;
-                if (zz < 0 || zz > 2) continue;
-                const float4 u = s_foot[w][(zz * kTY + y) * kTX + x];
-                v.x += u.x;
-                v.y += u.y;
-                v.z += u.z;
-                v.w += u.w;
+                for (int k = 0; k < 32; ++k) {
+                    v[4 * k + 0] = k < 27 ? am[k < 27 ? k : 0] : 0.f;
+                    v[4 * k + 1] = k < 27 ? ax[k < 27 ? k : 0] : 0.f;
+                    v[4 * k + 2] = k < 27 ? ay[k < 27 ? k : 0] : 0.f;
+                    v[4 * k + 3] = k < 27 ? az[k < 27 ? k : 0] : 0.f;
+                }
+#pragma unroll
+                for (int d = 16, h = 64; d >= 1; d >>= 1, h >>= 1) {
+                    const bool upper = (lane & d) != 0;
+#pragma unroll
+                    for (int i = 0; i < h; ++i) {
+                        const float send = upper ? v[i] : v[i + h];
+                        const float keep = upper ? v[i + h] : v[i];
+                        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
+                    }
+                }
+                if (lane < 27) {
+                    const int a = lane % 3, b = (lane / 3) % 3, c = lane / 9;
+                    const int tx = target % kBinX, ty = target / kBinX;
+                    float4* d = &s_foot[(c * kTY + ty + b) * kTX + tx + a];
+                    float4 u = *d;
+                    u.x += v[0];
+                    u.y += v[1];
+                    u.z += v[2];
+                    u.w += v[3];
+                    *d = u;
+                }
             }
-            const int gx = ox + x, gy = oy + y, gz = oz + z;
-            if (node_in_grid(p, gx, gy, gz) && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))  // NaN counts
-                red_add_v4(accum + node_index(p, gx, gy, gz), v.x, v.y, v.z, v.w);
+            __syncwarp();
+            if (!crowded) break;
+            const int src = __ffs(crowded) - 1;
+            crowded &= crowded - 1;
+            const int hcnt = __shfl_sync(0xffffffffu, full, src);
+            first = __shfl_sync(0xffffffffu, cs, src) + kCellCap + lane;
+            step = 32;
+            cnt = max(0, (hcnt - kCellCap - lane + 31) / 32);
+            target = src;
         }
-        __syncthreads();
-        for (int q = t; q < kBinZ * kFootNodes; q += kP2GThreads) foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncwarp();
+        for (int q = lane; q < kFootNodes; q += 32) {
+            const int x = ox + q % kTX, y = oy + (q / kTX) % kTY, z = oz + q / (kTX * kTY);
+            const float4 v = s_foot[q];
+            s_foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (node_in_grid(p, x, y, z) && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))  // NaN counts
+                red_add_v4(accum + node_index(p, x, y, z), v.x, v.y, v.z, v.w);
+        }
+        __syncwarp();
     }
 }
 
@@ -723,11 +736,11 @@ int launch_bin_order(const SimParams& p, const BinSet& cur, const BinSet& other,
     return 3;
 }
 
-int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, const int32_t* bstart, const int32_t* cstart,
-               const BinSet& cur, uint32_t* work, float4* accum, cudaStream_t st) {
+int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, const int32_t* cstart, const BinSet& cur,
+               uint32_t* work, float4* accum, uint32_t* status, cudaStream_t st) {
     if (p.n <= 0 || p.nb <= 0) return 0;
-    const int ctas = std::min(p.nb + 1, 148 * kP2GBlocksPerSM);
-    p2g_kernel<<<ctas, kP2GThreads, 0, st>>>(p, P, gidx, bstart, cstart, cur, work, accum);
+    const int warps = (int)std::min<long long>((long long)(p.nb + 1) * kBinZ, 148LL * kP2GWarpsPerSM);
+    p2g_kernel<<<warps, 32, 0, st>>>(p, P, gidx, cstart, cur, work, accum, status);
     return 1;
 }
 
