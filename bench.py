@@ -58,6 +58,8 @@ def parse_args(argv=None):
     ap.add_argument("--workload", choices=sorted(SEEDS), default="dam_break_2M")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget (0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--advance", type=int, default=0,
+                    help="substeps simulated before the warm-up, to measure a later state of the scene")
     return ap.parse_args(argv)
 
 
@@ -69,8 +71,9 @@ def make_scene(workload: str, rank: int = 0):
     return scenes.dam_break(seed, literal_extent=(workload == "dam_break_5M"))
 
 
-def workload_config(workload, cfg, n, t):
+def workload_config(workload, cfg, n, t, advance=0):
     return {"workload": workload, "grid": f"{cfg.size_x}x{cfg.size_y}x{cfg.size_z}", "particles": n,
+            "advanced_substeps": advance,
             "triangles": t, "substeps_per_step": cfg.substeps,
             "physics": {"padding": cfg.padding, "gravity": cfg.gravity, "dt": cfg.dt, "gamma": cfg.gamma,
                         "compression": cfg.compression, "resolution": cfg.resolution},
@@ -256,6 +259,8 @@ def run_engine(args, rank, world, local):
     eng = mpm_b200.Engine(cfg, device=local)
     eng.init(st)
     eng.init_sdf(tris)
+    if args.advance > 0:
+        eng.step(args.advance)
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
 
     for _ in range(max(args.warmup, 3)):
@@ -331,7 +336,7 @@ def run_engine(args, rank, world, local):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": dict(workload_config(args.workload, cfg, n, len(tris)), parallelism=f"replicas{world}"),
+            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism=f"replicas{world}"),
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk.summary(), "stage_ms_per_substep": {k: round(v, 5) for k, v in per_sub.items()},
             "impl": "engine"}
@@ -356,7 +361,7 @@ def run_reference(args, rank, world, local):
     n, sub = st.shape[1], cfg.substeps
     ref = RefEngine()
     ref.create(cfg, st, tris, f"/tmp/ref_bench_config_{os.getpid()}.txt")
-    ref.step(max(args.warmup, 3) * sub)
+    ref.step(args.advance + max(args.warmup, 3) * sub)
     with ClockSampler(local) as clk:
         ms = ref.time_steps(args.steps * sub)
     ref.destroy()
@@ -364,7 +369,7 @@ def run_reference(args, rank, world, local):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": dict(workload_config(args.workload, cfg, n, len(tris)), parallelism="replicas1"),
+            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism="replicas1"),
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                              "sample": f"{args.steps} frames x {sub} Engine::step() of the reference's own CUDA "

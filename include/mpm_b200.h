@@ -106,14 +106,15 @@ enum {
 typedef struct mpm_stats {
     int64_t substeps;          /* substeps completed since mpm_init_particles */
     int64_t kernel_launches;   /* kernels this engine launched since creation */
-    int64_t sort_passes;       /* radix passes run since creation */
+    int64_t sort_passes;       /* radix-sort passes run since creation (mpm_get_sort) */
     uint32_t health;           /* MPM_HEALTH_* bits seen since init or the last reset */
     uint32_t reserved;
 } mpm_stats;
 
 /* Stages of one substep, for mpm_substep_partial. */
 enum {
-    MPM_STAGE_SORT = 1,  /* Morton keys + stable sort (engine.cu:92-102) */
+    MPM_STAGE_SORT = 1,  /* particle ordering (the reference's Morton keys + stable sort,
+                          * engine.cu:92-102); here the ordering by stencil cell */
     MPM_STAGE_P2G = 2,   /* + grid clear + particle-to-grid scatter (kernels.cu:6-142, 311-318) */
     MPM_STAGE_GRID = 3,  /* + grid update (kernels.cu:144-196) */
     MPM_STAGE_G2P = 4    /* + grid-to-particle gather: a full substep (kernels.cu:199-280) */
@@ -256,8 +257,12 @@ mpm_status mpm_get_sdf(mpm_engine* engine, float* sdf_host);
  * reference's sortParticles leaves them (engine.cu:92-102): keys_host[i] is
  * setKeys' key of particle i (original order, kernels.cu:361-371) and
  * perm_host[j] is the original index of the j-th particle in stable
- * ascending key order (d_values after thrust::sort_by_key).  Either pointer
- * may be NULL.  Before any substep: keys of the current state, identity. */
+ * ascending key order (d_values after thrust::sort_by_key).  The engine
+ * itself orders particles by stencil cell, which its P2G needs, not by this
+ * key; it computes the reference's keys and permutation on request,
+ * bit-exactly, from the state that substep started from (kept until the
+ * next substep).  Either pointer may be NULL.  Before any substep: keys of
+ * the current state, identity. */
 mpm_status mpm_get_sort(mpm_engine* engine, int32_t* keys_host, int32_t* perm_host);
 
 /* Counters and accumulated health bits; reset_health clears the bits. */

@@ -374,45 +374,71 @@ __global__ void __launch_bounds__(256) bin_count_kernel(SimParams p, const float
 
 // bstart[i] = sum of bcount[0..i) over nbins = nb + 1 bins, bstart[nbins] =
 // n.  Also zeroes the bin counters of the other set and the P2G work
-// counter.  One CTA.
+// counter.  One CTA, in chunks of kScanChunk counters: coalesced loads into
+// shared memory, a contiguous run of kScanPer counters per thread, a block
+// scan of the run sums, coalesced stores.
 constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 8;
+constexpr int kScanChunk = kScanThreads * kScanPer;
 __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(const uint32_t* __restrict__ bcount,
                                                                 uint32_t* __restrict__ bclear,
                                                                 int32_t* __restrict__ bstart, int nbins,
                                                                 uint32_t* __restrict__ work) {
+    __shared__ int s_val[kScanChunk];
     __shared__ int s_warp[kScanThreads / 32];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int per = (nbins + kScanThreads - 1) / kScanThreads;
-    const int lo = min(t * per, nbins), hi = min(lo + per, nbins);
-    int sum = 0;
-    for (int i = lo; i < hi; ++i) sum += (int)bcount[i];
-    int incl = sum;
+    int carry = 0;
+    for (int c0 = 0; c0 < nbins; c0 += kScanChunk) {
+        const int m = min(kScanChunk, nbins - c0);
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        int w = s_warp[lane];
+        for (int k = 0; k < kScanPer; ++k) {
+            const int i = k * kScanThreads + t;
+            s_val[i] = i < m ? (int)bcount[c0 + i] : 0;
+            if (i < m) bclear[c0 + i] = 0u;
+        }
+        __syncthreads();
+        int v[kScanPer], sum = 0;
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            v[k] = s_val[t * kScanPer + k];
+            sum += v[k];
+        }
+        int incl = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
         }
-        s_warp[lane] = w;
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            int w = s_warp[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            s_warp[lane] = w;
+        }
+        __syncthreads();
+        int run = carry + incl - sum + (warp > 0 ? s_warp[warp - 1] : 0);
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            s_val[t * kScanPer + k] = run;
+            run += v[k];
+        }
+        const int total = s_warp[31];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            const int i = k * kScanThreads + t;
+            if (i < m) bstart[c0 + i] = s_val[i];
+        }
+        carry += total;
+        __syncthreads();
     }
-    __syncthreads();
-    int run = incl - sum + (warp > 0 ? s_warp[warp - 1] : 0);
-    for (int i = lo; i < hi; ++i) {
-        const int c = (int)bcount[i];
-        bstart[i] = run;
-        run += c;
-        bclear[i] = 0u;
-    }
-    if (t == kScanThreads - 1) {
-        bstart[nbins] = s_warp[31];
+    if (t == 0) {
+        bstart[nbins] = carry;
         *work = 0u;
     }
 }
