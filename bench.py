@@ -43,7 +43,7 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-substeps/s"
 UNIT = "particle-substeps/s"
 FALLBACK_HBM_GBS = 6650.0
-SEEDS = {"dam_break_2M": 1235, "dam_break_5M": 1235, "sphere_drop": 1234}
+SEEDS = {"dam_break_2M": 1235, "dam_break_5M": 1235, "sphere_drop": 1234, "scale_256": 1236, "batched_64": 1237}
 # Algorithmic bytes per unit (FP32 reference state): per particle and per grid
 # node of each stage, from the hot-path scope table of this project.
 ALGO_BYTES = {"sort": (16, 0), "p2g": (108, 16), "grid": (0, 48), "g2p": (148, 12)}
@@ -68,11 +68,18 @@ def make_scene(workload: str, rank: int = 0):
     seed = SEEDS[workload] + 1000 * rank
     if workload == "sphere_drop":
         return scenes.sphere_drop(seed)
+    if workload == "scale_256":
+        return scenes.scale_scene(seed)
+    if workload == "batched_64":
+        return scenes.batched_scenes(64, seed)
     return scenes.dam_break(seed, literal_extent=(workload == "dam_break_5M"))
 
 
 def workload_config(workload, cfg, n, t, advance=0):
-    return {"workload": workload, "grid": f"{cfg.size_x}x{cfg.size_y}x{cfg.size_z}", "particles": n,
+    grid = f"{cfg.size_x}x{cfg.size_y}x{cfg.size_z}"
+    if workload == "batched_64":
+        grid = "64 independent scenes, 32-96 nodes per axis each, one launch per stage"
+    return {"workload": workload, "grid": grid, "particles": n,
             "advanced_substeps": advance,
             "triangles": t, "substeps_per_step": cfg.substeps,
             "physics": {"padding": cfg.padding, "gravity": cfg.gravity, "dt": cfg.dt, "gamma": cfg.gamma,
@@ -254,11 +261,29 @@ def run_engine(args, rank, world, local):
     dist = Dist(world, local)
     import mpm_b200
 
-    cfg, st, tris = make_scene(args.workload, rank)
-    n, sub = st.shape[1], cfg.substeps
-    eng = mpm_b200.Engine(cfg, device=local)
-    eng.init(st)
-    eng.init_sdf(tris)
+    scene = make_scene(args.workload, rank)
+    batched = isinstance(scene, list)
+    if batched:
+        cfgs = [c for c, _, _ in scene]
+        states = [x for _, x, _ in scene]
+        tri_sets = [t for _, _, t in scene]
+        cfg, st, tris = cfgs[0], None, np.concatenate(tri_sets)
+        n, sub = sum(x.shape[1] for x in states), cfg.substeps
+
+        def make_engine(state_list):
+            e = mpm_b200.Batch(cfgs, device=local)
+            e.init_all(state_list)
+            for k, t in enumerate(tri_sets):
+                if len(t):
+                    e.init_scene_sdf(k, t)
+            return e
+        eng = make_engine(states)
+    else:
+        cfg, st, tris = scene
+        n, sub = st.shape[1], cfg.substeps
+        eng = mpm_b200.Engine(cfg, device=local)
+        eng.init(st)
+        eng.init_sdf(tris)
     if args.advance > 0:
         eng.step(args.advance)
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
@@ -291,9 +316,12 @@ def run_engine(args, rank, world, local):
     stage_ms, cnt = eng.stage_times()
     eng.set_stage_timing(0)
     per_sub = {k: v / max(cnt, 1) for k, v in stage_ms.items()}
-    grid = eng.get_grid()
-    g_dense = cfg.grid_number
-    g_active = int(np.count_nonzero(grid[0] > 0))
+    if batched:
+        g_dense = sum(c.grid_number for c in cfgs)
+        g_active = sum(int(np.count_nonzero(eng.scene_grid(k)[0] > 0)) for k in range(len(cfgs)))
+    else:
+        g_dense = cfg.grid_number
+        g_active = int(np.count_nonzero(eng.get_grid()[0] > 0))
     peak, peak_kind = load_peaks()
     dom = max(("p2g", "g2p", "grid", "sort"), key=lambda k: per_sub[k])
     bpp, bpn = ALGO_BYTES[dom]
@@ -308,18 +336,32 @@ def run_engine(args, rank, world, local):
     # End to end through the C ABI with host buffers (pinned).
     e2e = None
     if not args.no_e2e:
-        st_pin = torch.from_numpy(np.ascontiguousarray(st)).pin_memory().numpy()
-        pos_pin = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
-        eng2 = mpm_b200.Engine(cfg, device=local)
-        eng2.init_sdf(tris)
-        eng2.init(st_pin)  # warm the allocation path once
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        if batched:
+            st_pins = [pin(x) for x in states]
+            pos_pins = [torch.empty((x.shape[1], 3), dtype=torch.float32).pin_memory().numpy() for x in states]
+            eng2 = make_engine(st_pins)
+            init2 = lambda: eng2.init_all(st_pins)
+
+            def read_positions():
+                for k, buf in enumerate(pos_pins):
+                    lib.mpm_scene_get_positions(eng2._h, k, buf.ctypes.data)
+        else:
+            st_pin = pin(st)
+            pos_pin = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
+            eng2 = mpm_b200.Engine(cfg, device=local)
+            eng2.init_sdf(tris)
+            init2 = lambda: eng2.init(st_pin)
+            read_positions = lambda: eng2.get_positions(pos_pin)
+        lib = mpm_b200.lib
+        init2()  # warm the allocation path once
         eng2.step(sub)
         dist.barrier()
         t0 = time.perf_counter()
-        eng2.init(st_pin)
+        init2()
         for _ in range(args.steps):
             eng2.step(sub)
-            eng2.get_positions(pos_pin)
+            read_positions()
         t1 = time.perf_counter()
         dist.barrier()
         e2e_s = dist.max(t1 - t0)
@@ -330,7 +372,7 @@ def run_engine(args, rank, world, local):
         eng2.close()
 
     cpu = None
-    if rank == 0 and world == 1 and args.cpu_seconds > 0:
+    if rank == 0 and world == 1 and args.cpu_seconds > 0 and not batched:
         cpu = cpu_baseline(args.workload, args.cpu_seconds, eng.get_sdf())
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -355,21 +397,32 @@ def run_reference(args, rank, world, local):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_engine.so was not built "
                           "(the reference sources were absent at build time)"}))
         return
+    import numpy as np
     import torch
     torch.cuda.set_device(local)
-    cfg, st, tris = make_scene(args.workload, 0)
-    n, sub = st.shape[1], cfg.substeps
+    scene = make_scene(args.workload, 0)
+    # The reference runs one scene per process (a __constant__ config); a
+    # batch is timed scene after scene, over the scenes whose grid it can run
+    # (its grid kernels have no bounds check: node count a multiple of 256).
+    runs = scene if isinstance(scene, list) else [scene]
+    runs = [r for r in runs if r[0].grid_number % 256 == 0]
+    cfg, tris = runs[0][0], np.concatenate([r[2] for r in runs])
+    sub = cfg.substeps
+    n, ms = 0, 0.0
     ref = RefEngine()
-    ref.create(cfg, st, tris, f"/tmp/ref_bench_config_{os.getpid()}.txt")
-    ref.step(args.advance + max(args.warmup, 3) * sub)
     with ClockSampler(local) as clk:
-        ms = ref.time_steps(args.steps * sub)
+        for c, st, t in runs:
+            ref.create(c, st, t, f"/tmp/ref_bench_config_{os.getpid()}.txt")
+            ref.step(args.advance + max(args.warmup, 3) * sub)
+            ms += ref.time_steps(args.steps * sub)
+            n += st.shape[1]
     ref.destroy()
     value = n * sub * args.steps / (ms / 1e3)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism="replicas1"),
+            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism="replicas1",
+                           reference_scenes=len(runs)),
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                              "sample": f"{args.steps} frames x {sub} Engine::step() of the reference's own CUDA "

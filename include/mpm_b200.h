@@ -170,6 +170,8 @@ mpm_status mpm_create(const mpm_config* cfg, int32_t device, mpm_engine** out);
 void mpm_destroy(mpm_engine* engine);
 
 /* Replaces Engine::init(int n, float* h_buffer) (engine.cu:45-52, 72-83).
+ * For an engine of one scene (mpm_create); batches use
+ * mpm_init_particles_batch.
  * soa26_host holds 26*n floats (layout above).  Unlike the reference, the
  * buffer is COPIED, not adopted (the reference delete[]s it in ~Engine).
  * As the reference's initFMatrices does (kernels.cu:349-358), F00/F11/F22
@@ -229,7 +231,8 @@ int64_t mpm_num_particles(const mpm_engine* engine);
  * 26*n state in ORIGINAL particle order (the order of mpm_init_particles). */
 mpm_status mpm_get_state(mpm_engine* engine, float* soa26_host);
 
-/* Loads a 26*n state saved by mpm_get_state (checkpoint resume).  n must
+/* Loads a 26*n state saved by mpm_get_state (checkpoint resume), for an
+ * engine of one scene.  n must
  * equal the engine's particle count.  Unlike mpm_init_particles no plane is
  * overwritten.  VOL and MASS must each hold one value for all particles, as
  * every state the reference can produce does (initFMatrices sets them and
@@ -288,6 +291,41 @@ const char* mpm_last_error(const mpm_engine* engine);
 /* Text of the last error of a call that had no engine to record it on
  * (mpm_create, mpm_sort_particles_device).  Thread-local.  Never NULL. */
 const char* mpm_global_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* Batches of independent scenes                                        */
+/* ------------------------------------------------------------------ */
+
+/* No counterpart in the reference (one scene per process, its config lives
+ * in a process-global __constant__).  An engine of nscenes independent
+ * scenes, each with its own grid size, physics constants, particles and
+ * obstacles, on one device.  Every substep stage runs as one launch over all
+ * scenes, and mpm_step / mpm_step_async / mpm_synchronize /
+ * mpm_substep_partial / mpm_set_stage_timing act on all of them.  An engine
+ * from mpm_create is the batch of one scene, and the single-scene calls
+ * (mpm_init_sdf, mpm_get_state, ...) address its scene 0. */
+mpm_status mpm_create_batch(const mpm_config* cfgs, int32_t nscenes, int32_t device, mpm_engine** out);
+
+/* Number of scenes (0 for NULL). */
+int32_t mpm_num_scenes(const mpm_engine* engine);
+
+/* Engine::init for every scene at once: scene s gets counts[s] particles
+ * from soa26_host[s] (26 * counts[s] floats, copied; the same rules as
+ * mpm_init_particles).  counts[s] may be 0. */
+mpm_status mpm_init_particles_batch(mpm_engine* engine, const int64_t* counts, const float* const* soa26_host);
+
+/* Per-scene forms of mpm_init_sdf, mpm_num_particles, mpm_get_state,
+ * mpm_positions_device, mpm_get_positions, mpm_get_grid, mpm_get_sdf and
+ * mpm_get_sort.  scene outside [0, mpm_num_scenes) is
+ * MPM_ERR_INVALID_ARGUMENT (0 / NULL for the value-returning ones). */
+mpm_status mpm_scene_init_sdf(mpm_engine* engine, int32_t scene, const float* triangles_host, int64_t t);
+int64_t mpm_scene_num_particles(const mpm_engine* engine, int32_t scene);
+mpm_status mpm_scene_get_state(mpm_engine* engine, int32_t scene, float* soa26_host);
+const float* mpm_scene_positions_device(mpm_engine* engine, int32_t scene);
+mpm_status mpm_scene_get_positions(mpm_engine* engine, int32_t scene, float* xyz_host);
+mpm_status mpm_scene_get_grid(mpm_engine* engine, int32_t scene, float* grid4_host);
+mpm_status mpm_scene_get_sdf(mpm_engine* engine, int32_t scene, float* sdf_host);
+mpm_status mpm_scene_get_sort(mpm_engine* engine, int32_t scene, int32_t* keys_host, int32_t* perm_host);
 
 /* ------------------------------------------------------------------ */
 /* Stand-alone device operators                                         */

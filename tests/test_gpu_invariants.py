@@ -123,3 +123,28 @@ def test_checkpoint_round_trip(gpu_ok, mpm):
     # with the continued one to a small multiple of the one-substep tolerance.
     d = np.abs(resumed[0:3].astype(np.float64) - cont[0:3]).max()
     assert d <= 1e-3, d
+
+
+def test_scale_256_invariants(gpu_ok, mpm):
+    """The at-scale scene (256^3, three seeded water boxes, sphere, torus and
+    box obstacles; 6,856,623 particles): after a few substeps the grid holds
+    the particle mass, the state stays finite, and the reference's keys and
+    permutation (recomputed by mpm_get_sort) are the stable sort of the keys
+    of the state the substep started from."""
+    from mpm_b200 import scenes
+    cfg, st, tris = scenes.scale_scene(1236)
+    n = st.shape[1]
+    with mpm.Engine(cfg) as eng:
+        eng.init(st)
+        eng.init_sdf(tris)
+        eng.step(3)
+        before = eng.get_buffer()
+        eng.substep_partial(mpm.STAGE_P2G)
+        mass = float(eng.get_grid()[0].astype(np.float64).sum())
+        eng.substep_partial(mpm.STAGE_G2P)
+        keys, perm = eng.get_sort()
+        after = eng.get_buffer()
+    assert abs(mass - n) <= 1e-6 * n
+    assert np.isfinite(after[0:24]).all()
+    assert np.array_equal(keys, morton_reference(before[0:3]))
+    assert np.array_equal(perm, stable_sort_reference(keys))

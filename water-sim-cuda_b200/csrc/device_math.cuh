@@ -33,6 +33,9 @@ enum ParticleField : int {
 constexpr int kBinX = 8, kBinY = 4, kBinZ = 4;
 constexpr int kBinCells = kBinX * kBinY * kBinZ;  // 128
 
+// One scene.  An engine holds one or more independent scenes whose arrays are
+// concatenated: particle slots, grid nodes, cells and bins are numbered
+// globally, and poff/goff/coff/boff give where this scene's part begins.
 struct SimParams {
     int sx, sy, sz;       // SIZE_X/Y/Z
     int padding;          // PADDING
@@ -42,7 +45,32 @@ struct SimParams {
     int g;                // grid nodes sx*sy*sz
     int nbx, nby, nbz;    // bin blocks per axis: ceil((SIZE+2) / kBin*)
     int nb;               // bin blocks; bin nb holds the particles that reach no node
+    long long poff;       // first particle slot
+    long long goff;       // first grid node
+    long long coff;       // first cell: (nb + 1) * kBinCells cells per scene
+    long long boff;       // first bin entry: nb + 2 entries per scene
 };
+
+// The scenes of an engine on the device: prm[s], and the prefix arrays
+// poff[s] / goff[s] (S + 1 entries each) that map a global particle slot or
+// grid node to its scene.
+struct SceneTable {
+    const SimParams* prm;
+    const long long* poff;
+    const long long* goff;
+    int count;
+};
+
+// Largest s with first[s] <= i (first[0] = 0, first is non-decreasing).
+__device__ __forceinline__ int scene_of(const long long* __restrict__ first, int count, long long i) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(first + mid) <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
 
 // Node index z*SX*SY + y*SX + x (getGridIdx, common.cuh:131-134).
 __device__ __forceinline__ int node_index(const SimParams& p, int x, int y, int z) {

@@ -2,7 +2,12 @@
 //
 // Restates the reference's `Engine` (engine.h:14-43, engine.cu:36-114) and
 // the config upload (config.cu:5-8, Simulation.cpp:56-77) with per-engine
-// state: one device, one stream, and a CUDA graph per substep parity.
+// state: one device, one stream, and a CUDA graph per substep parity.  An
+// engine holds one or more independent scenes (the batched form): their
+// particle, grid, cell and bin arrays are concatenated, a device table of
+// SimParams carries each scene's constants and offsets, and every substep
+// stage is one launch over all scenes.  The reference's single Engine is an
+// engine of one scene.
 //
 // Particle order.  The reference never moves particle data: every substep it
 // sorts (Morton key, 0..n-1) and gathers through the permutation, so that
@@ -12,10 +17,10 @@
 // cell scatter to the same 27 nodes.  A substep from parity p, state P[p]
 // filed into counter set p:
 //   bin order: bin and cell starts from set p, gidx[new slot] = old slot;
-//   P2G: one warp per listed bin, lane = cell, reading P[p] through gidx;
+//   P2G: one warp per (bin, layer) item, lane = cell, reading P[p] via gidx;
 //   grid update;
 //   G2P reads P[p] through gidx and writes P[1-p] at the new slot, i.e. the
-//       state is regrouped for free, carries sigma (slot -> original index)
+//       state is regrouped for free, carries sigma (slot -> original slot)
 //       along and files every particle into set 1-p for the next substep.
 // The reference's keys and sort permutation of a substep are a function of
 // the state the substep started from, which stays intact in P[p] until the
@@ -50,30 +55,42 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 struct mpm_engine {
     int device = 0;
     cudaStream_t stream = nullptr;
-    mpm_config cfg{};
-    SimParams prm{};
     std::string last_error;
     uint32_t checks = 0;
 
+    // Scenes: config, constants and offsets (host copy of the device table).
+    std::vector<mpm_config> cfg;
+    std::vector<SimParams> prm;
+    int scenes = 0;
+    long long g_total = 0;      // grid nodes
+    long long cells_total = 0;  // cells of all bins (incl. each overflow bin)
+    long long bins_total = 0;   // bin entries: nb + 2 per scene
+    long long bins_scan = 0;    // bins scanned: nb + 1 per scene
+    SimParams* d_prm = nullptr;
+    long long* d_poff = nullptr;     // S + 1 first slots
+    long long* d_goff = nullptr;     // S + 1 first nodes
+    long long* d_itemoff = nullptr;  // S + 1 first P2G items
+    mpm::SceneTable table{};
+
     bool initialized = false;
-    int n = 0;
+    long long n = 0;  // particles of all scenes
+    int max_n = 0;    // largest scene
     float* P[2] = {nullptr, nullptr};        // particle-major state, 24 floats per particle
-    int32_t* sigma[2] = {nullptr, nullptr};  // slot -> original index
+    int32_t* sigma[2] = {nullptr, nullptr};  // slot -> original slot (global)
     int32_t* gidx = nullptr;                 // new slot -> old slot of the current binning
-    int32_t* pcell = nullptr;                // cell of each slot of P[parity]
+    int32_t* pcell = nullptr;                // global cell of each slot of P[parity]
     int32_t* prank = nullptr;                // rank within its cell
-    int32_t* ref_keys = nullptr;             // mpm_get_sort: keys in original order
+    int32_t* ref_keys = nullptr;             // mpm_get_sort: keys in original order (one scene)
     int32_t* ref_perm = nullptr;             // mpm_get_sort: stable sort permutation
     void* sort_mem = nullptr;
-    mpm::SortScratch sort;
-    float* pos_out = nullptr;
+    float* pos_out = nullptr;  // float3 positions, all scenes, original order
 
     float4* accum = nullptr;
     float4* vgrid = nullptr;
     float* sdf = nullptr;
     // Binning: two counter sets (cell counts, bin counts, bin lists) in one
     // allocation, the bin and cell starts of the current order, and ctl =
-    // {list length of set 0, of set 1, P2G work counter}.
+    // {list lengths of set 0 (S), of set 1 (S), P2G work, G2P work}.
     void* bins_mem = nullptr;
     mpm::BinSet bins[2] = {};
     int32_t* bstart = nullptr;
@@ -165,10 +182,11 @@ mpm_status ensure_staging(mpm_engine* e, size_t bytes) {
     return MPM_OK;
 }
 
-mpm_status alloc_particles(mpm_engine* e, int n) {
+mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_bytes) {
     free_particles(e);
     e->n = n;
-    const size_t cap = (size_t)std::max(n, 1);
+    e->max_n = max_n;
+    const size_t cap = (size_t)std::max(n, 1LL);
     const size_t ibytes = cap * sizeof(int32_t);
     for (int k = 0; k < 2; ++k) {
         CK(e, cudaMalloc(&e->P[k], cap * mpm::kAFloats * sizeof(float)));
@@ -177,59 +195,77 @@ mpm_status alloc_particles(mpm_engine* e, int n) {
     CK(e, cudaMalloc(&e->gidx, ibytes));
     CK(e, cudaMalloc(&e->pcell, ibytes));
     CK(e, cudaMalloc(&e->prank, ibytes));
-    CK(e, cudaMalloc(&e->ref_keys, ibytes));
-    CK(e, cudaMalloc(&e->ref_perm, ibytes));
-    CK(e, cudaMalloc(&e->sort_mem, mpm::sort_scratch_bytes(std::max(n, 1))));
-    mpm::sort_scratch_carve(e->sort_mem, std::max(n, 1), &e->sort);
-    e->sort.n = n;
-    CK(e, cudaMalloc(&e->pos_out, (size_t)std::max(n, 1) * 3 * sizeof(float)));
+    const size_t sbytes = (size_t)std::max(max_n, 1) * sizeof(int32_t);
+    CK(e, cudaMalloc(&e->ref_keys, sbytes));
+    CK(e, cudaMalloc(&e->ref_perm, sbytes));
+    CK(e, cudaMalloc(&e->sort_mem, sort_bytes));
+    CK(e, cudaMalloc(&e->pos_out, cap * 3 * sizeof(float)));
     return MPM_OK;
 }
 
-// Bytes of the two counter sets: per set (nb + 1) * kBinCells cell counts,
-// nb + 1 bin counts and nb + 1 list entries, rounded up to 256 bytes so that
-// the second set's cell counts stay 16-byte aligned for vector access.
-size_t bins_set_words(const SimParams& p) { return align_up((size_t)(p.nb + 1) * (mpm::kBinCells + 2), 64); }
-size_t bins_bytes(const SimParams& p) { return 2 * bins_set_words(p) * sizeof(uint32_t); }
+// Words of one counter set: cell counts, bin counts and bin lists, rounded up
+// to 256 bytes so that the second set's cell counts stay 16-byte aligned for
+// vector access.
+size_t bins_set_words(const mpm_engine* e) {
+    return align_up((size_t)e->cells_total + 2 * (size_t)e->bins_total, 64);
+}
+size_t bins_bytes(const mpm_engine* e) { return 2 * bins_set_words(e) * sizeof(uint32_t); }
 
 void carve_bins(mpm_engine* e) {
-    const SimParams& p = e->prm;
     uint32_t* base = static_cast<uint32_t*>(e->bins_mem);
     for (int k = 0; k < 2; ++k) {
-        uint32_t* s = base + k * bins_set_words(p);  // cell counts first: 16-byte aligned
+        uint32_t* s = base + k * bins_set_words(e);  // cell counts first: 16-byte aligned
         e->bins[k].ccount = s;
-        e->bins[k].bcount = s + (size_t)(p.nb + 1) * mpm::kBinCells;
-        e->bins[k].blist = reinterpret_cast<int32_t*>(e->bins[k].bcount + (p.nb + 1));
-        e->bins[k].nlist = e->ctl + k;
+        e->bins[k].bcount = s + e->cells_total;
+        e->bins[k].blist = reinterpret_cast<int32_t*>(e->bins[k].bcount + e->bins_total);
+        e->bins[k].nlist = e->ctl + k * e->scenes;
     }
 }
 
+// Uploads the scene table (after the particle offsets change).
+mpm_status upload_table(mpm_engine* e) {
+    std::vector<long long> poff(e->scenes + 1), goff(e->scenes + 1);
+    for (int s = 0; s < e->scenes; ++s) {
+        poff[s] = e->prm[s].poff;
+        goff[s] = e->prm[s].goff;
+    }
+    poff[e->scenes] = e->n;
+    goff[e->scenes] = e->g_total;
+    CK(e, cudaMemcpyAsync(e->d_prm, e->prm.data(), e->scenes * sizeof(SimParams), cudaMemcpyHostToDevice, e->stream));
+    CK(e, cudaMemcpyAsync(e->d_poff, poff.data(), poff.size() * sizeof(long long), cudaMemcpyHostToDevice, e->stream));
+    CK(e, cudaMemcpyAsync(e->d_goff, goff.data(), goff.size() * sizeof(long long), cudaMemcpyHostToDevice, e->stream));
+    // Pageable host copies: wait before the vectors go out of scope.
+    CK(e, cudaStreamSynchronize(e->stream));
+    return MPM_OK;
+}
+
 // Enqueues stages `from`..`upto` (MPM_STAGE_*) of one substep from parity
-// `par`.  With `marks` (only while capturing a graph), records marks[0..4]
-// as event-record nodes before the sort and after each stage.
+// `par`, for all scenes.  With `marks` (only while capturing a graph), records
+// marks[0..4] as event-record nodes before the ordering and after each stage.
 int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_t* marks = nullptr) {
-    const SimParams& p = e->prm;
+    const mpm::SceneTable& sc = e->table;
     cudaStream_t st = e->stream;
     auto mark = [&](int k) {
         if (marks) cudaEventRecordWithFlags(marks[k], st, cudaEventRecordExternal);
     };
     int launches = 0;
-    uint32_t* work = e->ctl + 2;
+    uint32_t* work = e->ctl + 2 * e->scenes;
     mark(0);
     if (from <= MPM_STAGE_SORT && upto >= MPM_STAGE_SORT)
-        launches += mpm::launch_bin_order(p, e->bins[par], e->bins[1 - par], e->bstart, e->cstart, e->pcell, e->prank,
-                                          e->gidx, work, st);
+        launches += mpm::launch_bin_order(sc, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart, e->cstart,
+                                          e->pcell, e->prank, e->gidx, e->d_itemoff, work, st);
     mark(1);
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
-        launches += mpm::launch_p2g(p, e->P[par], e->gidx, e->cstart, e->bins[par], work, e->accum, e->d_flags + 1,
-                                    st);
+        launches += mpm::launch_p2g(sc, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par], e->d_itemoff,
+                                    work, e->accum, e->d_flags + 1, st);
     mark(2);
     if (from <= MPM_STAGE_GRID && upto >= MPM_STAGE_GRID)
-        launches += mpm::launch_grid_update(p, e->accum, e->vgrid, e->sdf, st);
+        launches += mpm::launch_grid_update(sc, e->prm[0], e->g_total, e->accum, e->vgrid, e->sdf, st);
     mark(3);
     if (from <= MPM_STAGE_G2P && upto >= MPM_STAGE_G2P)
-        launches += mpm::launch_g2p(p, e->P[par], e->P[1 - par], e->gidx, e->sigma[par], e->sigma[1 - par], e->vgrid,
-                                    e->sdf, e->pcell, e->prank, e->bins[1 - par], e->d_flags, st);
+        launches += mpm::launch_g2p(sc, e->prm[0], e->n, e->P[par], e->P[1 - par], e->gidx, e->sigma[par],
+                                    e->sigma[1 - par],
+                                    e->vgrid, e->sdf, e->pcell, e->prank, e->bins[1 - par], e->d_flags, st);
     mark(4);
     return launches;
 }
@@ -319,35 +355,42 @@ bool finite_cfg(const mpm_config* c) {
            std::isfinite(c->compression) && std::isfinite(c->resolution);
 }
 
-// Uploads a 26-plane host state and imports it (init_rules: Engine::init).
-mpm_status load_state(mpm_engine* e, const float* soa26_host, bool init_rules) {
-    const int n = e->n;
-    if (n > 0) {
-        const size_t bytes = (size_t)MPM_PARTICLE_PLANES * n * sizeof(float);
-        mpm_status s = ensure_staging(e, bytes);
-        if (s != MPM_OK) return s;
-        CK(e, cudaMemcpyAsync(e->staging, soa26_host, bytes, cudaMemcpyHostToDevice, e->stream));
-        e->kernel_launches += mpm::launch_state_import(e->prm, e->staging, e->P[0], e->sigma[0], init_rules, e->stream);
+// Uploads each scene's 26-plane host state and imports it (init_rules:
+// Engine::init), then files all particles into counter set 0.
+mpm_status load_states(mpm_engine* e, const float* const* soa26_host, bool init_rules) {
+    for (int s = 0; s < e->scenes; ++s) {
+        const SimParams& p = e->prm[s];
+        if (p.n <= 0) continue;
+        const size_t bytes = (size_t)MPM_PARTICLE_PLANES * p.n * sizeof(float);
+        mpm_status st = ensure_staging(e, bytes);
+        if (st != MPM_OK) return st;
+        CK(e, cudaMemcpyAsync(e->staging, soa26_host[s], bytes, cudaMemcpyHostToDevice, e->stream));
+        e->kernel_launches += mpm::launch_state_import(p, e->staging, e->P[0] + p.poff * mpm::kAFloats,
+                                                       e->sigma[0] + p.poff, init_rules, e->stream);
         CK(e, cudaGetLastError());
     }
     // Both counter sets empty, then the imported particles filed into set 0.
-    CK(e, cudaMemsetAsync(e->bins_mem, 0, bins_bytes(e->prm), e->stream));
-    CK(e, cudaMemsetAsync(e->ctl, 0, 4 * sizeof(uint32_t), e->stream));
-    e->kernel_launches += mpm::launch_bin_count(e->prm, e->P[0], e->pcell, e->prank, e->bins[0], e->stream);
+    CK(e, cudaMemsetAsync(e->bins_mem, 0, bins_bytes(e), e->stream));
+    CK(e, cudaMemsetAsync(e->ctl, 0, (2 * e->scenes + 2) * sizeof(uint32_t), e->stream));
+    e->kernel_launches += mpm::launch_bin_count(e->table, e->n, e->P[0], e->pcell, e->prank, e->bins[0], e->stream);
     CK(e, cudaGetLastError());
     e->parity = 0;
     e->sort_src = kNoSort;
     e->partial_stage = 0;
-    CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
-    CK(e, cudaMemsetAsync(e->vgrid, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
+    CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->g_total * sizeof(float4), e->stream));
+    CK(e, cudaMemsetAsync(e->vgrid, 0, (size_t)e->g_total * sizeof(float4), e->stream));
     CK(e, cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(uint32_t), e->stream));
     e->accum_dirty = false;
     e->grid_view = GridView::kVelocity;
     e->health = 0;
-    e->kernel_launches += mpm::launch_positions_export(e->prm, e->P[0], e->sigma[0], e->pos_out, e->stream);
+    for (int s = 0; s < e->scenes; ++s) {
+        const SimParams& p = e->prm[s];
+        e->kernel_launches += mpm::launch_positions_export(p, e->P[0] + p.poff * mpm::kAFloats, e->sigma[0] + p.poff,
+                                                           e->pos_out + p.poff * 3, e->stream);
+    }
     CK(e, cudaGetLastError());
-    mpm_status s = capture_graphs(e);
-    if (s != MPM_OK) return s;
+    mpm_status st = capture_graphs(e);
+    if (st != MPM_OK) return st;
     e->initialized = true;
     return sync_and_collect(e);
 }
@@ -359,12 +402,30 @@ mpm_status enter(mpm_engine* e) {
     return MPM_OK;
 }
 
+mpm_status enter_scene(mpm_engine* e, int32_t scene) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (scene < 0 || scene >= e->scenes) return record(e, MPM_ERR_INVALID_ARGUMENT, "scene index out of range");
+    return MPM_OK;
+}
+
+mpm_status export_positions(mpm_engine* e) {
+    for (int sc = 0; sc < e->scenes; ++sc) {
+        const SimParams& p = e->prm[sc];
+        e->kernel_launches += mpm::launch_positions_export(p, e->P[e->parity] + p.poff * mpm::kAFloats,
+                                                           e->sigma[e->parity] + p.poff, e->pos_out + p.poff * 3,
+                                                           e->stream);
+    }
+    CK(e, cudaGetLastError());
+    return MPM_OK;
+}
+
 mpm_status run_steps(mpm_engine* e, int32_t nsub) {
     if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
     if (nsub < 0) return record(e, MPM_ERR_INVALID_ARGUMENT, "nsub < 0");
     e->partial_stage = 0;  // a partial substep in progress is discarded (it changed no particle)
     if (e->accum_dirty) {
-        CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
+        CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->g_total * sizeof(float4), e->stream));
         e->accum_dirty = false;
     }
     for (int s = 0; s < nsub; ++s) {
@@ -383,10 +444,141 @@ mpm_status run_steps(mpm_engine* e, int32_t nsub) {
         ++e->substeps;
     }
     if (nsub > 0) e->grid_view = GridView::kVelocity;
-    e->kernel_launches +=
-        mpm::launch_positions_export(e->prm, e->P[e->parity], e->sigma[e->parity], e->pos_out, e->stream);
-    CK(e, cudaGetLastError());
+    return export_positions(e);
+}
+
+// Engine with `count` scenes; grid arrays, counter sets and the scene table
+// are allocated here, particle arrays by the first init.
+mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, mpm_engine** out) {
+    g_global_error.clear();
+    if (!cfgs || !out) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "configs and out must be non-NULL");
+    *out = nullptr;
+    if (count <= 0 || count > 65536) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "scene count out of range");
+    long long g_total = 0, cells_total = 0, bins_total = 0;
+    std::vector<SimParams> prm(count);
+    for (int s = 0; s < count; ++s) {
+        const mpm_config* cfg = cfgs + s;
+        if (cfg->size_x <= 0 || cfg->size_y <= 0 || cfg->size_z <= 0)
+            return record(nullptr, MPM_ERR_BAD_CONFIG, "SIZE_X/Y/Z must be positive");
+        const long long g = (long long)cfg->size_x * cfg->size_y * cfg->size_z;
+        if (g > 0x7fffffffLL) return record(nullptr, MPM_ERR_BAD_CONFIG, "grid has more than 2^31-1 nodes");
+        if (!finite_cfg(cfg)) return record(nullptr, MPM_ERR_BAD_CONFIG, "a float parameter is not finite");
+        SimParams& p = prm[s];
+        p.sx = cfg->size_x;
+        p.sy = cfg->size_y;
+        p.sz = cfg->size_z;
+        p.padding = cfg->padding;
+        p.gravity = cfg->gravity;
+        p.dt = cfg->dt;
+        p.gamma = cfg->gamma;
+        p.compression = cfg->compression;
+        p.pvol = cfg->resolution * cfg->resolution * cfg->resolution;  // kernels.cu:356
+        p.pmass = 1.0f;                                                // kernels.cu:357
+        p.n = 0;
+        p.g = (int)g;
+        p.nbx = (cfg->size_x + 2 + mpm::kBinX - 1) / mpm::kBinX;
+        p.nby = (cfg->size_y + 2 + mpm::kBinY - 1) / mpm::kBinY;
+        p.nbz = (cfg->size_z + 2 + mpm::kBinZ - 1) / mpm::kBinZ;
+        p.nb = p.nbx * p.nby * p.nbz;
+        p.poff = 0;
+        p.goff = g_total;
+        p.coff = cells_total;
+        p.boff = bins_total;
+        g_total += g;
+        cells_total += (long long)(p.nb + 1) * mpm::kBinCells;
+        bins_total += p.nb + 2;
+    }
+    if (cells_total >= 0x7fffffffLL || g_total >= (1LL << 40))
+        return record(nullptr, MPM_ERR_BAD_CONFIG, "grids too large for the cell index");
+
+    int ndev = 0;
+    cudaError_t err = cudaGetDeviceCount(&ndev);
+    if (err != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return record(nullptr, MPM_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(err));
+    }
+    if (device < 0 || device >= ndev) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "device index out of range");
+    cudaDeviceProp prop;
+    err = cudaGetDeviceProperties(&prop, device);
+    if (err != cudaSuccess) return cuda_fail(nullptr, err, "cudaGetDeviceProperties");
+    if (prop.major != 10 || prop.minor != 0)
+        return record(nullptr, MPM_ERR_NO_DEVICE,
+                      std::string("this library is built for sm_100a (B200); device is ") + prop.name);
+
+    mpm_engine* e = new mpm_engine();
+    e->device = device;
+    e->cfg.assign(cfgs, cfgs + count);
+    e->prm = prm;
+    e->scenes = count;
+    e->g_total = g_total;
+    e->cells_total = cells_total;
+    e->bins_total = bins_total;
+    e->bins_scan = bins_total - count;
+
+    auto fail = [&](mpm_status s) {
+        g_global_error = e->last_error;
+        mpm_destroy(e);
+        return s;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(cuda_fail(e, cudaGetLastError(), "cudaSetDevice"));
+    if ((err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(cuda_fail(e, err, "cudaStreamCreate"));
+    if ((err = cudaMalloc(&e->accum, (size_t)g_total * sizeof(float4))) != cudaSuccess ||
+        (err = cudaMalloc(&e->vgrid, (size_t)g_total * sizeof(float4))) != cudaSuccess ||
+        (err = cudaMalloc(&e->sdf, (size_t)g_total * sizeof(float))) != cudaSuccess ||
+        (err = cudaMalloc(&e->d_flags, 2 * sizeof(uint32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->ctl, (2 * count + 2) * sizeof(uint32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->bins_mem, bins_bytes(e))) != cudaSuccess ||
+        (err = cudaMalloc(&e->bstart, (size_t)bins_total * sizeof(int32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->cstart, (size_t)cells_total * sizeof(int32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->d_prm, count * sizeof(SimParams))) != cudaSuccess ||
+        (err = cudaMalloc(&e->d_poff, (count + 1) * sizeof(long long))) != cudaSuccess ||
+        (err = cudaMalloc(&e->d_goff, (count + 1) * sizeof(long long))) != cudaSuccess ||
+        (err = cudaMalloc(&e->d_itemoff, (count + 1) * sizeof(long long))) != cudaSuccess)
+        return fail(cuda_fail(e, err, "cudaMalloc(grid)"));
+    carve_bins(e);
+    e->table.prm = e->d_prm;
+    e->table.poff = e->d_poff;
+    e->table.goff = e->d_goff;
+    e->table.count = count;
+    cudaMemsetAsync(e->accum, 0, (size_t)g_total * sizeof(float4), e->stream);
+    cudaMemsetAsync(e->vgrid, 0, (size_t)g_total * sizeof(float4), e->stream);
+    cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(uint32_t), e->stream);
+    // An empty triangle list leaves sqrt(1e30) everywhere (kernels.cu:289,299).
+    e->kernel_launches += mpm::launch_fill(e->sdf, g_total, sqrtf(1e30f), e->stream);
+    if ((err = cudaGetLastError()) != cudaSuccess) return fail(cuda_fail(e, err, "sdf fill"));
+    if (upload_table(e) != MPM_OK) return fail(MPM_ERR_CUDA);
+    if ((err = cudaStreamSynchronize(e->stream)) != cudaSuccess) return fail(cuda_fail(e, err, "create sync"));
+    *out = e;
     return MPM_OK;
+}
+
+mpm_status init_all(mpm_engine* e, const int64_t* counts, const float* const* soa26_host) {
+    long long total = 0;
+    int max_n = 0;
+    size_t sort_bytes = mpm::sort_scratch_bytes(1);  // radix-sort scratch of mpm_get_sort: any scene
+    for (int s = 0; s < e->scenes; ++s) {
+        if (counts[s] < 0 || counts[s] > 0x7fffffffLL - 64) return record(e, MPM_ERR_INVALID_ARGUMENT, "n out of range");
+        if (counts[s] > 0 && !soa26_host[s]) return record(e, MPM_ERR_INVALID_ARGUMENT, "soa26_host is NULL");
+        total += counts[s];
+        max_n = std::max(max_n, (int)counts[s]);
+        sort_bytes = std::max(sort_bytes, mpm::sort_scratch_bytes(std::max((int)counts[s], 1)));
+    }
+    if (total > 0x7fffffffLL - 64) return record(e, MPM_ERR_INVALID_ARGUMENT, "more than 2^31 particles in total");
+    mpm_status st = alloc_particles(e, total, max_n, sort_bytes);
+    if (st != MPM_OK) return st;
+    long long off = 0;
+    for (int s = 0; s < e->scenes; ++s) {
+        SimParams& p = e->prm[s];
+        p.n = (int)counts[s];
+        p.poff = off;
+        p.pvol = e->cfg[s].resolution * e->cfg[s].resolution * e->cfg[s].resolution;
+        p.pmass = 1.0f;
+        off += counts[s];
+    }
+    if ((st = upload_table(e)) != MPM_OK) return st;
+    e->substeps = 0;
+    return load_states(e, soa26_host, true);
 }
 
 }  // namespace
@@ -414,80 +606,14 @@ extern "C" const char* mpm_status_string(mpm_status s) {
 }
 
 extern "C" mpm_status mpm_create(const mpm_config* cfg, int32_t device, mpm_engine** out) {
-    g_global_error.clear();
-    if (!cfg || !out) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "cfg and out must be non-NULL");
-    *out = nullptr;
-    if (cfg->size_x <= 0 || cfg->size_y <= 0 || cfg->size_z <= 0)
-        return record(nullptr, MPM_ERR_BAD_CONFIG, "SIZE_X/Y/Z must be positive");
-    const long long g = (long long)cfg->size_x * cfg->size_y * cfg->size_z;
-    if (g > 0x7fffffffLL) return record(nullptr, MPM_ERR_BAD_CONFIG, "grid has more than 2^31-1 nodes");
-    if (!finite_cfg(cfg)) return record(nullptr, MPM_ERR_BAD_CONFIG, "a float parameter is not finite");
-
-    int count = 0;
-    cudaError_t err = cudaGetDeviceCount(&count);
-    if (err != cudaSuccess || count == 0) {
-        cudaGetLastError();
-        return record(nullptr, MPM_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(err));
-    }
-    if (device < 0 || device >= count) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "device index out of range");
-    cudaDeviceProp prop;
-    err = cudaGetDeviceProperties(&prop, device);
-    if (err != cudaSuccess) return cuda_fail(nullptr, err, "cudaGetDeviceProperties");
-    if (prop.major != 10 || prop.minor != 0)
-        return record(nullptr, MPM_ERR_NO_DEVICE,
-                      std::string("this library is built for sm_100a (B200); device is ") + prop.name);
-
-    mpm_engine* e = new mpm_engine();
-    e->device = device;
-    e->cfg = *cfg;
-    SimParams& p = e->prm;
-    p.sx = cfg->size_x;
-    p.sy = cfg->size_y;
-    p.sz = cfg->size_z;
-    p.padding = cfg->padding;
-    p.gravity = cfg->gravity;
-    p.dt = cfg->dt;
-    p.gamma = cfg->gamma;
-    p.compression = cfg->compression;
-    p.pvol = cfg->resolution * cfg->resolution * cfg->resolution;  // kernels.cu:356
-    p.pmass = 1.0f;                                                // kernels.cu:357
-    p.n = 0;
-    p.g = (int)g;
-    p.nbx = (cfg->size_x + 2 + mpm::kBinX - 1) / mpm::kBinX;
-    p.nby = (cfg->size_y + 2 + mpm::kBinY - 1) / mpm::kBinY;
-    p.nbz = (cfg->size_z + 2 + mpm::kBinZ - 1) / mpm::kBinZ;
-    if ((long long)p.nbx * p.nby * p.nbz >= 0x7fffffffLL / mpm::kBinCells - 1)
-        return record(nullptr, MPM_ERR_BAD_CONFIG, "grid too large for the cell index");
-    p.nb = p.nbx * p.nby * p.nbz;
-
-    auto fail = [&](mpm_status s) {
-        g_global_error = e->last_error;
-        mpm_destroy(e);
-        return s;
-    };
-    if (cudaSetDevice(device) != cudaSuccess) return fail(cuda_fail(e, cudaGetLastError(), "cudaSetDevice"));
-    if ((err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess)
-        return fail(cuda_fail(e, err, "cudaStreamCreate"));
-    if ((err = cudaMalloc(&e->accum, (size_t)g * sizeof(float4))) != cudaSuccess ||
-        (err = cudaMalloc(&e->vgrid, (size_t)g * sizeof(float4))) != cudaSuccess ||
-        (err = cudaMalloc(&e->sdf, (size_t)g * sizeof(float))) != cudaSuccess ||
-        (err = cudaMalloc(&e->d_flags, 2 * sizeof(uint32_t))) != cudaSuccess ||
-        (err = cudaMalloc(&e->bins_mem, bins_bytes(p))) != cudaSuccess ||
-        (err = cudaMalloc(&e->bstart, (size_t)(p.nb + 2) * sizeof(int32_t))) != cudaSuccess ||
-        (err = cudaMalloc(&e->cstart, (size_t)(p.nb + 1) * mpm::kBinCells * sizeof(int32_t))) != cudaSuccess ||
-        (err = cudaMalloc(&e->ctl, 4 * sizeof(uint32_t))) != cudaSuccess)
-        return fail(cuda_fail(e, err, "cudaMalloc(grid)"));
-    carve_bins(e);
-    cudaMemsetAsync(e->accum, 0, (size_t)g * sizeof(float4), e->stream);
-    cudaMemsetAsync(e->vgrid, 0, (size_t)g * sizeof(float4), e->stream);
-    cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(uint32_t), e->stream);
-    // An empty triangle list leaves sqrt(1e30) everywhere (kernels.cu:289,299).
-    e->kernel_launches += mpm::launch_fill(e->sdf, g, sqrtf(1e30f), e->stream);
-    if ((err = cudaGetLastError()) != cudaSuccess) return fail(cuda_fail(e, err, "sdf fill"));
-    if ((err = cudaStreamSynchronize(e->stream)) != cudaSuccess) return fail(cuda_fail(e, err, "create sync"));
-    *out = e;
-    return MPM_OK;
+    return create_engine(cfg, 1, device, out);
 }
+
+extern "C" mpm_status mpm_create_batch(const mpm_config* cfgs, int32_t nscenes, int32_t device, mpm_engine** out) {
+    return create_engine(cfgs, nscenes, device, out);
+}
+
+extern "C" int32_t mpm_num_scenes(const mpm_engine* e) { return e ? e->scenes : 0; }
 
 extern "C" void mpm_destroy(mpm_engine* e) {
     if (!e) return;
@@ -502,6 +628,10 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->bstart);
     free_dev(e->cstart);
     free_dev(e->ctl);
+    free_dev(e->d_prm);
+    free_dev(e->d_poff);
+    free_dev(e->d_goff);
+    free_dev(e->d_itemoff);
     free_dev(e->d_flags);
     free_dev(e->staging);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -511,20 +641,22 @@ extern "C" void mpm_destroy(mpm_engine* e) {
 extern "C" mpm_status mpm_init_particles(mpm_engine* e, int64_t n, const float* soa26_host) {
     mpm_status s = enter(e);
     if (s != MPM_OK) return s;
-    if (n < 0 || n > 0x7fffffffLL - 64) return record(e, MPM_ERR_INVALID_ARGUMENT, "n out of range");
-    if (n > 0 && !soa26_host) return record(e, MPM_ERR_INVALID_ARGUMENT, "soa26_host is NULL");
-    if ((s = alloc_particles(e, (int)n)) != MPM_OK) return s;
-    e->prm.n = (int)n;
-    e->prm.pvol = e->cfg.resolution * e->cfg.resolution * e->cfg.resolution;
-    e->prm.pmass = 1.0f;
-    e->substeps = 0;
-    return load_state(e, soa26_host, true);
+    if (e->scenes != 1) return record(e, MPM_ERR_UNSUPPORTED, "engine holds several scenes: use mpm_init_particles_batch");
+    return init_all(e, &n, &soa26_host);
+}
+
+extern "C" mpm_status mpm_init_particles_batch(mpm_engine* e, const int64_t* counts, const float* const* soa26_host) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!counts || !soa26_host) return record(e, MPM_ERR_INVALID_ARGUMENT, "counts and soa26_host must be non-NULL");
+    return init_all(e, counts, soa26_host);
 }
 
 extern "C" mpm_status mpm_set_state(mpm_engine* e, int64_t n, const float* soa26_host) {
     mpm_status s = enter(e);
     if (s != MPM_OK) return s;
     if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (e->scenes != 1) return record(e, MPM_ERR_UNSUPPORTED, "mpm_set_state serves engines of one scene");
     if (n != e->n) return record(e, MPM_ERR_INVALID_ARGUMENT, "n differs from the engine's particle count");
     if (n > 0 && !soa26_host) return record(e, MPM_ERR_INVALID_ARGUMENT, "soa26_host is NULL");
     if (n > 0) {
@@ -534,19 +666,22 @@ extern "C" mpm_status mpm_set_state(mpm_engine* e, int64_t n, const float* soa26
             if (std::memcmp(&vol[i], &vol[0], sizeof(float)) != 0 || std::memcmp(&mass[i], &mass[0], sizeof(float)) != 0)
                 return record(e, MPM_ERR_UNSUPPORTED, "VOL and MASS must each be uniform over the particles");
         }
-        e->prm.pvol = vol[0];
-        e->prm.pmass = mass[0];
+        e->prm[0].pvol = vol[0];
+        e->prm[0].pmass = mass[0];
+        if ((s = upload_table(e)) != MPM_OK) return s;
     }
-    return load_state(e, soa26_host, false);
+    return load_states(e, &soa26_host, false);
 }
 
-extern "C" mpm_status mpm_init_sdf(mpm_engine* e, const float* tris, int64_t t) {
-    mpm_status s = enter(e);
+extern "C" mpm_status mpm_scene_init_sdf(mpm_engine* e, int32_t scene, const float* tris, int64_t t) {
+    mpm_status s = enter_scene(e, scene);
     if (s != MPM_OK) return s;
     if (t < 0 || t > 0x7fffffffLL / 9) return record(e, MPM_ERR_INVALID_ARGUMENT, "triangle count out of range");
     if (t > 0 && !tris) return record(e, MPM_ERR_INVALID_ARGUMENT, "triangles_host is NULL");
+    const SimParams& p = e->prm[scene];
+    float* sdf = e->sdf + p.goff;
     if (t == 0) {
-        e->kernel_launches += mpm::launch_fill(e->sdf, e->prm.g, sqrtf(1e30f), e->stream);
+        e->kernel_launches += mpm::launch_fill(sdf, p.g, sqrtf(1e30f), e->stream);
         CK(e, cudaGetLastError());
         CK(e, cudaStreamSynchronize(e->stream));
         return MPM_OK;
@@ -559,12 +694,16 @@ extern "C" mpm_status mpm_init_sdf(mpm_engine* e, const float* tris, int64_t t) 
     cudaError_t err = cudaMemsetAsync(d_tris, 0, align_up(bytes, 16) + 16, e->stream);
     if (err == cudaSuccess) err = cudaMemcpyAsync(d_tris, tris, bytes, cudaMemcpyHostToDevice, e->stream);
     if (err == cudaSuccess) {
-        e->kernel_launches += mpm::launch_sdf_build(e->prm, d_tris, (int)t, e->sdf, e->d_flags + 1, e->stream);
+        e->kernel_launches += mpm::launch_sdf_build(p, d_tris, (int)t, sdf, e->d_flags + 1, e->stream);
         err = cudaGetLastError();
     }
     const mpm_status s2 = err != cudaSuccess ? cuda_fail(e, err, "sdf build") : sync_and_collect(e);
     cudaFree(d_tris);
     return s2;
+}
+
+extern "C" mpm_status mpm_init_sdf(mpm_engine* e, const float* tris, int64_t t) {
+    return mpm_scene_init_sdf(e, 0, tris, t);
 }
 
 extern "C" mpm_status mpm_step_async(mpm_engine* e, int32_t nsub) {
@@ -597,7 +736,7 @@ extern "C" mpm_status mpm_substep_partial(mpm_engine* e, int32_t upto) {
     int from = e->partial_stage + 1;
     if (upto <= e->partial_stage) from = MPM_STAGE_SORT;
     if (from == MPM_STAGE_SORT && e->accum_dirty) {
-        CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->prm.g * sizeof(float4), e->stream));
+        CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->g_total * sizeof(float4), e->stream));
         e->accum_dirty = false;
     }
     e->kernel_launches += enqueue_substep(e, e->parity, from, upto);
@@ -615,9 +754,7 @@ extern "C" mpm_status mpm_substep_partial(mpm_engine* e, int32_t upto) {
         e->partial_stage = 0;
         e->parity ^= 1;
         ++e->substeps;
-        e->kernel_launches +=
-            mpm::launch_positions_export(e->prm, e->P[e->parity], e->sigma[e->parity], e->pos_out, e->stream);
-        CK(e, cudaGetLastError());
+        if ((s = export_positions(e)) != MPM_OK) return s;
     }
     if ((s = sync_and_collect(e)) != MPM_OK) return s;
     return upto == MPM_STAGE_G2P ? check_health(e) : MPM_OK;
@@ -629,76 +766,102 @@ extern "C" mpm_status mpm_set_checks(mpm_engine* e, uint32_t flags) {
     return MPM_OK;
 }
 
-extern "C" int64_t mpm_num_particles(const mpm_engine* e) { return (e && e->initialized) ? e->n : 0; }
+extern "C" int64_t mpm_scene_num_particles(const mpm_engine* e, int32_t scene) {
+    if (!e || !e->initialized || scene < 0 || scene >= e->scenes) return 0;
+    return e->prm[scene].n;
+}
 
-extern "C" mpm_status mpm_get_state(mpm_engine* e, float* out) {
-    mpm_status s = enter(e);
+extern "C" int64_t mpm_num_particles(const mpm_engine* e) { return mpm_scene_num_particles(e, 0); }
+
+extern "C" mpm_status mpm_scene_get_state(mpm_engine* e, int32_t scene, float* out) {
+    mpm_status s = enter_scene(e, scene);
     if (s != MPM_OK) return s;
     if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
-    if (e->n == 0) return MPM_OK;
+    const SimParams& p = e->prm[scene];
+    if (p.n == 0) return MPM_OK;
     if (!out) return record(e, MPM_ERR_INVALID_ARGUMENT, "soa26_host is NULL");
-    const size_t bytes = (size_t)MPM_PARTICLE_PLANES * e->n * sizeof(float);
+    const size_t bytes = (size_t)MPM_PARTICLE_PLANES * p.n * sizeof(float);
     if ((s = ensure_staging(e, bytes)) != MPM_OK) return s;
-    e->kernel_launches += mpm::launch_state_export(e->prm, e->P[e->parity], e->sigma[e->parity], e->staging, e->stream);
+    e->kernel_launches += mpm::launch_state_export(p, e->P[e->parity] + p.poff * mpm::kAFloats,
+                                                   e->sigma[e->parity] + p.poff, e->staging, e->stream);
     CK(e, cudaGetLastError());
     CK(e, cudaMemcpyAsync(out, e->staging, bytes, cudaMemcpyDeviceToHost, e->stream));
     CK(e, cudaStreamSynchronize(e->stream));
     return MPM_OK;
 }
 
-extern "C" const float* mpm_positions_device(mpm_engine* e) {
-    return (e && e->initialized) ? e->pos_out : nullptr;
+extern "C" mpm_status mpm_get_state(mpm_engine* e, float* out) { return mpm_scene_get_state(e, 0, out); }
+
+extern "C" const float* mpm_scene_positions_device(mpm_engine* e, int32_t scene) {
+    if (!e || !e->initialized || scene < 0 || scene >= e->scenes) return nullptr;
+    return e->pos_out + e->prm[scene].poff * 3;
 }
 
-extern "C" mpm_status mpm_get_positions(mpm_engine* e, float* xyz) {
-    mpm_status s = enter(e);
+extern "C" const float* mpm_positions_device(mpm_engine* e) { return mpm_scene_positions_device(e, 0); }
+
+extern "C" mpm_status mpm_scene_get_positions(mpm_engine* e, int32_t scene, float* xyz) {
+    mpm_status s = enter_scene(e, scene);
     if (s != MPM_OK) return s;
     if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
-    if (e->n == 0) return MPM_OK;
+    const SimParams& p = e->prm[scene];
+    if (p.n == 0) return MPM_OK;
     if (!xyz) return record(e, MPM_ERR_INVALID_ARGUMENT, "xyz_host is NULL");
-    CK(e, cudaMemcpyAsync(xyz, e->pos_out, (size_t)e->n * 3 * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    CK(e, cudaMemcpyAsync(xyz, e->pos_out + p.poff * 3, (size_t)p.n * 3 * sizeof(float), cudaMemcpyDeviceToHost,
+                          e->stream));
     CK(e, cudaStreamSynchronize(e->stream));
     return MPM_OK;
 }
 
-extern "C" mpm_status mpm_get_grid(mpm_engine* e, float* out) {
-    mpm_status s = enter(e);
+extern "C" mpm_status mpm_get_positions(mpm_engine* e, float* xyz) { return mpm_scene_get_positions(e, 0, xyz); }
+
+extern "C" mpm_status mpm_scene_get_grid(mpm_engine* e, int32_t scene, float* out) {
+    mpm_status s = enter_scene(e, scene);
     if (s != MPM_OK) return s;
     if (!out) return record(e, MPM_ERR_INVALID_ARGUMENT, "grid4_host is NULL");
-    const size_t bytes = (size_t)MPM_GRID_PLANES * e->prm.g * sizeof(float);
+    const SimParams& p = e->prm[scene];
+    const size_t bytes = (size_t)MPM_GRID_PLANES * p.g * sizeof(float);
     if ((s = ensure_staging(e, bytes)) != MPM_OK) return s;
-    const float4* src = e->grid_view == GridView::kAccum ? e->accum : e->vgrid;
-    e->kernel_launches += mpm::launch_grid_export(e->prm, src, e->staging, e->stream);
+    const float4* src = (e->grid_view == GridView::kAccum ? e->accum : e->vgrid) + p.goff;
+    e->kernel_launches += mpm::launch_grid_export(p, src, e->staging, e->stream);
     CK(e, cudaGetLastError());
     CK(e, cudaMemcpyAsync(out, e->staging, bytes, cudaMemcpyDeviceToHost, e->stream));
     CK(e, cudaStreamSynchronize(e->stream));
     return MPM_OK;
 }
 
-extern "C" mpm_status mpm_get_sdf(mpm_engine* e, float* out) {
-    mpm_status s = enter(e);
+extern "C" mpm_status mpm_get_grid(mpm_engine* e, float* out) { return mpm_scene_get_grid(e, 0, out); }
+
+extern "C" mpm_status mpm_scene_get_sdf(mpm_engine* e, int32_t scene, float* out) {
+    mpm_status s = enter_scene(e, scene);
     if (s != MPM_OK) return s;
     if (!out) return record(e, MPM_ERR_INVALID_ARGUMENT, "sdf_host is NULL");
-    CK(e, cudaMemcpyAsync(out, e->sdf, (size_t)e->prm.g * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    const SimParams& p = e->prm[scene];
+    CK(e, cudaMemcpyAsync(out, e->sdf + p.goff, (size_t)p.g * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
     CK(e, cudaStreamSynchronize(e->stream));
     return MPM_OK;
 }
 
-extern "C" mpm_status mpm_get_sort(mpm_engine* e, int32_t* keys_host, int32_t* perm_host) {
-    mpm_status s = enter(e);
+extern "C" mpm_status mpm_get_sdf(mpm_engine* e, float* out) { return mpm_scene_get_sdf(e, 0, out); }
+
+extern "C" mpm_status mpm_scene_get_sort(mpm_engine* e, int32_t scene, int32_t* keys_host, int32_t* perm_host) {
+    mpm_status s = enter_scene(e, scene);
     if (s != MPM_OK) return s;
     if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
-    if (e->n == 0) return MPM_OK;
-    const size_t bytes = (size_t)e->n * sizeof(int32_t);
+    const SimParams& p = e->prm[scene];
+    if (p.n == 0) return MPM_OK;
+    const size_t bytes = (size_t)p.n * sizeof(int32_t);
     // The state the most recent substep started from (intact until the next
     // substep), or the current state before any substep.
     const int src = e->sort_src == kNoSort ? e->parity : e->sort_src;
-    e->kernel_launches += mpm::launch_reference_keys(e->prm, e->P[src], e->sigma[src], e->ref_keys, e->stream);
+    e->kernel_launches += mpm::launch_reference_keys(p, e->P[src] + p.poff * mpm::kAFloats, e->sigma[src] + p.poff,
+                                                     e->ref_keys, e->stream);
     if (e->sort_src == kNoSort) {
-        e->kernel_launches += mpm::launch_identity(e->ref_perm, e->n, e->stream);
+        e->kernel_launches += mpm::launch_identity(e->ref_perm, p.n, e->stream);
     } else {
-        e->kernel_launches += mpm::launch_radix_sort(e->ref_keys, e->n, e->sort, e->ref_perm, nullptr, nullptr,
-                                                     nullptr, e->stream);
+        mpm::SortScratch sort;
+        mpm::sort_scratch_carve(e->sort_mem, p.n, &sort);
+        e->kernel_launches +=
+            mpm::launch_radix_sort(e->ref_keys, p.n, sort, e->ref_perm, nullptr, nullptr, nullptr, e->stream);
         e->sort_passes += 4;
     }
     CK(e, cudaGetLastError());
@@ -706,6 +869,10 @@ extern "C" mpm_status mpm_get_sort(mpm_engine* e, int32_t* keys_host, int32_t* p
     if (perm_host) CK(e, cudaMemcpyAsync(perm_host, e->ref_perm, bytes, cudaMemcpyDeviceToHost, e->stream));
     CK(e, cudaStreamSynchronize(e->stream));
     return MPM_OK;
+}
+
+extern "C" mpm_status mpm_get_sort(mpm_engine* e, int32_t* keys_host, int32_t* perm_host) {
+    return mpm_scene_get_sort(e, 0, keys_host, perm_host);
 }
 
 extern "C" mpm_status mpm_get_stats(mpm_engine* e, mpm_stats* st, int32_t reset_health) {

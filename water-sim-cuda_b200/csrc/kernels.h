@@ -45,13 +45,15 @@ int launch_radix_sort(const int32_t* keys, int n, const SortScratch& s, int32_t*
                       const int32_t* rank_in, int32_t* gidx, cudaStream_t st);
 
 // ------------------------------------------------------------- substep ----
-// P is the particle-major state (device_math.cuh), ordered by cell of the
-// binning that produced it.  pcell[j]/prank[j] are the cell of slot j and its
-// rank among the cell's particles.  A counter set holds, for the cells
-// (nb + 1) * kBinCells of the grid, their particle counts, the bin counts
-// (nb + 1), and the list of bins that hold particles (nb + 1 entries + its
-// length).  Two sets alternate: a substep orders the particles by one and
-// its G2P fills the other, which that substep clears first.
+// The substep kernels work on all scenes of a SceneTable at once; particle
+// slots, cells and bins are global (device_math.cuh).  P is the
+// particle-major state, ordered by cell of the binning that produced it.
+// pcell[j]/prank[j] are the global cell of slot j and its rank among the
+// cell's particles.  A counter set holds the cell counts (global cells), the
+// bin counts and the per-scene lists of bins that hold particles (global bin
+// entries: nb + 2 per scene), and the per-scene list lengths nlist[scene].
+// Two sets alternate: a substep orders the particles by one and its G2P
+// fills the other, which that substep clears first.
 struct BinSet {
     uint32_t* ccount;
     uint32_t* bcount;
@@ -59,31 +61,39 @@ struct BinSet {
     uint32_t* nlist;
 };
 
-// Files the particles of P in slot order into an empty set (after an import).
-int launch_bin_count(const SimParams& p, const float* P, int32_t* pcell, int32_t* prank, const BinSet& set,
-                     cudaStream_t st);
-// Order by cell from set `cur`: bstart (nb + 2 bin starts), cstart (first slot
-// of every cell of a listed bin), gidx[new slot] = old slot; clears `other`
-// and the P2G work counter.
-int launch_bin_order(const SimParams& p, const BinSet& cur, const BinSet& other, int32_t* bstart, int32_t* cstart,
-                     const int32_t* pcell, const int32_t* prank, int32_t* gidx, uint32_t* work, cudaStream_t st);
-// P2G over the bins listed in `cur`; gidx maps slots of the new order to P.
-int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, const int32_t* cstart, const BinSet& cur,
-               uint32_t* work, float4* accum, uint32_t* status, cudaStream_t st);
-int launch_grid_update(const SimParams& p, float4* accum, float4* vgrid, const float* sdf, cudaStream_t st);
+// Files the n particles of P (all scenes, slot order) into an empty set.
+int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t* pcell, int32_t* prank,
+                     const BinSet& set, cudaStream_t st);
+// Order by cell from set `cur`: bstart (global first slots of every bin), cstart
+// (first slot of every cell of a listed bin), gidx[new slot] = old slot, and
+// itemoff (the P2G work items of each scene: kBinZ per listed bin, prefix,
+// S + 1 entries); clears `other` and the work counters work[0..1].
+// bins_total: sum over scenes of nb + 1.
+int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
+                     int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
+                     long long* itemoff, uint32_t* work, cudaStream_t st);
+// P2G over the items of `cur`; gidx maps slots of the new order to P.
+int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
+               const int32_t* cstart, const BinSet& cur, const long long* itemoff, uint32_t* work, float4* accum,
+               uint32_t* status, cudaStream_t st);
+// p0: the parameters of scene 0, used directly when the table holds one scene.
+int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
+                       const float* sdf, cudaStream_t st);
 // G2P: slot j of Pout = particle gidx[j] of Pin advanced one substep;
 // sig_out[j] = sig_in[gidx[j]]; files slot j into `next`.
-int launch_g2p(const SimParams& p, const float* Pin, float* Pout, const int32_t* gidx, const int32_t* sig_in,
-               int32_t* sig_out, const float4* vgrid, const float* sdf, int32_t* pcell, int32_t* prank,
-               const BinSet& next, uint32_t* health, cudaStream_t st);
+int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const float* Pin, float* Pout,
+               const int32_t* gidx, const int32_t* sig_in, int32_t* sig_out, const float4* vgrid, const float* sdf,
+               int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st);
 
+// The kernels below take one scene's SimParams and pointers already offset to
+// that scene's part of the arrays.
 // ------------------------------------------------------ state transfer ----
 // Loads a 26-plane host-layout state (already on the device, stride n) into
-// P (original order) and sets sigma to the identity.  init_rules applies
-// initFMatrices (kernels.cu:349-358): F diagonal = 1.
+// P (original order) and sets sigma[i] = p.poff + i (global slots).
+// init_rules applies initFMatrices (kernels.cu:349-358): F diagonal = 1.
 int launch_state_import(const SimParams& p, const float* soa26, float* P, int32_t* sigma, bool init_rules,
                         cudaStream_t st);
-// keys[sigma[j]] = setKeys' Morton key of slot j of P (original order).
+// keys[sigma[j] - p.poff] = setKeys' Morton key of slot j of P (original order).
 int launch_reference_keys(const SimParams& p, const float* P, const int32_t* sigma, int32_t* keys, cudaStream_t st);
 // Writes the 26-plane state in original order: plane k of particle sigma[j]
 // from slot j of P (VOL and MASS from the scalars).

@@ -46,24 +46,67 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Files this lane's particle under `cell` (bin `bin`) of a counter set and
-// returns its rank among the cell's particles: one atomic per distinct cell
-// and per distinct bin of the warp; the first particle of a bin appends the
-// bin to the set's list.  Every lane of the warp must call it; lanes with
-// cell < 0 take part without counting.
-__device__ __forceinline__ int file_particle(int cell, int bin, const BinSet& set) {
+// Files this lane's particle under global cell `gcell` (global bin `gbin`,
+// bin `bin` of scene `scene`, whose bin entries start at `boff`) of a counter
+// set and returns its rank among the cell's particles: one atomic per
+// distinct cell and per distinct bin of the warp; the first particle of a
+// bin appends the bin to its scene's list.  Every lane of the warp must call
+// it; lanes with gcell < 0 take part without counting.
+__device__ __forceinline__ int file_particle(int gcell, int gbin, int bin, int scene, long long boff,
+                                             const BinSet& set) {
     const int lane = threadIdx.x & 31;
-    const uint32_t peers = __match_any_sync(0xffffffffu, cell);
+    const uint32_t peers = __match_any_sync(0xffffffffu, gcell);
     const int leader = __ffs(peers) - 1;
     uint32_t base = 0;
-    if (cell >= 0 && lane == leader) base = atomicAdd(set.ccount + cell, (uint32_t)__popc(peers));
+    if (gcell >= 0 && lane == leader) base = atomicAdd(set.ccount + gcell, (uint32_t)__popc(peers));
     base = __shfl_sync(0xffffffffu, base, leader);
-    const uint32_t bpeers = __match_any_sync(0xffffffffu, bin);
-    if (bin >= 0 && lane == __ffs(bpeers) - 1) {
-        if (atomicAdd(set.bcount + bin, (uint32_t)__popc(bpeers)) == 0u) set.blist[atomicAdd(set.nlist, 1u)] = bin;
+    const uint32_t bpeers = __match_any_sync(0xffffffffu, gbin);
+    if (gbin >= 0 && lane == __ffs(bpeers) - 1) {
+        if (atomicAdd(set.bcount + gbin, (uint32_t)__popc(bpeers)) == 0u)
+            set.blist[boff + atomicAdd(set.nlist + scene, 1u)] = bin;
     }
     return (int)base + __popc(peers & lanemask_lt());
 }
+
+// Scene lookup for the per-particle and per-node kernels.  With one scene
+// (kBatch false) the parameters are the kernel argument p0, read from the
+// parameter bank; with several, the CTA stages up to kTableScenes scene
+// records and their first indices in shared memory and each thread finds its
+// scene there by binary search (in global memory beyond that).
+constexpr int kTableScenes = 64;
+
+template <bool kBatch>
+struct SceneLookup {
+    const SimParams* prm;
+    const long long* first;
+    int count;
+
+    // Must be reached by every thread of the CTA (it may synchronize).
+    __device__ __forceinline__ SceneLookup(const SceneTable& sc, const long long* first_global, SimParams* s_prm,
+                                           long long* s_first)
+        : prm(sc.prm), first(first_global), count(sc.count) {
+        if constexpr (kBatch) {
+            if (count <= kTableScenes) {
+                for (int i = threadIdx.x; i < count; i += blockDim.x) s_prm[i] = sc.prm[i];
+                for (int i = threadIdx.x; i <= count; i += blockDim.x) s_first[i] = first_global[i];
+                __syncthreads();
+                prm = s_prm;
+                first = s_first;
+            }
+        }
+    }
+
+    __device__ __forceinline__ int scene(long long i) const {
+        if constexpr (!kBatch) return 0;
+        int lo = 0, hi = count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (first[mid] <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        return lo;
+    }
+};
 
 // ------------------------------------------------------------------ P2G ----
 // P2G (p2GTransferScatter, kernels.cu:6-142).  Persistent single-warp CTAs
@@ -189,29 +232,35 @@ __device__ __forceinline__ void p2g_stencil(const P2GParticle& r, Emit emit) {
     }
 }
 
-__global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SimParams p, const float* __restrict__ P,
+__global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, const float* __restrict__ P,
                                                                   const int32_t* __restrict__ gidx,
                                                                   const int32_t* __restrict__ cstart, BinSet set,
+                                                                  const long long* __restrict__ itemoff,
                                                                   uint32_t* __restrict__ work,
-                                                                  float4* __restrict__ accum,
+                                                                  float4* __restrict__ accum_all,
                                                                   uint32_t* __restrict__ status) {
     __shared__ __align__(16) float4 s_ring[kRing][6][32];
     __shared__ float4 s_foot[kFootNodes];
     __shared__ int32_t s_gidx[kGidxStage];
     const int lane = threadIdx.x;
-    const int nitems = (int)*reinterpret_cast<volatile uint32_t*>(set.nlist) * kBinZ;
+    const long long nitems = *reinterpret_cast<volatile const long long*>(itemoff + sc.count);
     for (int q = lane; q < kFootNodes; q += 32) s_foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (;;) {
         int item = 0;
         if (lane == 0) item = (int)atomicAdd(work, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= nitems) return;
-        const int bin = __ldg(set.blist + item / kBinZ), layer = item % kBinZ;
+        // Items: kBinZ layers per listed bin, scene after scene.
+        const int scene = scene_of(itemoff, sc.count, item);
+        const SimParams p = sc.prm[scene];
+        const int local = item - (int)__ldg(itemoff + scene);
+        const int bin = __ldg(set.blist + p.boff + local / kBinZ), layer = local % kBinZ;
         if (bin >= p.nb) continue;  // the overflow bin reaches no node
+        float4* accum = accum_all + p.goff;
         const int bxi = bin % p.nbx, byi = (bin / p.nbx) % p.nby, bzi = bin / (p.nbx * p.nby);
         // Node origin of the footprint = base cell of lane 0 of this layer.
         const int ox = bxi * kBinX - 2, oy = byi * kBinY - 2, oz = bzi * kBinZ - 2 + layer;
-        const int cell = bin * kBinCells + layer * 32 + lane;
+        const int cell = (int)p.coff + bin * kBinCells + layer * 32 + lane;
         const int cs = __ldg(cstart + cell);
         const int full = (int)__ldg(set.ccount + cell);
         const int l0 = __shfl_sync(0xffffffffu, cs, 0);
@@ -355,39 +404,51 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SimParams p, co
 
 // -------------------------------------------------------------- binning ----
 // Files the particles of an imported state (slot order) into a counter set.
-__global__ void __launch_bounds__(256) bin_count_kernel(SimParams p, const float* __restrict__ P,
+__global__ void __launch_bounds__(256) bin_count_kernel(SceneTable sc, long long n, const float* __restrict__ P,
                                                         int32_t* __restrict__ pcell, int32_t* __restrict__ prank,
                                                         BinSet set) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = j < p.n;
-    int cell = -1, bin = -1;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool valid = j < n;
+    int gcell = -1, gbin = -1, bin = -1, scene = 0;
+    long long boff = 0;
     if (valid) {
+        scene = scene_of(sc.poff, sc.count, j);
+        const SimParams p = sc.prm[scene];
         const float4 q = __ldg(reinterpret_cast<const float4*>(P + (size_t)j * kAFloats));
-        cell = cell_of(p, q.x, q.y, q.z, &bin);
+        const int cell = cell_of(p, q.x, q.y, q.z, &bin);
+        gcell = (int)p.coff + cell;
+        gbin = (int)p.boff + bin;
+        boff = p.boff;
     }
-    const int r = file_particle(cell, bin, set);
+    const int r = file_particle(gcell, gbin, bin, scene, boff, set);
     if (valid) {
-        pcell[j] = cell;
+        pcell[j] = gcell;
         prank[j] = r;
     }
 }
 
-// bstart[i] = sum of bcount[0..i) over nbins = nb + 1 bins, bstart[nbins] =
-// n.  Also zeroes the bin counters of the other set and the P2G work
-// counter.  One CTA, in chunks of kScanChunk counters: coalesced loads into
-// shared memory, a contiguous run of kScanPer counters per thread, a block
-// scan of the run sums, coalesced stores.
+// One CTA per scene: bstart[i] = poff + sum of bcount[0..i) over the scene's
+// nbins = nb + 1 bins, bstart[nbins] = poff + its particle count (global
+// slots).  Also zeroes the scene's bin counters of the other set, and CTA 0
+// the P2G and G2P work counters.  In chunks of kScanChunk counters: coalesced
+// loads into shared memory, a contiguous run of kScanPer counters per thread,
+// a block scan of the run sums, coalesced stores.
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 8;
 constexpr int kScanChunk = kScanThreads * kScanPer;
-__global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(const uint32_t* __restrict__ bcount,
-                                                                uint32_t* __restrict__ bclear,
-                                                                int32_t* __restrict__ bstart, int nbins,
+__global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(SceneTable sc, const uint32_t* __restrict__ bcount_all,
+                                                                uint32_t* __restrict__ bclear_all,
+                                                                int32_t* __restrict__ bstart_all,
                                                                 uint32_t* __restrict__ work) {
     __shared__ int s_val[kScanChunk];
     __shared__ int s_warp[kScanThreads / 32];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    int carry = 0;
+    const SimParams p = sc.prm[blockIdx.x];
+    const uint32_t* bcount = bcount_all + p.boff;
+    uint32_t* bclear = bclear_all + p.boff;
+    int32_t* bstart = bstart_all + p.boff;
+    const int nbins = p.nb + 1;
+    int carry = (int)p.poff;
     for (int c0 = 0; c0 < nbins; c0 += kScanChunk) {
         const int m = min(kScanChunk, nbins - c0);
 #pragma unroll
@@ -439,54 +500,75 @@ __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(const uint32_t* 
     }
     if (t == 0) {
         bstart[nbins] = carry;
-        *work = 0u;
+        if (blockIdx.x == 0) {
+            work[0] = 0u;  // P2G items
+            work[1] = 0u;  // G2P items
+        }
     }
 }
 
-// One warp per listed bin: cstart of its 128 cells = bstart[bin] + the
-// exclusive scan of their counts.  Then clears the cell counters of the
-// other set for the bins on that set's list (the cells it last filled).
-__global__ void __launch_bounds__(128) cell_scan_kernel(BinSet set, const int32_t* __restrict__ bstart,
+// One warp per listed bin of each scene: cstart of its 128 cells = bstart of
+// the bin + the exclusive scan of their counts.  Then clears the cell
+// counters of the other set for the bins on that set's lists (the cells it
+// last filled).
+__global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet set, const int32_t* __restrict__ bstart,
                                                         int32_t* __restrict__ cstart, BinSet clear) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    const int nlist = (int)*set.nlist;
-    for (int item = gw; item < nlist; item += nw) {
-        const int bin = set.blist[item];
-        const uint4 c = *reinterpret_cast<const uint4*>(set.ccount + (size_t)bin * kBinCells + lane * 4);
-        const int sum = (int)(c.x + c.y + c.z + c.w);
-        int incl = sum;
+    for (int scene = 0; scene < sc.count; ++scene) {
+        const long long coff = sc.prm[scene].coff, boff = sc.prm[scene].boff;
+        const int nlist = (int)set.nlist[scene];
+        for (int item = gw; item < nlist; item += nw) {
+            const int bin = set.blist[boff + item];
+            const size_t c0 = (size_t)coff + (size_t)bin * kBinCells + lane * 4;
+            const uint4 c = *reinterpret_cast<const uint4*>(set.ccount + c0);
+            const int sum = (int)(c.x + c.y + c.z + c.w);
+            int incl = sum;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int e0 = bstart[boff + bin] + incl - sum;
+            int4 st;
+            st.x = e0;
+            st.y = e0 + (int)c.x;
+            st.z = st.y + (int)c.y;
+            st.w = st.z + (int)c.z;
+            *reinterpret_cast<int4*>(cstart + c0) = st;
         }
-        const int e0 = bstart[bin] + incl - sum;
-        int4 st;
-        st.x = e0;
-        st.y = e0 + (int)c.x;
-        st.z = st.y + (int)c.y;
-        st.w = st.z + (int)c.z;
-        *reinterpret_cast<int4*>(cstart + (size_t)bin * kBinCells + lane * 4) = st;
-    }
-    const int nclear = (int)*clear.nlist;
-    for (int item = gw; item < nclear; item += nw) {
-        const int bin = clear.blist[item];
-        *reinterpret_cast<uint4*>(clear.ccount + (size_t)bin * kBinCells + lane * 4) = make_uint4(0u, 0u, 0u, 0u);
+        const int nclear = (int)clear.nlist[scene];
+        for (int item = gw; item < nclear; item += nw) {
+            const int bin = clear.blist[boff + item];
+            *reinterpret_cast<uint4*>(clear.ccount + (size_t)coff + (size_t)bin * kBinCells + lane * 4) =
+                make_uint4(0u, 0u, 0u, 0u);
+        }
     }
 }
 
-// gidx[cstart[cell[j]] + rank[j]] = j: the order by cell.  Thread 0 resets
-// the other set's list, which cell_scan_kernel has just cleared.
-__global__ void __launch_bounds__(256) bin_scatter_kernel(int n, const int32_t* __restrict__ pcell,
+// gidx[cstart[cell[j]] + rank[j]] = j: the order by cell.  Thread 0 also
+// writes the P2G item offsets (kBinZ items per listed bin, scene after
+// scene) and resets the other set's lists, which cell_scan_kernel has just
+// cleared.
+__global__ void __launch_bounds__(256) bin_scatter_kernel(long long n, int scenes, const int32_t* __restrict__ pcell,
                                                           const int32_t* __restrict__ prank,
                                                           const int32_t* __restrict__ cstart,
-                                                          int32_t* __restrict__ gidx, uint32_t* __restrict__ clear_nlist) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j == 0) *clear_nlist = 0u;
+                                                          int32_t* __restrict__ gidx, const uint32_t* __restrict__ cur_nlist,
+                                                          long long* __restrict__ itemoff,
+                                                          uint32_t* __restrict__ clear_nlist) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j == 0) {
+        long long run = 0;
+        for (int s2 = 0; s2 < scenes; ++s2) {
+            itemoff[s2] = run;
+            run += (long long)cur_nlist[s2] * kBinZ;
+            clear_nlist[s2] = 0u;
+        }
+        itemoff[scenes] = run;
+    }
     if (j >= n) return;
-    gidx[__ldg(cstart + __ldg(pcell + j)) + __ldg(prank + j)] = j;
+    gidx[__ldg(cstart + __ldg(pcell + j)) + __ldg(prank + j)] = (int32_t)j;
 }
 
 // ---------------------------------------------------------- grid update ----
@@ -495,12 +577,19 @@ __global__ void __launch_bounds__(256) bin_scatter_kernel(int n, const int32_t* 
 // zeroes accum for the next P2G.  The wall tests use the reference's
 // unsigned arithmetic (SimConfig fields are uint32_t): x < PADDING and
 // x > SIZE-1-PADDING with wrap-around.
-__global__ void __launch_bounds__(256) grid_update_kernel(SimParams p, float4* __restrict__ accum,
-                                                          float4* __restrict__ vgrid,
-                                                          const float* __restrict__ sdf) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= p.g) return;
-    const float4 a = accum[idx];
+template <bool kBatch>
+__global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimParams p0, long long g_total,
+                                                          float4* __restrict__ accum, float4* __restrict__ vgrid,
+                                                          const float* __restrict__ sdf_all) {
+    __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
+    __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
+    const SceneLookup<kBatch> look(sc, sc.goff, s_prm, s_first);
+    const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gi >= g_total) return;
+    const SimParams& p = kBatch ? look.prm[look.scene(gi)] : p0;
+    const int idx = (int)(gi - p.goff);
+    const float* sdf = sdf_all + p.goff;
+    const float4 a = accum[gi];
     float4 out = make_float4(a.x, 0.f, 0.f, 0.f);
     if (a.x > 1e-9f) {
         const int x = idx % p.sx, y = (idx / p.sx) % p.sy, z = idx / (p.sx * p.sy);
@@ -525,8 +614,8 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SimParams p, float4* _
         if ((uint32_t)z > (uint32_t)p.sz - 1u - pad && vz > 0.f) vz = 0.f;
         out = make_float4(a.x, vx, vy, vz);
     }
-    vgrid[idx] = out;
-    if (a.x != 0.f || a.y != 0.f || a.z != 0.f || a.w != 0.f) accum[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+    vgrid[gi] = out;
+    if (a.x != 0.f || a.y != 0.f || a.z != 0.f || a.w != 0.f) accum[gi] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // ------------------------------------------------------------------ G2P ----
@@ -534,15 +623,23 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SimParams p, float4* _
 // slot gidx[j] of the old state and writes slot j of the new one, so the
 // state ends up ordered by cell.  It also files the new position into the
 // counter set of the next substep.
-__global__ void __launch_bounds__(256) g2p_kernel(SimParams p, const float* __restrict__ Pin,
+template <bool kBatch>
+__global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, long long n_total, const float* __restrict__ Pin,
                                                   float* __restrict__ Pout, const int32_t* __restrict__ gidx,
                                                   const int32_t* __restrict__ sig_in, int32_t* __restrict__ sig_out,
-                                                  const float4* __restrict__ vgrid, const float* __restrict__ sdf,
+                                                  const float4* __restrict__ vgrid_all, const float* __restrict__ sdf_all,
                                                   int32_t* __restrict__ pcell, int32_t* __restrict__ prank, BinSet next,
                                                   uint32_t* __restrict__ health) {
-    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = jj < p.n;
-    const int j = valid ? jj : p.n - 1;  // idle lanes redo the last particle and store nothing
+    __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
+    __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
+    const SceneLookup<kBatch> look(sc, sc.poff, s_prm, s_first);
+    const long long jj = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool valid = jj < n_total;
+    const long long j = valid ? jj : n_total - 1;  // idle lanes redo the last particle and store nothing
+    const int scene = look.scene(j);
+    const SimParams& p = kBatch ? look.prm[scene] : p0;
+    const float4* vgrid = vgrid_all + p.goff;
+    const float* sdf = sdf_all + p.goff;
     const int src = __ldg(gidx + j);
     const float4* q = reinterpret_cast<const float4*>(Pin + (size_t)src * kAFloats);
     const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
@@ -624,9 +721,12 @@ __global__ void __launch_bounds__(256) g2p_kernel(SimParams p, const float* __re
             tv[2] -= nrm.z * vdn;
         }
     }
-    int bin = -1, cell = -1;
-    if (valid) cell = cell_of(p, nx, ny, nz, &bin);
-    const int rank = file_particle(cell, bin, next);
+    int bin = -1, gcell = -1, gbin = -1;
+    if (valid) {
+        gcell = (int)p.coff + cell_of(p, nx, ny, nz, &bin);
+        gbin = (int)p.boff + bin;
+    }
+    const int rank = file_particle(gcell, gbin, bin, scene, p.boff, next);
     if (!valid) return;
     float4* o = reinterpret_cast<float4*>(Pout + (size_t)j * kAFloats);
     o[0] = make_float4(nx, ny, nz, NF[0]);
@@ -636,7 +736,7 @@ __global__ void __launch_bounds__(256) g2p_kernel(SimParams p, const float* __re
     o[4] = make_float4(tc[1], tc[2], tc[3], tc[4]);
     o[5] = make_float4(tc[5], tc[6], tc[7], tc[8]);
     sig_out[j] = __ldg(sig_in + src);
-    pcell[j] = cell;
+    pcell[j] = gcell;
     prank[j] = rank;
 
     uint32_t flags = 0;
@@ -669,7 +769,7 @@ __global__ void __launch_bounds__(256) state_import_kernel(SimParams p, const fl
     float4* o = reinterpret_cast<float4*>(P + (size_t)i * kAFloats);
 #pragma unroll
     for (int k = 0; k < 6; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
-    sigma[i] = i;
+    sigma[i] = (int32_t)(p.poff + i);
 }
 
 // keys[sigma[j]] = setKeys' Morton key of the particle in slot j
@@ -680,7 +780,7 @@ __global__ void __launch_bounds__(256) reference_keys_kernel(SimParams p, const 
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= p.n) return;
     const float4 q = __ldg(reinterpret_cast<const float4*>(P + (size_t)j * kAFloats));
-    keys[__ldg(sigma + j)] = morton_key(q.x, q.y, q.z);
+    keys[__ldg(sigma + j) - p.poff] = morton_key(q.x, q.y, q.z);
 }
 
 __global__ void __launch_bounds__(256) state_export_kernel(SimParams p, const float* __restrict__ P,
@@ -689,7 +789,7 @@ __global__ void __launch_bounds__(256) state_export_kernel(SimParams p, const fl
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= p.n) return;
     const long long n = p.n;
-    const int o = __ldg(sigma + j);
+    const long long o = __ldg(sigma + j) - p.poff;
     const float4* q = reinterpret_cast<const float4*>(P + (size_t)j * kAFloats);
     float v[kAFloats];
 #pragma unroll
@@ -711,7 +811,7 @@ __global__ void __launch_bounds__(256) positions_export_kernel(SimParams p, cons
                                                                float* __restrict__ xyz) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= p.n) return;
-    const long long o = __ldg(sigma + j);
+    const long long o = __ldg(sigma + j) - p.poff;
     const float4 q = __ldg(reinterpret_cast<const float4*>(P + (size_t)j * kAFloats));
     xyz[3 * o + 0] = q.x;
     xyz[3 * o + 1] = q.y;
@@ -745,42 +845,54 @@ inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-int launch_bin_count(const SimParams& p, const float* P, int32_t* pcell, int32_t* prank, const BinSet& set,
-                     cudaStream_t st) {
-    if (p.n <= 0) return 0;
-    bin_count_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p, P, pcell, prank, set);
+int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t* pcell, int32_t* prank,
+                     const BinSet& set, cudaStream_t st) {
+    if (n <= 0) return 0;
+    bin_count_kernel<<<blocks_for(n, 256), 256, 0, st>>>(sc, n, P, pcell, prank, set);
     return 1;
 }
 
-int launch_bin_order(const SimParams& p, const BinSet& cur, const BinSet& other, int32_t* bstart, int32_t* cstart,
-                     const int32_t* pcell, const int32_t* prank, int32_t* gidx, uint32_t* work, cudaStream_t st) {
-    if (p.n <= 0) return 0;
-    bin_scan_kernel<<<1, kScanThreads, 0, st>>>(cur.bcount, other.bcount, bstart, p.nb + 1, work);
-    const int ctas = std::max(1, std::min(blocks_for((long long)(p.nb + 1) * 32, 128), 148 * 8));
-    cell_scan_kernel<<<ctas, 128, 0, st>>>(cur, bstart, cstart, other);
-    bin_scatter_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p.n, pcell, prank, cstart, gidx, other.nlist);
+int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
+                     int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
+                     long long* itemoff, uint32_t* work, cudaStream_t st) {
+    if (n <= 0) return 0;
+    bin_scan_kernel<<<sc.count, kScanThreads, 0, st>>>(sc, cur.bcount, other.bcount, bstart, work);
+    const int ctas = (int)std::max(1LL, std::min((long long)blocks_for(bins_total * 32, 128), 148LL * 8));
+    cell_scan_kernel<<<ctas, 128, 0, st>>>(sc, cur, bstart, cstart, other);
+    bin_scatter_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, sc.count, pcell, prank, cstart, gidx, cur.nlist, itemoff,
+                                                         other.nlist);
     return 3;
 }
 
-int launch_p2g(const SimParams& p, const float* P, const int32_t* gidx, const int32_t* cstart, const BinSet& cur,
-               uint32_t* work, float4* accum, uint32_t* status, cudaStream_t st) {
-    if (p.n <= 0 || p.nb <= 0) return 0;
-    const int warps = (int)std::min<long long>((long long)(p.nb + 1) * kBinZ, 148LL * kP2GWarpsPerSM);
-    p2g_kernel<<<warps, 32, 0, st>>>(p, P, gidx, cstart, cur, work, accum, status);
+int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
+               const int32_t* cstart, const BinSet& cur, const long long* itemoff, uint32_t* work, float4* accum,
+               uint32_t* status, cudaStream_t st) {
+    if (n <= 0) return 0;
+    const int warps = (int)std::min(bins_total * kBinZ, 148LL * kP2GWarpsPerSM);
+    p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, itemoff, work, accum, status);
     return 1;
 }
 
-int launch_grid_update(const SimParams& p, float4* accum, float4* vgrid, const float* sdf, cudaStream_t st) {
-    grid_update_kernel<<<blocks_for(p.g, 256), 256, 0, st>>>(p, accum, vgrid, sdf);
+int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
+                       const float* sdf, cudaStream_t st) {
+    if (g_total <= 0) return 0;
+    if (sc.count == 1)
+        grid_update_kernel<false><<<blocks_for(g_total, 256), 256, 0, st>>>(sc, p0, g_total, accum, vgrid, sdf);
+    else
+        grid_update_kernel<true><<<blocks_for(g_total, 256), 256, 0, st>>>(sc, p0, g_total, accum, vgrid, sdf);
     return 1;
 }
 
-int launch_g2p(const SimParams& p, const float* Pin, float* Pout, const int32_t* gidx, const int32_t* sig_in,
-               int32_t* sig_out, const float4* vgrid, const float* sdf, int32_t* pcell, int32_t* prank,
-               const BinSet& next, uint32_t* health, cudaStream_t st) {
-    if (p.n <= 0) return 0;
-    g2p_kernel<<<blocks_for(p.n, 256), 256, 0, st>>>(p, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, prank,
-                                                     next, health);
+int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const float* Pin, float* Pout,
+               const int32_t* gidx, const int32_t* sig_in, int32_t* sig_out, const float4* vgrid, const float* sdf,
+               int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st) {
+    if (n <= 0) return 0;
+    if (sc.count == 1)
+        g2p_kernel<false><<<blocks_for(n, 256), 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+                                                              pcell, prank, next, health);
+    else
+        g2p_kernel<true><<<blocks_for(n, 256), 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+                                                             pcell, prank, next, health);
     return 1;
 }
 

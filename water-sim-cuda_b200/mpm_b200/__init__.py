@@ -147,6 +147,17 @@ def _load() -> ctypes.CDLL:
         "mpm_global_last_error": (ctypes.c_char_p, []),
         "mpm_sort_particles_device": (I32, [P, P, P, I64, P, P, P]),
         "mpm_sort_particles_device_static": (I32, [P, P, P, I64, P, P, P]),
+        "mpm_create_batch": (I32, [P, I32, I32, P]),
+        "mpm_num_scenes": (I32, [P]),
+        "mpm_init_particles_batch": (I32, [P, P, P]),
+        "mpm_scene_init_sdf": (I32, [P, I32, P, I64]),
+        "mpm_scene_num_particles": (I64, [P, I32]),
+        "mpm_scene_get_state": (I32, [P, I32, P]),
+        "mpm_scene_positions_device": (P, [P, I32]),
+        "mpm_scene_get_positions": (I32, [P, I32, P]),
+        "mpm_scene_get_grid": (I32, [P, I32, P]),
+        "mpm_scene_get_sdf": (I32, [P, I32, P]),
+        "mpm_scene_get_sort": (I32, [P, I32, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -331,3 +342,66 @@ def sort_particles_device_static(px: int, py: int, pz: int, n: int, keys: int, p
     st = lib.mpm_sort_particles_device_static(px, py, pz, n, keys, perm, stream or None)
     if st != 0:
         raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
+
+
+class Batch(Engine):
+    """Independent scenes of their own sizes, physics and obstacles, stepped
+    together on one device: every substep stage is one launch over all
+    scenes.  No counterpart in the reference (one scene per process)."""
+
+    def __init__(self, cfgs, device: int = 0):
+        self.cfgs = list(cfgs)
+        self.cfg = self.cfgs[0]
+        arr = (_Config * len(self.cfgs))(*[c.to_c() for c in self.cfgs])
+        handle = ctypes.c_void_p()
+        st = lib.mpm_create_batch(arr, len(self.cfgs), device, ctypes.byref(handle))
+        if st != 0:
+            raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
+        self._h = handle
+        self.n = 0
+        self.counts = [0] * len(self.cfgs)
+
+    @property
+    def scenes(self) -> int:
+        return int(lib.mpm_num_scenes(self._h))
+
+    def init_all(self, states):
+        """Engine::init for every scene: states[s] is (26, n_s) or flat 26*n_s float32."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float32).reshape(-1) for a in states]
+        if len(arrs) != len(self.cfgs) or any(a.size % PARTICLE_PLANES for a in arrs):
+            raise ValueError("one 26-plane state per scene expected")
+        counts = (ctypes.c_int64 * len(arrs))(*[a.size // PARTICLE_PLANES for a in arrs])
+        ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data if a.size else None for a in arrs])
+        self._check(lib.mpm_init_particles_batch(self._h, counts, ptrs))
+        self.counts = list(counts)
+        self.n = sum(self.counts)
+
+    def init_scene_sdf(self, scene: int, triangles):
+        t = np.ascontiguousarray(triangles, dtype=np.float32).reshape(-1)
+        self._check(lib.mpm_scene_init_sdf(self._h, scene, _ptr(t) if t.size else None, t.size // 9))
+
+    def scene_buffer(self, scene: int) -> np.ndarray:
+        out = np.empty((PARTICLE_PLANES, self.counts[scene]), np.float32)
+        self._check(lib.mpm_scene_get_state(self._h, scene, _ptr(out)))
+        return out
+
+    def scene_positions(self, scene: int) -> np.ndarray:
+        out = np.empty((self.counts[scene], 3), np.float32)
+        self._check(lib.mpm_scene_get_positions(self._h, scene, _ptr(out)))
+        return out
+
+    def scene_grid(self, scene: int) -> np.ndarray:
+        out = np.empty((GRID_PLANES, self.cfgs[scene].grid_number), np.float32)
+        self._check(lib.mpm_scene_get_grid(self._h, scene, _ptr(out)))
+        return out
+
+    def scene_sdf(self, scene: int) -> np.ndarray:
+        out = np.empty(self.cfgs[scene].grid_number, np.float32)
+        self._check(lib.mpm_scene_get_sdf(self._h, scene, _ptr(out)))
+        return out
+
+    def scene_sort(self, scene: int):
+        keys = np.empty(self.counts[scene], np.int32)
+        perm = np.empty(self.counts[scene], np.int32)
+        self._check(lib.mpm_scene_get_sort(self._h, scene, _ptr(keys), _ptr(perm)))
+        return keys, perm

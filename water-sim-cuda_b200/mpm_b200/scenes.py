@@ -225,3 +225,36 @@ def small_scene(n: int, size=(32, 32, 32), seed: int = 7, obstacle: bool = True,
     if obstacle:
         tris = uv_sphere(r, c, 16, 8)
     return cfg, st.astype(np.float32), tris
+
+
+def batched_scenes(count: int = 64, seed: int = 1237):
+    """Independent scenes for the batched engine: grid size per axis uniform in
+    [32, 96]; one water sphere whose particle count is log-uniform in
+    [10k, 500k] (its radius, from 8 particles per cell, is clamped to
+    0.2-0.4 of the smallest grid extent and the sphere kept 4 cells off the
+    walls); 0-2 obstacles, a torus or a box, at seeded positions.  Returns a
+    list of (cfg, state26, triangles)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        size = tuple(int(v) for v in rng.integers(32, 97, size=3))
+        cfg = _cfg(size)
+        ext = float(min(size))
+        target = float(np.exp(rng.uniform(np.log(1e4), np.log(5e5))))
+        r = (3.0 * target / (4.0 * np.pi * 8.0)) ** (1.0 / 3.0)
+        r = float(np.clip(r, 0.2 * ext, 0.4 * ext))
+        lo = np.array([4.0 + r] * 3)
+        hi = np.array(size, np.float64) - 4.0 - r
+        c = rng.uniform(lo, np.maximum(hi, lo))
+        pos = seed_sphere(tuple(c), r, cfg.resolution, rng)
+        tris = []
+        for _k in range(int(rng.integers(0, 3))):
+            oc = rng.uniform(0.2, 0.8, size=3) * np.array(size)
+            s = float(rng.uniform(0.1, 0.2) * ext)
+            if rng.random() < 0.5:
+                tris.append(torus(s, s / 3.0, tuple(oc), 24, 12))
+            else:
+                tris.append(box_mesh((s, s / 2.0, s), tuple(oc)))
+        t = np.concatenate(tris) if tris else np.zeros((0, 9), np.float32)
+        out.append((cfg, pack_state(pos), t))
+    return out
