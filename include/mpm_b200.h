@@ -372,6 +372,79 @@ mpm_status mpm_sort_particles_device(const float* d_pos_x, const float* d_pos_y,
 mpm_status mpm_sort_particles_device_static(const float* d_pos_x, const float* d_pos_y, const float* d_pos_z,
                                             int64_t n, int32_t* d_keys, int32_t* d_perm, void* stream);
 
+/* ------------------------------------------------------------------ */
+/* Learned large step (no counterpart in the reference)                 */
+/* ------------------------------------------------------------------ */
+/* Beside the plain substep, never replacing it: one substep of RATIO x DT
+ * whose G2P adds a velocity correction predicted per particle by a small MLP
+ * (16 -> 64 -> 64 -> 3, GELU, bf16 weights on the tensor cores, fp32
+ * accumulation).  Inputs: the particle's APIC matrix C (9), grid velocity
+ * (3), interpolated grid mass over the seeding density, minus 1 (1), and the
+ * obstacle SDF folded into one vector n * phi * max(0, 1 - |phi| / 4) (3), all
+ * gathered from the large step's grid at the particle's start position.
+ * The plain substep is the fallback and the judge: a large step whose mean
+ * predicted relative density change, mean over particles of
+ * |1 / det(I + RATIO DT C) - 1|, exceeds max_density_change is undone and
+ * replaced by RATIO plain substeps.  Engines of one scene only. */
+#define MPM_CORRECTOR_PARAMS 5478   /* fp32 parameter vector, layout below */
+#define MPM_CORRECTOR_FEATURES 16
+#define MPM_CORRECTOR_OUTPUTS 3
+/* Parameter layout (offsets in floats): input mean [16] @0, input 1/std [16]
+ * @16, output scale [3] @32, W1 [64][16] @35, b1 [64] @1059, W2 [64][64]
+ * @1123, b2 [64] @5219, W3 [3][64] @5283, b3 [3] @5475.  W rows are outputs.
+ * out = (W3 g(W2 g(W1 x' + b1) + b2) + b3) * scale, x' = (x - mean) / std,
+ * g = GELU (tanh form); x', the weights and g's outputs rounded to bf16. */
+
+typedef struct mpm_learned_stats {
+    int64_t large_steps;         /* large steps accepted since creation */
+    int64_t fallbacks;           /* large steps replaced by RATIO plain substeps */
+    double last_density_change;  /* the statistic of the last large step */
+} mpm_learned_stats;
+
+/* Sets the corrector (params_host: MPM_CORRECTOR_PARAMS floats, or NULL for
+ * the uncorrected large step, which has no fallback), the step ratio and the
+ * fallback threshold (negative: never fall back). */
+mpm_status mpm_set_corrector(mpm_engine* engine, const float* params_host, int32_t ratio,
+                             float max_density_change);
+/* nlarge large steps (each RATIO x DT of simulated time); stats optional. */
+mpm_status mpm_step_learned(mpm_engine* engine, int32_t nlarge, mpm_learned_stats* stats);
+
+/* Training data and training.  A corrector holds a dataset of (features,
+ * target) pairs on the device and the parameters with their Adam state. */
+typedef struct mpm_corrector mpm_corrector;
+mpm_status mpm_corrector_create(int32_t device, int64_t capacity, mpm_corrector** out);
+void mpm_corrector_destroy(mpm_corrector* corrector);
+const char* mpm_corrector_last_error(const mpm_corrector* corrector);
+int64_t mpm_corrector_size(const mpm_corrector* corrector);
+mpm_status mpm_corrector_clear(mpm_corrector* corrector);
+/* The collection probe on the engine's current state: one uncorrected large
+ * step records every particle's features and velocity, the state goes back
+ * to the start of that step, RATIO plain substeps follow (the engine keeps
+ * their result: the plain trajectory goes on), and `samples` particles drawn
+ * with replacement (seeded) are appended with target = velocity after the
+ * plain substeps - velocity after the large step. */
+mpm_status mpm_corrector_collect(mpm_corrector* corrector, mpm_engine* engine, int64_t samples, uint64_t seed);
+mpm_status mpm_corrector_add_data(mpm_corrector* corrector, int64_t count, const float* features_host,
+                                  const float* targets_host);
+mpm_status mpm_corrector_get_data(mpm_corrector* corrector, int64_t first, int64_t count, float* features_host,
+                                  float* targets_host);
+/* Input normalisation and output scale from the dataset, seeded random
+ * weights, Adam state reset. */
+mpm_status mpm_corrector_init(mpm_corrector* corrector, uint64_t seed);
+/* `steps` Adam steps (lr, beta 0.9 / 0.999) on batches of `batch` samples
+ * (a multiple of 64) drawn with replacement; mean_loss: mean squared error of
+ * the scaled targets over the steps. */
+mpm_status mpm_corrector_train(mpm_corrector* corrector, int32_t steps, int32_t batch, float lr, uint64_t seed,
+                               float* mean_loss);
+/* Gradient of the loss on the samples idx_host[0..count) (count a multiple
+ * of 64) at the current parameters, without a step. */
+mpm_status mpm_corrector_gradient(mpm_corrector* corrector, int64_t count, const int64_t* idx_host,
+                                  float* grad_host, float* loss_host);
+mpm_status mpm_corrector_get_params(mpm_corrector* corrector, float* params_host);
+mpm_status mpm_corrector_set_params(mpm_corrector* corrector, const float* params_host);
+/* The tensor-core inference of the learned G2P on n feature rows. */
+mpm_status mpm_corrector_forward(mpm_corrector* corrector, int64_t n, const float* features_host, float* out_host);
+
 #ifdef __cplusplus
 }
 #endif

@@ -83,3 +83,15 @@ def test_wrapper_marshalling_against_null_engine(mpm):
     with pytest.raises(mpm.MpmError):
         mpm.sort_particles_device(0, 0, 0, 5, 0, 0, 0)
     assert mpm.lib.mpm_sort_particles_device(None, None, None, 0, None, None, None) == 0
+
+
+def test_corrector_layout_matches_header():
+    """The parameter offsets documented in mpm_b200.h match the reference MLP."""
+    import re
+    import mlp_ref
+    hdr = open(os.path.join(ROOT, "include", "mpm_b200.h")).read()
+    assert int(re.search(r"#define MPM_CORRECTOR_PARAMS (\d+)", hdr).group(1)) == mlp_ref.NPARAMS
+    for name, label in (("in_mean", "input mean"), ("in_inv_std", "input 1/std"), ("out_std", "output scale"),
+                        ("W1", "W1"), ("b1", "b1"), ("W2", "W2"), ("b2", "b2"), ("W3", "W3"), ("b3", "b3")):
+        m = re.search(re.escape(label) + r" \[[^\]]*\](?:\[[^\]]*\])?[\s*]*@(\d+)", hdr)
+        assert m and int(m.group(1)) == mlp_ref.OFF[name][0], name

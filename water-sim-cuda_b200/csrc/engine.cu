@@ -124,6 +124,24 @@ struct mpm_engine {
     int64_t kernel_launches = 0;
     int64_t sort_passes = 0;
     uint32_t health = 0;
+
+    // Learned large step (engines of one scene): the RATIO x DT parameter
+    // table, the packed corrector, the per-step density-change statistic and
+    // the buffers of the collection probe (by original index).
+    int ratio = 4;
+    float max_density_change = 0.02f;
+    bool mlp_set = false;
+    SimParams* d_prm_large = nullptr;
+    mpm::SceneTable table_large{};
+    mpm::MlpPacked* mlp = nullptr;
+    float* d_params = nullptr;
+    float* d_stat = nullptr;
+    float* feat_all = nullptr;  // [n][16]
+    float* vlarge = nullptr;    // [n][3]
+    float* vplain = nullptr;    // [n][3]
+    int64_t large_steps = 0;
+    int64_t fallbacks = 0;
+    double last_density_change = 0.0;
 };
 
 namespace {
@@ -170,6 +188,9 @@ void free_particles(mpm_engine* e) {
     free_dev(e->ref_perm);
     free_dev(e->sort_mem);
     free_dev(e->pos_out);
+    free_dev(e->feat_all);
+    free_dev(e->vlarge);
+    free_dev(e->vplain);
     e->initialized = false;
 }
 
@@ -581,6 +602,81 @@ mpm_status init_all(mpm_engine* e, const int64_t* counts, const float* const* so
     return load_states(e, soa26_host, true);
 }
 
+// ------------------------------------------------------ learned step ----
+// Parameters of the large step: every scene's with DT x RATIO.
+SimParams large_params(const mpm_engine* e, int s) {
+    SimParams p = e->prm[s];
+    p.dt = e->prm[s].dt * (float)e->ratio;
+    return p;
+}
+
+mpm_status prepare_large(mpm_engine* e) {
+    if (!e->d_prm_large) {
+        CK(e, cudaMalloc(&e->d_prm_large, e->scenes * sizeof(SimParams)));
+        CK(e, cudaMalloc(&e->d_stat, sizeof(float)));
+    }
+    std::vector<SimParams> big(e->scenes);
+    for (int s = 0; s < e->scenes; ++s) big[s] = large_params(e, s);
+    CK(e, cudaMemcpyAsync(e->d_prm_large, big.data(), big.size() * sizeof(SimParams), cudaMemcpyHostToDevice,
+                          e->stream));
+    CK(e, cudaStreamSynchronize(e->stream));
+    e->table_large = e->table;
+    e->table_large.prm = e->d_prm_large;
+    if (e->accum_dirty) {
+        CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->g_total * sizeof(float4), e->stream));
+        e->accum_dirty = false;
+    }
+    e->partial_stage = 0;
+    return MPM_OK;
+}
+
+// One substep of RATIO x DT from parity `par` into 1 - par (learn: the
+// learned or collection G2P; null: the uncorrected large step).
+int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
+    cudaStream_t st = e->stream;
+    uint32_t* work = e->ctl + 2 * e->scenes;
+    const SimParams big = large_params(e, 0);
+    int launches = 0;
+    launches += mpm::launch_bin_order(e->table, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart,
+                                      e->cstart, e->pcell, e->prank, e->gidx, e->d_itemoff, work, st);
+    launches += mpm::launch_p2g(e->table_large, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par],
+                                e->d_itemoff, work, e->accum, e->d_flags + 1, st);
+    launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, st);
+    launches += mpm::launch_g2p(e->table_large, big, e->n, e->P[par], e->P[1 - par], e->gidx, e->sigma[par],
+                                e->sigma[1 - par], e->vgrid, e->sdf, e->pcell, e->prank, e->bins[1 - par], e->d_flags,
+                                st, learn);
+    return launches;
+}
+
+// Files the particles of P[par] afresh into counter set `par` (both sets
+// emptied first): the state of parity `par` becomes the current one again.
+mpm_status rebin(mpm_engine* e, int par) {
+    CK(e, cudaMemsetAsync(e->bins_mem, 0, bins_bytes(e), e->stream));
+    CK(e, cudaMemsetAsync(e->ctl, 0, (2 * e->scenes + 2) * sizeof(uint32_t), e->stream));
+    e->kernel_launches += mpm::launch_bin_count(e->table, e->n, e->P[par], e->pcell, e->prank, e->bins[par], e->stream);
+    CK(e, cudaGetLastError());
+    e->parity = par;
+    return MPM_OK;
+}
+
+// `count` plain substeps through the captured graphs.
+mpm_status plain_substeps(mpm_engine* e, int count) {
+    for (int s = 0; s < count; ++s) {
+        CK(e, cudaGraphLaunch(e->graph[e->parity], e->stream));
+        e->kernel_launches += e->graph_kernels[e->parity];
+        e->sort_src = e->parity;
+        e->parity ^= 1;
+        ++e->substeps;
+    }
+    return MPM_OK;
+}
+
+mpm_status learned_ready(mpm_engine* e) {
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (e->scenes != 1) return record(e, MPM_ERR_UNSUPPORTED, "the learned large step serves engines of one scene");
+    return prepare_large(e);
+}
+
 }  // namespace
 
 // -------------------------------------------------------------------------
@@ -634,6 +730,10 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->d_itemoff);
     free_dev(e->d_flags);
     free_dev(e->staging);
+    free_dev(e->d_prm_large);
+    free_dev(e->mlp);
+    free_dev(e->d_params);
+    free_dev(e->d_stat);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -953,4 +1053,111 @@ extern "C" mpm_status mpm_get_stage_times(mpm_engine* e, double* ms, int32_t* co
     *count = e->timing_used;
     e->timing_used = 0;
     return MPM_OK;
+}
+
+// ------------------------------------------------------- learned step ----
+namespace mpm {
+mpm_status corrector_append(mpm_corrector* c, const float* feat_all, const float* vplain, const float* vlarge,
+                            long long n, long long samples, unsigned long long seed, cudaStream_t st);
+int launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t st);
+int launch_velocity_export(const float* P, const int32_t* sigma, long long n, float* out, cudaStream_t st);
+}  // namespace mpm
+
+extern "C" mpm_status mpm_set_corrector(mpm_engine* e, const float* params_host, int32_t ratio,
+                                        float max_density_change) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (ratio < 1 || ratio > 64) return record(e, MPM_ERR_INVALID_ARGUMENT, "ratio must be in [1, 64]");
+    if (std::isnan(max_density_change)) return record(e, MPM_ERR_INVALID_ARGUMENT, "max_density_change is NaN");
+    if (params_host) {
+        for (int i = 0; i < MPM_CORRECTOR_PARAMS; ++i)
+            if (!std::isfinite(params_host[i])) return record(e, MPM_ERR_INVALID_ARGUMENT, "a parameter is not finite");
+        if (!e->mlp) {
+            CK(e, cudaMalloc(&e->mlp, sizeof(mpm::MlpPacked)));
+            CK(e, cudaMalloc(&e->d_params, MPM_CORRECTOR_PARAMS * sizeof(float)));
+        }
+        CK(e, cudaMemcpyAsync(e->d_params, params_host, MPM_CORRECTOR_PARAMS * sizeof(float), cudaMemcpyHostToDevice,
+                              e->stream));
+        e->kernel_launches += mpm::launch_mlp_pack(e->d_params, e->mlp, e->stream);
+        CK(e, cudaGetLastError());
+        CK(e, cudaStreamSynchronize(e->stream));
+    }
+    e->mlp_set = params_host != nullptr;
+    e->ratio = ratio;
+    e->max_density_change = max_density_change;
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_step_learned(mpm_engine* e, int32_t nlarge, mpm_learned_stats* stats) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (nlarge < 0) return record(e, MPM_ERR_INVALID_ARGUMENT, "nlarge < 0");
+    if ((s = learned_ready(e)) != MPM_OK) return s;
+    for (int k = 0; k < nlarge; ++k) {
+        const int par = e->parity;
+        mpm::LearnArgs la{e->mlp, nullptr, nullptr, e->d_stat};
+        if (e->mlp_set) CK(e, cudaMemsetAsync(e->d_stat, 0, sizeof(float), e->stream));
+        e->kernel_launches += enqueue_large(e, par, e->mlp_set ? &la : nullptr);
+        CK(e, cudaGetLastError());
+        e->sort_src = par;
+        bool accept = true;
+        if (e->mlp_set) {
+            float sum = 0.f;
+            CK(e, cudaMemcpyAsync(&sum, e->d_stat, sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+            CK(e, cudaStreamSynchronize(e->stream));
+            e->last_density_change = e->n > 0 ? (double)sum / (double)e->n : 0.0;
+            accept = !(e->max_density_change >= 0.f) || e->last_density_change <= e->max_density_change;
+        }
+        if (accept) {
+            e->parity = 1 - par;
+            ++e->large_steps;
+        } else {
+            if ((s = rebin(e, par)) != MPM_OK) return s;
+            if ((s = plain_substeps(e, e->ratio)) != MPM_OK) return s;
+            ++e->fallbacks;
+        }
+    }
+    if (nlarge > 0) e->grid_view = GridView::kVelocity;
+    if ((s = export_positions(e)) != MPM_OK) return s;
+    if (stats) {
+        stats->large_steps = e->large_steps;
+        stats->fallbacks = e->fallbacks;
+        stats->last_density_change = e->last_density_change;
+    }
+    if ((s = sync_and_collect(e)) != MPM_OK) return s;
+    return check_health(e);
+}
+
+extern "C" mpm_status mpm_corrector_collect(mpm_corrector* c, mpm_engine* e, int64_t samples, uint64_t seed) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!c) return record(e, MPM_ERR_INVALID_ARGUMENT, "corrector is NULL");
+    if (samples < 0) return record(e, MPM_ERR_INVALID_ARGUMENT, "samples < 0");
+    if ((s = learned_ready(e)) != MPM_OK) return s;
+    if (e->n <= 0) return MPM_OK;
+    if (!e->feat_all) {
+        CK(e, cudaMalloc(&e->feat_all, (size_t)e->n * mpm::kMlpIn * sizeof(float)));
+        CK(e, cudaMalloc(&e->vlarge, (size_t)e->n * 3 * sizeof(float)));
+        CK(e, cudaMalloc(&e->vplain, (size_t)e->n * 3 * sizeof(float)));
+    }
+    // The uncorrected large step, recording features and final velocities;
+    // then back to its start state for RATIO plain substeps.
+    const int par = e->parity;
+    mpm::LearnArgs la{nullptr, e->feat_all, e->vlarge, nullptr};
+    e->kernel_launches += enqueue_large(e, par, &la);
+    CK(e, cudaGetLastError());
+    if ((s = rebin(e, par)) != MPM_OK) return s;
+    if ((s = plain_substeps(e, e->ratio)) != MPM_OK) return s;
+    e->kernel_launches += mpm::launch_velocity_export(e->P[e->parity], e->sigma[e->parity], e->n, e->vplain, e->stream);
+    CK(e, cudaGetLastError());
+    s = mpm::corrector_append(c, e->feat_all, e->vplain, e->vlarge, e->n, samples, seed, e->stream);
+    if (s != MPM_OK) {
+        cudaStreamSynchronize(e->stream);
+        return record(e, s, mpm_corrector_last_error(c));
+    }
+    ++e->kernel_launches;
+    e->grid_view = GridView::kVelocity;
+    if ((s = export_positions(e)) != MPM_OK) return s;
+    if ((s = sync_and_collect(e)) != MPM_OK) return s;
+    return check_health(e);
 }

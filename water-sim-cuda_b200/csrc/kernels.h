@@ -8,6 +8,7 @@
 
 #include <string>
 
+#include "corrector.cuh"
 #include "device_math.cuh"
 
 namespace mpm {
@@ -79,11 +80,25 @@ int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const fl
 // p0: the parameters of scene 0, used directly when the table holds one scene.
 int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
                        const float* sdf, cudaStream_t st);
+// Large-step G2P (one scene).  With mlp set: the corrector's correction is
+// added to each particle's velocity and stat[0] += sum over particles of
+// |1 / det(I + dt C) - 1| (the step's predicted relative density change).
+// With mlp null (collection probe): feat[orig] receives the 16 features and
+// vel[orig] the final velocity, by original index.
+struct LearnArgs {
+    const MlpPacked* mlp;
+    float* feat;
+    float* vel;
+    float* stat;
+};
+
 // G2P: slot j of Pout = particle gidx[j] of Pin advanced one substep;
-// sig_out[j] = sig_in[gidx[j]]; files slot j into `next`.
+// sig_out[j] = sig_in[gidx[j]]; files slot j into `next`.  learn: a large
+// step of one scene (LearnArgs), else null.
 int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const float* Pin, float* Pout,
                const int32_t* gidx, const int32_t* sig_in, int32_t* sig_out, const float4* vgrid, const float* sdf,
-               int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st);
+               int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st,
+               const LearnArgs* learn = nullptr);
 
 // The kernels below take one scene's SimParams and pointers already offset to
 // that scene's part of the arrays.

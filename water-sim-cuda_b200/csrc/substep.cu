@@ -623,15 +623,29 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
 // slot gidx[j] of the old state and writes slot j of the new one, so the
 // state ends up ordered by cell.  It also files the new position into the
 // counter set of the next substep.
-template <bool kBatch>
+// G2P modes: the plain substep; the learned large step (features -> MLP ->
+// velocity correction before advection); the collection probe (the large
+// step without correction, recording each particle's features and final
+// velocity by original index).
+enum G2PMode : int { kG2PPlain = 0, kG2PLearned = 1, kG2PCollect = 2 };
+
+template <bool kBatch, int kMode>
 __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, long long n_total, const float* __restrict__ Pin,
                                                   float* __restrict__ Pout, const int32_t* __restrict__ gidx,
                                                   const int32_t* __restrict__ sig_in, int32_t* __restrict__ sig_out,
                                                   const float4* __restrict__ vgrid_all, const float* __restrict__ sdf_all,
                                                   int32_t* __restrict__ pcell, int32_t* __restrict__ prank, BinSet next,
-                                                  uint32_t* __restrict__ health) {
+                                                  uint32_t* __restrict__ health, LearnArgs la) {
     __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
     __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
+    __shared__ __align__(16) unsigned char s_mlp_raw[kMode == kG2PLearned ? sizeof(MlpPacked) : 16];
+    __shared__ uint32_t s_stage[kMode == kG2PLearned ? 8 * 32 * kMlpStageStride : 1];
+    if constexpr (kMode == kG2PLearned) {
+        const uint4* src = reinterpret_cast<const uint4*>(la.mlp);
+        uint4* dst = reinterpret_cast<uint4*>(s_mlp_raw);
+        for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) dst[i] = __ldg(src + i);
+        __syncthreads();
+    }
     const SceneLookup<kBatch> look(sc, sc.poff, s_prm, s_first);
     const long long jj = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const bool valid = jj < n_total;
@@ -654,7 +668,7 @@ __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, l
         wy[a] = bspline_weight(pos[1] - (float)(by + a));
         wz[a] = bspline_weight(pos[2] - (float)(bz + a));
     }
-    float tv[3] = {0.f, 0.f, 0.f}, tc[9];
+    float tv[3] = {0.f, 0.f, 0.f}, tc[9], tm = 0.f;
 #pragma unroll
     for (int k = 0; k < 9; ++k) tc[k] = 0.f;
 #pragma unroll
@@ -677,6 +691,7 @@ __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, l
                 tv[0] += w * g.y;
                 tv[1] += w * g.z;
                 tv[2] += w * g.w;
+                if constexpr (kMode != kG2PPlain) tm += w * g.x;
                 const float term = 4.0f * w;
                 tc[0] += term * g.y * dxv;
                 tc[1] += term * g.y * dyv;
@@ -688,6 +703,39 @@ __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, l
                 tc[7] += term * g.w * dyv;
                 tc[8] += term * g.w * dzv;
             }
+        }
+    }
+    if constexpr (kMode != kG2PPlain) {
+        float f[kMlpIn];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) f[k] = tc[k];
+        f[9] = tv[0], f[10] = tv[1], f[11] = tv[2];
+        f[12] = tm * (p.pvol / p.pmass) - 1.0f;
+        f[13] = f[14] = f[15] = 0.f;
+        const float phi = sdf_trilinear(p, sdf, pos[0], pos[1], pos[2]);
+        if (fabsf(phi) < 4.0f) {
+            const float3 nrm = sdf_gradient_dir(p, sdf, pos[0], pos[1], pos[2]);
+            const float s = phi * (1.0f - fabsf(phi) * 0.25f);
+            f[13] = nrm.x * s, f[14] = nrm.y * s, f[15] = nrm.z * s;
+        }
+        if constexpr (kMode == kG2PLearned) {
+            float dv[3];
+            mlp_forward_warp(*reinterpret_cast<const MlpPacked*>(s_mlp_raw), s_stage + (threadIdx.x >> 5) * 32 * kMlpStageStride,
+                             f, dv);
+            tv[0] += dv[0], tv[1] += dv[1], tv[2] += dv[2];
+            // Predicted relative density change of the step: 1 / det(I + dt C) - 1.
+            float T[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) T[k] = ((k % 4 == 0) ? 1.0f : 0.0f) + p.dt * tc[k];
+            float dev = valid ? fabsf(1.0f / det3(T) - 1.0f) : 0.f;
+            if (!(dev < 1e30f)) dev = 1e30f;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) dev += __shfl_xor_sync(0xffffffffu, dev, o);
+            if ((threadIdx.x & 31) == 0) atomicAdd(la.stat, dev);
+        } else if (valid) {
+            float* fo = la.feat + (size_t)__ldg(sig_in + src) * kMlpIn;
+#pragma unroll
+            for (int k = 0; k < kMlpIn; k += 4) *reinterpret_cast<float4*>(fo + k) = make_float4(f[k], f[k + 1], f[k + 2], f[k + 3]);
         }
     }
     // F' = (I + DT C') F with the J < 0.3 volume rescue (calculateNewF,
@@ -738,6 +786,10 @@ __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, l
     sig_out[j] = __ldg(sig_in + src);
     pcell[j] = gcell;
     prank[j] = rank;
+    if constexpr (kMode == kG2PCollect) {
+        float* vo = la.vel + (size_t)__ldg(sig_in + src) * 3;
+        vo[0] = tv[0], vo[1] = tv[1], vo[2] = tv[2];
+    }
 
     uint32_t flags = 0;
     if (!(isfinite(nx) && isfinite(ny) && isfinite(nz) && isfinite(tv[0]) && isfinite(tv[1]) && isfinite(tv[2])))
@@ -885,14 +937,23 @@ int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_to
 
 int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const float* Pin, float* Pout,
                const int32_t* gidx, const int32_t* sig_in, int32_t* sig_out, const float4* vgrid, const float* sdf,
-               int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st) {
+               int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st,
+               const LearnArgs* learn) {
     if (n <= 0) return 0;
-    if (sc.count == 1)
-        g2p_kernel<false><<<blocks_for(n, 256), 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
-                                                              pcell, prank, next, health);
+    const LearnArgs la = learn ? *learn : LearnArgs{};
+    const unsigned grid = blocks_for(n, 256);
+    if (learn && sc.count == 1 && la.mlp)
+        g2p_kernel<false, kG2PLearned><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+                                                             pcell, prank, next, health, la);
+    else if (learn && sc.count == 1)
+        g2p_kernel<false, kG2PCollect><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+                                                             pcell, prank, next, health, la);
+    else if (sc.count == 1)
+        g2p_kernel<false, kG2PPlain><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+                                                           pcell, prank, next, health, la);
     else
-        g2p_kernel<true><<<blocks_for(n, 256), 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
-                                                             pcell, prank, next, health);
+        g2p_kernel<true, kG2PPlain><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+                                                          pcell, prank, next, health, la);
     return 1;
 }
 

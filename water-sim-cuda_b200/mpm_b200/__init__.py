@@ -24,6 +24,7 @@ POS_X, VEL_X, C00, F00, VOL, MASS = 0, 3, 6, 15, 24, 25
 STAGE_SORT, STAGE_P2G, STAGE_GRID, STAGE_G2P = 1, 2, 3, 4
 HEALTH_NONFINITE, HEALTH_OUT_OF_GRID = 1, 2
 SORT_STATIC_MAX_PARTICLES = 1 << 20  # MPM_SORT_STATIC_MAX_PARTICLES
+CORRECTOR_PARAMS, CORRECTOR_FEATURES, CORRECTOR_OUTPUTS = 5478, 16, 3
 
 STATUS = {
     0: "MPM_OK", 1: "MPM_ERR_INVALID_ARGUMENT", 2: "MPM_ERR_BAD_CONFIG", 3: "MPM_ERR_IO",
@@ -54,6 +55,11 @@ class _Config(ctypes.Structure):
 class _SceneEntry(ctypes.Structure):
     _fields_ = [("model_path", ctypes.c_char * 512), ("scale", ctypes.c_float),
                 ("x", ctypes.c_float), ("y", ctypes.c_float), ("z", ctypes.c_float)]
+
+
+class _LearnedStats(ctypes.Structure):
+    _fields_ = [("large_steps", ctypes.c_int64), ("fallbacks", ctypes.c_int64),
+                ("last_density_change", ctypes.c_double)]
 
 
 class _Stats(ctypes.Structure):
@@ -158,6 +164,22 @@ def _load() -> ctypes.CDLL:
         "mpm_scene_get_grid": (I32, [P, I32, P]),
         "mpm_scene_get_sdf": (I32, [P, I32, P]),
         "mpm_scene_get_sort": (I32, [P, I32, P, P]),
+        "mpm_set_corrector": (I32, [P, P, I32, ctypes.c_float]),
+        "mpm_step_learned": (I32, [P, I32, P]),
+        "mpm_corrector_create": (I32, [I32, I64, P]),
+        "mpm_corrector_destroy": (None, [P]),
+        "mpm_corrector_last_error": (ctypes.c_char_p, [P]),
+        "mpm_corrector_size": (I64, [P]),
+        "mpm_corrector_clear": (I32, [P]),
+        "mpm_corrector_collect": (I32, [P, P, I64, ctypes.c_uint64]),
+        "mpm_corrector_add_data": (I32, [P, I64, P, P]),
+        "mpm_corrector_get_data": (I32, [P, I64, I64, P, P]),
+        "mpm_corrector_init": (I32, [P, ctypes.c_uint64]),
+        "mpm_corrector_train": (I32, [P, I32, I32, ctypes.c_float, ctypes.c_uint64, P]),
+        "mpm_corrector_gradient": (I32, [P, I64, P, P, P]),
+        "mpm_corrector_get_params": (I32, [P, P]),
+        "mpm_corrector_set_params": (I32, [P, P]),
+        "mpm_corrector_forward": (I32, [P, I64, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -316,6 +338,24 @@ class Engine:
     def stream(self) -> int:
         return int(lib.mpm_stream(self._h) or 0)
 
+    # -- learned large step ---------------------------------------------------
+    def set_corrector(self, params: np.ndarray | None, ratio: int = 4, max_density_change: float = 0.02):
+        """The corrector's MPM_CORRECTOR_PARAMS floats (None: uncorrected large steps)."""
+        if params is None:
+            self._check(lib.mpm_set_corrector(self._h, None, int(ratio), float(max_density_change)))
+            return
+        w = np.ascontiguousarray(params, dtype=np.float32).reshape(-1)
+        if w.size != CORRECTOR_PARAMS:
+            raise ValueError(f"expected {CORRECTOR_PARAMS} parameters, got {w.size}")
+        self._check(lib.mpm_set_corrector(self._h, _ptr(w), int(ratio), float(max_density_change)))
+
+    def step_learned(self, nlarge: int = 1) -> dict:
+        """nlarge large steps of RATIO x DT; returns the running learned-step counters."""
+        s = _LearnedStats()
+        self._check(lib.mpm_step_learned(self._h, int(nlarge), ctypes.byref(s)))
+        return {"large_steps": s.large_steps, "fallbacks": s.fallbacks,
+                "last_density_change": s.last_density_change}
+
     def set_stage_timing(self, max_substeps: int):
         """Record CUDA events between the stages of the next max_substeps substeps."""
         self._check(lib.mpm_set_stage_timing(self._h, int(max_substeps)))
@@ -405,3 +445,94 @@ class Batch(Engine):
         perm = np.empty(self.counts[scene], np.int32)
         self._check(lib.mpm_scene_get_sort(self._h, scene, _ptr(keys), _ptr(perm)))
         return keys, perm
+
+
+class Corrector:
+    """Training data, parameters and Adam state of the learned corrector."""
+
+    def __init__(self, capacity: int, device: int = 0):
+        h = ctypes.c_void_p()
+        st = lib.mpm_corrector_create(int(device), int(capacity), ctypes.byref(h))
+        if st != 0:
+            raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
+        self._h = h
+        self.capacity = int(capacity)
+
+    def _check(self, st: int):
+        if st != 0:
+            raise MpmError(st, lib.mpm_corrector_last_error(self._h).decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.mpm_corrector_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def size(self) -> int:
+        return int(lib.mpm_corrector_size(self._h))
+
+    def clear(self):
+        self._check(lib.mpm_corrector_clear(self._h))
+
+    def collect(self, engine: Engine, samples: int, seed: int):
+        """The collection probe on the engine's current state (the engine advances RATIO substeps)."""
+        st = lib.mpm_corrector_collect(self._h, engine._h, int(samples), int(seed))
+        if st != 0:
+            raise MpmError(st, lib.mpm_last_error(engine._h).decode(errors="replace"))
+
+    def add_data(self, features: np.ndarray, targets: np.ndarray):
+        f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, CORRECTOR_FEATURES)
+        t = np.ascontiguousarray(targets, dtype=np.float32).reshape(-1, CORRECTOR_OUTPUTS)
+        if len(f) != len(t):
+            raise ValueError("features and targets differ in length")
+        self._check(lib.mpm_corrector_add_data(self._h, len(f), _ptr(f), _ptr(t)))
+
+    def get_data(self, first: int = 0, count: int | None = None):
+        count = self.size - first if count is None else count
+        f = np.empty((count, CORRECTOR_FEATURES), np.float32)
+        t = np.empty((count, CORRECTOR_OUTPUTS), np.float32)
+        self._check(lib.mpm_corrector_get_data(self._h, int(first), int(count), _ptr(f), _ptr(t)))
+        return f, t
+
+    def init(self, seed: int = 0):
+        self._check(lib.mpm_corrector_init(self._h, int(seed)))
+
+    def train(self, steps: int, batch: int = 65536, lr: float = 1e-3, seed: int = 0) -> float:
+        loss = ctypes.c_float(0.0)
+        self._check(lib.mpm_corrector_train(self._h, int(steps), int(batch), float(lr), int(seed),
+                                            ctypes.byref(loss)))
+        return float(loss.value)
+
+    def gradient(self, idx: np.ndarray):
+        i = np.ascontiguousarray(idx, dtype=np.int64)
+        g = np.empty(CORRECTOR_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(lib.mpm_corrector_gradient(self._h, len(i), _ptr(i), _ptr(g), _ptr(loss)))
+        return g, float(loss[0])
+
+    def get_params(self) -> np.ndarray:
+        w = np.empty(CORRECTOR_PARAMS, np.float32)
+        self._check(lib.mpm_corrector_get_params(self._h, _ptr(w)))
+        return w
+
+    def set_params(self, params: np.ndarray):
+        w = np.ascontiguousarray(params, dtype=np.float32).reshape(-1)
+        if w.size != CORRECTOR_PARAMS:
+            raise ValueError(f"expected {CORRECTOR_PARAMS} parameters")
+        self._check(lib.mpm_corrector_set_params(self._h, _ptr(w)))
+
+    def forward(self, features: np.ndarray) -> np.ndarray:
+        """The tensor-core inference of the learned G2P."""
+        f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, CORRECTOR_FEATURES)
+        out = np.empty((len(f), CORRECTOR_OUTPUTS), np.float32)
+        self._check(lib.mpm_corrector_forward(self._h, len(f), _ptr(f), _ptr(out)))
+        return out

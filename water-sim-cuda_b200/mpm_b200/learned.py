@@ -1,0 +1,243 @@
+"""Training and evaluation of the learned large-step corrector.
+
+The corrector (include/mpm_b200.h, "Learned large step") lets one substep of
+RATIO x DT stand in for RATIO plain substeps.  This module:
+
+  * builds seeded variants of the 128^3 dam-break scene (water-box extents
+    +-20 %, torus position +-15 cells);
+  * runs plain trajectories on them and, every few substeps, the collection
+    probe (one uncorrected large step vs RATIO plain substeps from the same
+    state), filling the corrector's dataset on the device;
+  * trains the MLP with the library's fused training kernel (Adam);
+  * evaluates a learned run against the plain run from the same state:
+    simulated time per second of each, the fallback count, the grid-density
+    error and the particle-position divergence.
+
+Density error: sum over nodes of |m_learned - m_plain| / sum of m_plain, with
+m the B-spline node mass of the particle positions (the P2G mass field).
+Divergence: mean distance in cells between a particle's two positions.
+
+Run `python -m mpm_b200.learned train --out FILE` to train and save the
+parameters, `python -m mpm_b200.learned evaluate --params FILE` to measure.
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+import os
+import time
+
+import numpy as np
+
+from . import Corrector, Engine, scenes
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_PARAMS = os.path.join(HERE, "corrector_dam_break.npz")
+
+
+def dam_break_variant(seed: int, physical: bool = False):
+    """The 2M dam break with seeded box extents (+-20 %) and torus position
+    (+-15 cells).  physical=True flips GRAVITY and GAMMA to the orientation in
+    which gravity pulls -y and the Tait law resists compression."""
+    rng = np.random.default_rng(seed)
+    cfg = scenes._cfg((128, 128, 128))
+    f = rng.uniform(0.8, 1.2, size=3)
+    hi = np.minimum(4.0 + np.array([56.0, 37.0, 120.0]) * f, 124.0)
+    pos = scenes.seed_box((4.0, 4.0, 4.0), hi, cfg.resolution, rng)
+    c = np.array([80.0, 30.0, 64.0]) + rng.uniform(-15, 15, size=3)
+    c[0] = min(c[0], 128 - 3 - 34.0)
+    tris = scenes.torus(25.0, 8.0, tuple(c), 48, 24)
+    if physical:
+        cfg = physical_config(cfg)
+    return cfg, scenes.pack_state(pos), tris
+
+
+def physical_config(cfg):
+    return dataclasses.replace(cfg, gravity=-cfg.gravity, gamma=-cfg.gamma)
+
+
+def collect(corr: Corrector, seeds, substeps: int, probe_every: int, samples: int, ratio: int = 4,
+            physical: bool = False, log=print):
+    """Plain trajectories of `substeps` substeps on dam_break_variant(seed),
+    with the collection probe every `probe_every` substeps."""
+    for k, seed in enumerate(seeds):
+        cfg, st, tris = dam_break_variant(seed, physical)
+        with Engine(cfg) as e:
+            e.init(st)
+            e.init_sdf(tris)
+            e.set_corrector(None, ratio=ratio)
+            done = 0
+            probe = 0
+            while done + ratio <= substeps:
+                if done % probe_every == 0:
+                    corr.collect(e, samples, seed=seed * 100003 + probe)
+                    probe += 1
+                    done += ratio
+                else:
+                    step = min(probe_every - done % probe_every, substeps - done)
+                    e.step(step)
+                    done += step
+        log(f"variant {k + 1}/{len(seeds)} seed {seed}: {corr.size} samples")
+
+
+def train(corr: Corrector, steps: int, batch: int = 65536, lr: float = 1e-3, seed: int = 0, log=print,
+          chunk: int = 1000):
+    """Adam with a cosine learning-rate decay, in chunks of `chunk` steps."""
+    corr.init(seed)
+    losses = []
+    done = 0
+    t0 = time.perf_counter()
+    while done < steps:
+        k = min(chunk, steps - done)
+        frac = (done + 0.5 * k) / steps
+        cur = lr * (0.05 + 0.95 * 0.5 * (1 + np.cos(np.pi * frac)))
+        losses.append(corr.train(k, batch=batch, lr=float(cur), seed=seed * 7919 + done))
+        done += k
+        log(f"step {done}/{steps}: loss {losses[-1]:.5f} lr {cur:.2e} ({time.perf_counter() - t0:.1f} s)")
+    return losses, time.perf_counter() - t0
+
+
+def density_field(pos: np.ndarray, cfg, device="cuda"):
+    """B-spline node mass of unit-mass particles (the P2G mass field), as a
+    torch tensor on `device`."""
+    import torch
+    x = torch.as_tensor(pos, dtype=torch.float32, device=device)
+    base = torch.floor(x - 0.5)
+    fx = x - base
+    w = torch.stack([0.5 * (1.5 - fx) ** 2, 0.75 - (fx - 1.0) ** 2, 0.5 * (fx - 0.5) ** 2], 0)  # (3, n, 3)
+    size = torch.tensor([cfg.size_x, cfg.size_y, cfg.size_z], device=device)
+    g = torch.zeros(cfg.size_x * cfg.size_y * cfg.size_z, dtype=torch.float64, device=device)
+    bi = base.long()
+    for a in range(3):
+        for b in range(3):
+            for c in range(3):
+                node = bi + torch.tensor([a, b, c], device=device)
+                ok = ((node >= 0) & (node < size)).all(1)
+                idx = (node[:, 2] * cfg.size_y + node[:, 1]) * cfg.size_x + node[:, 0]
+                wt = w[a, :, 0] * w[b, :, 1] * w[c, :, 2]
+                g.index_add_(0, idx[ok], wt[ok].double())
+    return g
+
+
+def compare(cfg, pos_learned: np.ndarray, pos_plain: np.ndarray) -> dict:
+    import torch
+    ml, mp = density_field(pos_learned, cfg), density_field(pos_plain, cfg)
+    rho0 = 1.0 / float(cfg.resolution) ** 3
+    occ = mp > 0.5 * rho0
+    d = np.linalg.norm(pos_learned.astype(np.float64) - pos_plain, axis=1)
+    return {
+        "density_err": float((ml - mp).abs().sum() / mp.sum()),
+        "density_err_occupied": float(((ml - mp).abs()[occ] / rho0).mean()) if bool(occ.any()) else 0.0,
+        "divergence_cells": float(d.mean()),
+        "divergence_p95_cells": float(np.percentile(d, 95)),
+    }
+
+
+def _timed(fn):
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = fn()
+    torch.cuda.synchronize()
+    return out, time.perf_counter() - t0
+
+
+def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_density_change: float = 0.02,
+             checkpoints=(100,)) -> dict:
+    """Plain (ratio * nlarge substeps) vs learned (nlarge large steps) vs the
+    uncorrected large step, from the same state; metrics at each checkpoint
+    (in large steps) and at the end."""
+    marks = sorted(set([c for c in checkpoints if c <= nlarge] + [nlarge]))
+    res = {"ratio": ratio, "large_steps": nlarge, "max_density_change": max_density_change}
+    runs = {}
+    for tag in ("plain", "learned", "uncorrected"):
+        with Engine(cfg) as e:
+            e.init(st)
+            e.init_sdf(tris)
+            if tag == "learned":
+                e.set_corrector(params, ratio=ratio, max_density_change=max_density_change)
+            elif tag == "uncorrected":
+                e.set_corrector(None, ratio=ratio)
+            pos, total, prev, stats = {}, 0.0, 0, {}
+            for m in marks:
+                k = m - prev
+                if tag == "plain":
+                    _, dt = _timed(lambda: e.step(k * ratio))
+                else:
+                    stats, dt = _timed(lambda: e.step_learned(k))
+                total += dt
+                prev = m
+                pos[m] = e.get_positions().copy()
+            sim_time = nlarge * ratio * float(cfg.dt)
+            runs[tag] = pos
+            res[tag] = {"seconds": total, "sim_time_per_s": sim_time / total,
+                        "particle_substeps_per_s": e.get_number() * nlarge * ratio / total}
+            if tag == "learned":
+                res[tag].update(stats)
+    for tag in ("learned", "uncorrected"):
+        for m in marks:
+            res[tag][f"at_{m}"] = compare(cfg, runs[tag][m], runs["plain"][m])
+    res["speedup_sim_time"] = res["learned"]["sim_time_per_s"] / res["plain"]["sim_time_per_s"]
+    return res
+
+
+def save_params(path: str, params: np.ndarray, meta: dict):
+    np.savez_compressed(path, params=params.astype(np.float32), meta=json.dumps(meta))
+
+
+def load_params(path: str = DEFAULT_PARAMS):
+    z = np.load(path)
+    return z["params"], json.loads(str(z["meta"]))
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--variants", type=int, default=200)
+    t.add_argument("--first-seed", type=int, default=5000)
+    t.add_argument("--substeps", type=int, default=1000)
+    t.add_argument("--probe-every", type=int, default=40)
+    t.add_argument("--samples", type=int, default=20000)
+    t.add_argument("--steps", type=int, default=50000)
+    t.add_argument("--batch", type=int, default=65536)
+    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--ratio", type=int, default=4)
+    t.add_argument("--physical", action="store_true")
+    t.add_argument("--out", default=DEFAULT_PARAMS)
+    ev = sub.add_parser("evaluate")
+    ev.add_argument("--params", default=DEFAULT_PARAMS)
+    ev.add_argument("--large-steps", type=int, default=250)
+    ev.add_argument("--threshold", type=float, default=0.02)
+    ev.add_argument("--physical", action="store_true")
+    ev.add_argument("--seed", type=int, default=1235)
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        seeds = list(range(a.first_seed, a.first_seed + a.variants))
+        probes = a.substeps // a.probe_every
+        cap = a.variants * (probes + 1) * a.samples
+        t0 = time.perf_counter()
+        with Corrector(cap) as c:
+            collect(c, seeds, a.substeps, a.probe_every, a.samples, a.ratio, a.physical)
+            t_collect = time.perf_counter() - t0
+            losses, t_train = train(c, a.steps, a.batch, a.lr)
+            params = c.get_params()
+            meta = {"variants": a.variants, "first_seed": a.first_seed, "substeps": a.substeps,
+                    "probe_every": a.probe_every, "samples_per_probe": a.samples, "dataset": c.size,
+                    "steps": a.steps, "batch": a.batch, "lr": a.lr, "ratio": a.ratio, "physical": a.physical,
+                    "losses": losses, "collect_s": t_collect, "train_s": t_train}
+        save_params(a.out, params, meta)
+        print(json.dumps({k: v for k, v in meta.items() if k != "losses"} | {"final_loss": losses[-1]}))
+    else:
+        params, meta = load_params(a.params)
+        cfg, st, tris = scenes.dam_break(seed=a.seed)
+        if a.physical:
+            cfg = physical_config(cfg)
+        res = evaluate(cfg, st, tris, params, nlarge=a.large_steps, ratio=int(meta.get("ratio", 4)),
+                       max_density_change=a.threshold)
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()
