@@ -54,6 +54,8 @@ def parse_args(argv=None):
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20, help="timed frames (each = SUBSTEPS substeps)")
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned 4xDT leg")
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--workload", choices=sorted(SEEDS), default="dam_break_2M")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget (0: skip)")
@@ -291,6 +293,9 @@ def run_engine(args, rank, world, local):
     for _ in range(max(args.warmup, 3)):
         eng.step_async(sub)
     eng.synchronize()
+    # Launch shapes: the engine's autotuner, timed on these particles (it
+    # does not advance the state).
+    tuning = None if args.no_autotune else eng.autotune(3)
 
     # Timed region: K frames, device time on the engine's stream.
     launches0 = eng.stats()["kernel_launches"]
@@ -355,6 +360,8 @@ def run_engine(args, rank, world, local):
             read_positions = lambda: eng2.get_positions(pos_pin)
         lib = mpm_b200.lib
         init2()  # warm the allocation path once
+        if tuning:
+            eng2.set_tuning(tuning["p2g_ctas_per_sm"], tuning["g2p_block"], tuning["grid_block"])
         eng2.step(sub)
         dist.barrier()
         t0 = time.perf_counter()
@@ -374,18 +381,49 @@ def run_engine(args, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0 and not batched:
         cpu = cpu_baseline(args.workload, args.cpu_seconds, eng.get_sdf())
+    learned = None
+    if not args.no_learned and args.workload == "dam_break_2M" and not batched:
+        learned = learned_leg(cfg, st, tris, local)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism=f"replicas{world}"),
+            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism=f"replicas{world}",
+                           tuning=None if tuning is None else
+                           {k: (round(v, 5) if isinstance(v, float) else v) for k, v in tuning.items()}),
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk.summary(), "stage_ms_per_substep": {k: round(v, 5) for k, v in per_sub.items()},
             "impl": "engine"}
+    if learned is not None:
+        line["learned"] = learned
     eng.close()
     dist.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def learned_leg(cfg, st, tris, device):
+    """The learned 4xDT path beside the plain engine on the same scene: both
+    from the same state, plain for 4 x 100 substeps, learned for 100 large
+    steps (density-change fallback at 2 %), simulated time per second of each
+    (host wall clock around synchronous calls: the learned step reads its
+    fallback statistic every large step), and the learned state's distance
+    from the plain one; "perturbed" is the plain run from positions moved by
+    1e-4 cells, the scene's chaos floor."""
+    from mpm_b200 import learned as L
+    if not os.path.exists(L.DEFAULT_PARAMS):
+        return {"unavailable": "no trained corrector parameters (mpm_b200/corrector_dam_break.npz)"}
+    params, meta = L.load_params()
+    res = L.evaluate(cfg, st, tris, params, nlarge=100, ratio=int(meta.get("ratio", 4)), max_density_change=0.02,
+                     checkpoints=(10, 25, 100))
+    out = {"ratio": res["ratio"], "large_steps": res["large_steps"], "max_density_change": 0.02,
+           "speedup_sim_time": round(res["speedup_sim_time"], 3),
+           "sim_time_per_s": {k: round(res[k]["sim_time_per_s"], 2) for k in ("plain", "learned", "uncorrected")},
+           "fallbacks": res["learned"].get("fallbacks"), "trained_on": {k: meta.get(k) for k in
+                                                                       ("variants", "dataset", "steps", "batch")}}
+    for tag in ("learned", "uncorrected", "perturbed"):
+        out[tag] = {m: {k: round(v, 4) for k, v in res[tag][f"at_{m}"].items()} for m in (10, 25, 100)}
+    return out
 
 
 # -------------------------------------------------------- reference arm ----

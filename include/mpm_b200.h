@@ -373,10 +373,151 @@ mpm_status mpm_sort_particles_device_static(const float* d_pos_x, const float* d
                                             int64_t n, int32_t* d_keys, int32_t* d_perm, void* stream);
 
 /* ------------------------------------------------------------------ */
+/* Headless screen-space fluid rendering                                */
+/* ------------------------------------------------------------------ */
+/* The reference's SSF passes (renderer.cpp:199-338; shaders ssf_depth.vert/
+ * .frag, ssf_blur.frag, screen.frag) as CUDA kernels writing device image
+ * buffers; no graphics API.  Images are width x height, row 0 at the bottom
+ * (GL window coordinates), RGB float in [0, 1+] (the composite can exceed 1
+ * by the specular term; the 8-bit copy clamps like a framebuffer). */
+typedef struct mpm_render_params {
+    int32_t width, height;        /* 1920 x 1600 (renderer.h:11-12) */
+    int32_t grid[3];              /* SIZE_X, SIZE_Y, SIZE_Z: camera and centre */
+    float fov_y_degrees;          /* 45 */
+    float near_clip, far_clip;    /* 0.1, 5000 */
+    float zoom_distance;          /* camera z: SIZE_Z * 2 */
+    float rotation;               /* about y through the grid centre (radians) */
+    float rotation_vertical;      /* about x */
+    float radius;                 /* sprite radius 2 */
+    float filter_size;            /* blur half-width 10 */
+    float depth_falloff;          /* 0.01 */
+    float light_dir[3];           /* world, (0.2, 10, 0.5) */
+    float clear_color[3];         /* background (0.85, 0.9, 0.95) */
+} mpm_render_params;
+typedef struct mpm_renderer mpm_renderer;
+void mpm_render_params_default(mpm_render_params* params, int32_t size_x, int32_t size_y, int32_t size_z);
+mpm_status mpm_renderer_create(const mpm_render_params* params, int32_t device, mpm_renderer** out);
+void mpm_renderer_destroy(mpm_renderer* renderer);
+const char* mpm_renderer_last_error(const mpm_renderer* renderer);
+/* Background image (width x height RGB8, row 0 at the bottom) in place of
+ * the clear colour: what the framebuffer held before the fluid pass. */
+mpm_status mpm_renderer_set_background(mpm_renderer* renderer, const uint8_t* rgb8_host);
+/* All passes for n positions (float3, device memory), enqueued on `stream`. */
+mpm_status mpm_render_points(mpm_renderer* renderer, const float* xyz_device, int64_t n, void* stream);
+/* All passes for the engine's current positions, on the engine's stream. */
+mpm_status mpm_render_frame(mpm_renderer* renderer, mpm_engine* engine);
+/* which: 0 = splat depth (view z, 99999 where no sprite), 1 = after the
+ * horizontal blur, 2 = after the vertical blur. */
+mpm_status mpm_renderer_get_depth(mpm_renderer* renderer, int32_t which, float* depth_host);
+/* Final colour as float RGB and / or 8-bit RGB (either may be NULL). */
+mpm_status mpm_renderer_get_image(mpm_renderer* renderer, float* rgb_host, uint8_t* rgb8_host);
+
+/* ------------------------------------------------------------------ */
+/* Checkpoints (no counterpart in the reference)                        */
+/* ------------------------------------------------------------------ */
+/* One file per engine of one scene, little-endian: a 128-byte header
+ * ("MPMCKPT1", version 1, header size 128, n, substeps done, the config
+ * fields, VOL, MASS, note length), the note (e.g. the config text), the state
+ * in the 26-plane layout of mpm_get_state (original particle order), the SDF
+ * (G floats), and a CRC-32 of everything before it.  Written to PATH.part and
+ * renamed, so a crash never leaves a truncated file under PATH.  Loading
+ * creates an engine with the state taken as it is (no initFMatrices) and the
+ * SDF restored; it continues as the saved engine would, up to the order of
+ * float sums. */
+mpm_status mpm_checkpoint_save(mpm_engine* engine, const char* path, const char* note);
+mpm_status mpm_checkpoint_load(const char* path, int32_t device, mpm_engine** out);
+/* Header and note of a checkpoint (any output may be NULL). */
+mpm_status mpm_checkpoint_info(const char* path, mpm_config* cfg, int64_t* n, int64_t* substeps, char* note,
+                               int32_t note_len);
+
+/* ------------------------------------------------------------------ */
+/* Scene construction from WATER= / OBJECT= entries                     */
+/* ------------------------------------------------------------------ */
+/* Simulation::Simulation()'s scene part (Simulation.cpp:4-38): each WATER
+ * model is loaded (ObjLoader::loadObj), voxelised at 100 voxels along its
+ * longest side (VoxelEngine::voxelize, VoxelEngine.cpp:120-243: the voxels
+ * the surface triangles touch), normalised into a SIZE_X cube, scaled so the
+ * longest side is `scale` cells, displaced, and snapped to the lattice of
+ * step getInt("RESOLUTION") with a 5x5x5 dilation (VoxelEngine::normalize,
+ * VoxelEngine.cpp:245-494); the particles of all WATER entries are
+ * concatenated (MergeVoxelData) in the layout of VoxelPipeline::process.
+ * OBJECT models give triangles (extractTriangles), normalised the same way
+ * and culled to those with a vertex in [0, SIZE_X]^3 (VoxelEngine.cpp:601-827).
+ * The triangle-box tests and the dilation run on `device`.  Model paths are
+ * relative to base_dir (the reference opens them from the working directory;
+ * NULL or "" = as given).  A WATER model that cannot be read, or that gives
+ * no voxels, fails the build (the reference throws); an OBJECT model that
+ * cannot be read is skipped and noted in mpm_scene_data_log.  A lattice step
+ * below 1 (RESOLUTION < 1, where the reference divides by zero,
+ * VoxelEngine.cpp:369-381) is MPM_ERR_BAD_CONFIG. */
+typedef struct mpm_scene_data mpm_scene_data;
+mpm_status mpm_scene_build(const char* config_text, const char* base_dir, int32_t device, mpm_scene_data** out);
+void mpm_scene_data_free(mpm_scene_data* scene);
+int64_t mpm_scene_data_num_particles(const mpm_scene_data* scene);
+int64_t mpm_scene_data_num_triangles(const mpm_scene_data* scene);
+/* 26 * n floats: positions, zeros, VOL = MASS = 1 (VoxelPipeline.cpp:5-33);
+ * mpm_init_particles applies initFMatrices to it. */
+mpm_status mpm_scene_data_state(const mpm_scene_data* scene, float* soa26_host);
+mpm_status mpm_scene_data_triangles(const mpm_scene_data* scene, float* triangles9_host);
+const char* mpm_scene_data_log(const mpm_scene_data* scene);
+const char* mpm_scene_last_error(void);
+
+/* The stages one by one.  A mesh is an OBJ's vertices and triangles (faces
+ * triangulated as tinyobjloader's LoadObj does; see csrc/scene.cu). */
+typedef struct mpm_mesh mpm_mesh;
+mpm_status mpm_mesh_load_obj(const char* path, mpm_mesh** out);
+mpm_status mpm_mesh_from_obj_text(const char* text, mpm_mesh** out);
+void mpm_mesh_free(mpm_mesh* mesh);
+int64_t mpm_mesh_num_vertices(const mpm_mesh* mesh);
+int64_t mpm_mesh_num_triangles(const mpm_mesh* mesh);
+/* Any output may be NULL: 3 floats per vertex, 3 indices per triangle,
+ * 9 floats per triangle (VoxelEngine::extractTriangles). */
+mpm_status mpm_mesh_get(const mpm_mesh* mesh, float* vertices3_host, int32_t* faces3_host, float* triangles9_host);
+
+/* A point set (x y z per point). */
+typedef struct mpm_points mpm_points;
+/* VoxelEngine::voxelize(obj, resolution): voxel centres in z, y, x order. */
+mpm_status mpm_voxelize(const mpm_mesh* mesh, float resolution, int32_t device, mpm_points** out);
+mpm_status mpm_points_create(const float* xyz_host, int64_t n, mpm_points** out);
+int64_t mpm_points_count(const mpm_points* points);
+mpm_status mpm_points_get(const mpm_points* points, float* xyz_host);
+void mpm_points_free(mpm_points* points);
+/* VoxelEngine::normalize(VoxelData&, normalizeSize, scale, displacement) in
+ * place, with the lattice step getInt("RESOLUTION"); the result is in
+ * (x, y, z) lexicographic order. */
+mpm_status mpm_points_normalize(mpm_points* points, float normalize_size, float scale, const float* displacement3,
+                                int32_t lattice_step, int32_t device);
+/* VoxelEngine::normalize(std::vector<Triangle>&, ...) in place; *t shrinks
+ * by the culled triangles.  Host only. */
+mpm_status mpm_triangles_normalize(float* triangles9_host, int64_t* t, float normalize_size, float scale,
+                                   const float* displacement3);
+
+/* ------------------------------------------------------------------ */
+/* Launch-shape tuning                                                   */
+/* ------------------------------------------------------------------ */
+/* The substep's launch shapes: persistent P2G CTAs per SM, and the CTA
+ * sizes of the plain G2P and of the grid update.  mpm_autotune times each
+ * candidate on the engine's current particles (each stage on its own, the
+ * median of `repeats` runs; every timed substep is undone, so the state does
+ * not advance) and keeps the fastest; results are identical for every shape
+ * up to the order of float sums. */
+typedef struct mpm_tuning {
+    int32_t p2g_ctas_per_sm;  /* 1 .. the most that fit (default 12) */
+    int32_t g2p_block;        /* 128 or 256 (default 256) */
+    int32_t grid_block;       /* 128 or 256 (default 256) */
+    float p2g_ms, g2p_ms, grid_ms;  /* stage times of the chosen shapes (mpm_autotune) */
+} mpm_tuning;
+mpm_status mpm_autotune(mpm_engine* engine, int32_t repeats, mpm_tuning* out);
+mpm_status mpm_set_tuning(mpm_engine* engine, const mpm_tuning* tuning);
+mpm_status mpm_get_tuning(mpm_engine* engine, mpm_tuning* tuning);
+
+/* ------------------------------------------------------------------ */
 /* Learned large step (no counterpart in the reference)                 */
 /* ------------------------------------------------------------------ */
 /* Beside the plain substep, never replacing it: one substep of RATIO x DT
- * whose G2P adds a velocity correction predicted per particle by a small MLP
+ * (particles advect with v_old + (RATIO + 1) / (2 RATIO) (v_new - v_old),
+ * the displacement of RATIO substeps under a constant acceleration) whose
+ * G2P adds a velocity correction predicted per particle by a small MLP
  * (16 -> 64 -> 64 -> 3, GELU, bf16 weights on the tensor cores, fp32
  * accumulation).  Inputs: the particle's APIC matrix C (9), grid velocity
  * (3), interpolated grid mass over the seeding density, minus 1 (1), and the

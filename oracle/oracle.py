@@ -6,6 +6,7 @@ The engine under test never calls into this module.
 
 * `Oracle(64)` - FP64 restatement of the reference step (lib/libmpm_oracle64.so)
 * `Oracle(32)` - FP32 OpenMP restatement, the timed CPU baseline
+* `SceneOracle` - scene construction from OBJ models (lib/libscene_oracle.so)
 * `RefEngine`  - the reference's own Engine compiled from its sources
                  (_ref/libref_engine.so); needs a GPU.
 """
@@ -212,3 +213,68 @@ class RefEngine:
 
     def destroy(self):
         self.lib.ref_engine_destroy()
+
+
+class SceneOracle:
+    """CPU restatement of the reference's OBJ -> particles / triangles path."""
+
+    def __init__(self):
+        path = os.path.join(HERE, "lib", "libscene_oracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: run `make -C oracle`")
+        self.lib = ctypes.CDLL(path)
+        P, L = ctypes.c_void_p, ctypes.c_long
+        PP = ctypes.POINTER(ctypes.c_void_p)
+        for name, res, args in [
+            ("sco_free", None, [P]),
+            ("sco_parse_obj", L, [ctypes.c_char_p, PP, ctypes.POINTER(L), PP, ctypes.POINTER(L)]),
+            ("sco_voxelize", L, [P, L, P, L, ctypes.c_float, PP]),
+            ("sco_normalize", L, [P, L, ctypes.c_float, ctypes.c_float, P, ctypes.c_int, PP]),
+            ("sco_normalize_triangles", L, [P, L, ctypes.c_float, ctypes.c_float, P]),
+        ]:
+            f = getattr(self.lib, name)
+            f.restype = res
+            f.argtypes = args
+
+    def _take(self, ptr, count, dtype):
+        if not ptr:
+            return np.zeros(0, dtype)
+        buf = (ctypes.c_char * (count * np.dtype(dtype).itemsize)).from_address(ptr)
+        out = np.frombuffer(bytes(buf), dtype=dtype).copy()
+        self.lib.sco_free(ptr)
+        return out
+
+    def parse_obj(self, text: str):
+        """(vertices (nv, 3) float32, faces (nt, 3) int32); raises on a malformed file."""
+        v, f = ctypes.c_void_p(), ctypes.c_void_p()
+        nv, nt = ctypes.c_long(), ctypes.c_long()
+        line = self.lib.sco_parse_obj(text.encode(), ctypes.byref(v), ctypes.byref(nv), ctypes.byref(f),
+                                      ctypes.byref(nt))
+        if line:
+            raise ValueError(f"OBJ line {line}")
+        return (self._take(v.value, 3 * nv.value, np.float32).reshape(-1, 3),
+                self._take(f.value, 3 * nt.value, np.int32).reshape(-1, 3))
+
+    def voxelize(self, verts, faces, resolution: float = 100.0):
+        v = np.ascontiguousarray(verts, np.float32)
+        f = np.ascontiguousarray(faces, np.int32)
+        out = ctypes.c_void_p()
+        n = self.lib.sco_voxelize(_p(v), len(v), _p(f), len(f), resolution, ctypes.byref(out))
+        if n < 0:
+            raise ValueError("degenerate mesh")
+        return self._take(out.value, 3 * n, np.float32).reshape(-1, 3)
+
+    def normalize(self, pts, size: float, scale: float, disp, step: int):
+        p = np.ascontiguousarray(pts, np.float32)
+        d = np.ascontiguousarray(disp, np.float32)
+        out = ctypes.c_void_p()
+        n = self.lib.sco_normalize(_p(p), len(p), size, scale, _p(d), step, ctypes.byref(out))
+        if n < 0:
+            raise ValueError("lattice step below 1")
+        return self._take(out.value, 3 * n, np.float32).reshape(-1, 3)
+
+    def normalize_triangles(self, tris, size: float, scale: float, disp):
+        t = np.ascontiguousarray(tris, np.float32).reshape(-1, 9).copy()
+        d = np.ascontiguousarray(disp, np.float32)
+        k = self.lib.sco_normalize_triangles(_p(t), len(t), size, scale, _p(d))
+        return t[:k]

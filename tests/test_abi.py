@@ -95,3 +95,18 @@ def test_corrector_layout_matches_header():
                         ("W1", "W1"), ("b1", "b1"), ("W2", "W2"), ("b2", "b2"), ("W3", "W3"), ("b3", "b3")):
         m = re.search(re.escape(label) + r" \[[^\]]*\](?:\[[^\]]*\])?[\s*]*@(\d+)", hdr)
         assert m and int(m.group(1)) == mlp_ref.OFF[name][0], name
+
+
+def test_cli_usage_and_checkpoint_errors_without_gpu(tmp_path):
+    import subprocess
+    cli = os.path.join(ROOT, "water-sim-cuda_b200", "bin", "mpm_run")
+    r = subprocess.run([cli], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
+    import mpm_b200
+    with pytest.raises(mpm_b200.MpmError) as ei:
+        mpm_b200.checkpoint_info(str(tmp_path / "none.ckpt"))
+    assert ei.value.name == "MPM_ERR_IO"
+    (tmp_path / "x.ckpt").write_bytes(b"NOTACKPT" + bytes(200))
+    with pytest.raises(mpm_b200.MpmError) as ei:
+        mpm_b200.checkpoint_info(str(tmp_path / "x.ckpt"))
+    assert "magic" in str(ei.value)

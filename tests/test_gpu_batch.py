@@ -97,3 +97,30 @@ def test_batch_errors(gpu_ok, mpm):
     assert np.array_equal(a0[24:26], a1[24:26])
     # identical scenes evolve identically up to float-sum order
     assert np.abs(a0[0:3].astype(np.float64) - a1[0:3]).max() < 1e-4
+
+
+def test_autotune_keeps_state_and_results(gpu_ok, mpm):
+    sc = _scenes()
+    with _batch(mpm, sc) as b:
+        b.step(2)
+        before = [b.scene_buffer(k) for k in range(len(sc))]
+        t = b.autotune(repeats=2)
+        assert t["p2g_ctas_per_sm"] >= 1 and t["g2p_block"] in (128, 256) and t["grid_block"] in (128, 256)
+        assert t["p2g_ms"] > 0 and t["g2p_ms"] > 0 and t["grid_ms"] > 0
+        assert b.tuning()["p2g_ctas_per_sm"] == t["p2g_ctas_per_sm"]
+        after = [b.scene_buffer(k) for k in range(len(sc))]
+        for x, y in zip(before, after):
+            assert np.array_equal(x, y)  # tuning does not advance the state
+        assert b.stats()["substeps"] == 2
+        b.step(3)
+        tuned = [b.scene_buffer(k) for k in range(len(sc))]
+    with _batch(mpm, sc) as b:
+        b.step(2)
+        b.set_tuning(4, 128, 128)
+        b.step(3)
+        other = [b.scene_buffer(k) for k in range(len(sc))]
+        with pytest.raises(mpm.MpmError):
+            b.set_tuning(0, 256, 256)
+    for k, (x, y) in enumerate(zip(tuned, other)):
+        if x.shape[1]:
+            assert_state_close(x, y.astype(np.float64), before[k], rtol=1e-4)

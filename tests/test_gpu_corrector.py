@@ -90,19 +90,25 @@ def _small(mpm, n=3000, obstacle=False, seed=11, **kw):
     return scenes.small_scene(n, (32, 32, 32), seed=seed, obstacle=obstacle, **kw)
 
 
-def test_uncorrected_large_step_is_substep_at_ratio_dt(gpu_ok, mpm, oracle64):
-    cfg, st, tris = _small(mpm, obstacle=True)
+@pytest.mark.parametrize("ratio", [1, 4])
+def test_uncorrected_large_step_is_substep_at_ratio_dt(gpu_ok, mpm, oracle64, ratio):
+    """Velocity, C and F: the substep at RATIO x DT.  Positions: advected
+    with v_old + (R + 1) / (2R) (v_new - v_old) (R = 1: the plain substep)."""
+    cfg, st, tris = _small(mpm, obstacle=False)
     with mpm.Engine(cfg) as e:
         e.init(st)
-        e.init_sdf(tris)
         start = e.get_buffer()
         sdf = e.get_sdf()
-        e.set_corrector(None, ratio=4)
+        e.set_corrector(None, ratio=ratio)
         stats = e.step_learned(1)
         got = e.get_buffer()
         assert stats["large_steps"] == 1 and stats["fallbacks"] == 0
-    big = dataclasses.replace(cfg, dt=float(np.float32(cfg.dt) * 4))
+    dt = float(np.float32(cfg.dt) * ratio)
+    big = dataclasses.replace(cfg, dt=dt)
     want, _, _, _ = oracle64.substep(big, start.astype(np.float64), sdf.astype(np.float64))
+    blend = (ratio + 1) / (2 * ratio)
+    v0 = start[3:6].astype(np.float64)
+    want[0:3] = start[0:3] + dt * (v0 + blend * (want[3:6] - v0))
     assert_state_close(got, want, start)
 
 
@@ -127,8 +133,9 @@ def test_zero_correction_and_bias_wiring(gpu_ok, mpm):
     assert np.abs(z[0:6] - a[0:6]).max() < 1e-4
     dv = np.array([0.05, -0.1, 0.15], np.float32)[:, None]
     dt = np.float32(cfg.dt) * 4
+    blend = 5.0 / 8.0
     assert np.abs((b[3:6] - a[3:6]) - dv).max() < 1e-4
-    assert np.abs((b[0:3] - a[0:3]) - dt * dv).max() < 1e-4 * max(1.0, float(dt))
+    assert np.abs((b[0:3] - a[0:3]) - dt * blend * dv).max() < 1e-4 * max(1.0, float(dt))
 
 
 def test_fallback_runs_plain_substeps(gpu_ok, mpm):

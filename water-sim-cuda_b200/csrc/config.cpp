@@ -212,3 +212,15 @@ extern "C" mpm_status mpm_config_parse_file(const char* path, mpm_config* cfg, m
     }
     return finish(in, cfg, waters, max_waters, n_waters, objects, max_objects, n_objects, err, err_len);
 }
+
+namespace mpm {
+// `key` of a config text read as GameConfigData::getInt reads it (std::stoi of
+// the space-stripped value): the scene builder's lattice step is
+// getInt("RESOLUTION") (VoxelEngine.cpp:369), not the float the kernels use.
+bool config_text_int(const char* text, const char* key, int32_t* out, std::string& err) {
+    std::istringstream in(text ? text : "");
+    Parsed p;
+    if (!parse_text(in, p, err)) return false;
+    return get_int(p, key, out, err);
+}
+}  // namespace mpm

@@ -142,6 +142,9 @@ struct mpm_engine {
     int64_t large_steps = 0;
     int64_t fallbacks = 0;
     double last_density_change = 0.0;
+
+    // Launch shapes of the substep (mpm_autotune / mpm_set_tuning).
+    mpm_tuning tune{12, 256, 256, 0.f, 0.f, 0.f};
 };
 
 namespace {
@@ -278,15 +281,16 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
     mark(1);
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
         launches += mpm::launch_p2g(sc, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par], e->d_itemoff,
-                                    work, e->accum, e->d_flags + 1, st);
+                                    work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm);
     mark(2);
     if (from <= MPM_STAGE_GRID && upto >= MPM_STAGE_GRID)
-        launches += mpm::launch_grid_update(sc, e->prm[0], e->g_total, e->accum, e->vgrid, e->sdf, st);
+        launches += mpm::launch_grid_update(sc, e->prm[0], e->g_total, e->accum, e->vgrid, e->sdf, st,
+                                            e->tune.grid_block);
     mark(3);
     if (from <= MPM_STAGE_G2P && upto >= MPM_STAGE_G2P)
         launches += mpm::launch_g2p(sc, e->prm[0], e->n, e->P[par], e->P[1 - par], e->gidx, e->sigma[par],
-                                    e->sigma[1 - par],
-                                    e->vgrid, e->sdf, e->pcell, e->prank, e->bins[1 - par], e->d_flags, st);
+                                    e->sigma[1 - par], e->vgrid, e->sdf, e->pcell, e->prank, e->bins[1 - par],
+                                    e->d_flags, st, nullptr, e->tune.g2p_block);
     mark(4);
     return launches;
 }
@@ -574,7 +578,10 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
     return MPM_OK;
 }
 
-mpm_status init_all(mpm_engine* e, const int64_t* counts, const float* const* soa26_host) {
+// init_rules: Engine::init's initFMatrices (false: the state is taken as it
+// is, with VOL and MASS from vol / mass when given).
+mpm_status init_all(mpm_engine* e, const int64_t* counts, const float* const* soa26_host, bool init_rules = true,
+                    const float* vol = nullptr, const float* mass = nullptr) {
     long long total = 0;
     int max_n = 0;
     size_t sort_bytes = mpm::sort_scratch_bytes(1);  // radix-sort scratch of mpm_get_sort: any scene
@@ -593,13 +600,13 @@ mpm_status init_all(mpm_engine* e, const int64_t* counts, const float* const* so
         SimParams& p = e->prm[s];
         p.n = (int)counts[s];
         p.poff = off;
-        p.pvol = e->cfg[s].resolution * e->cfg[s].resolution * e->cfg[s].resolution;
-        p.pmass = 1.0f;
+        p.pvol = vol ? vol[s] : e->cfg[s].resolution * e->cfg[s].resolution * e->cfg[s].resolution;
+        p.pmass = mass ? mass[s] : 1.0f;
         off += counts[s];
     }
     if ((st = upload_table(e)) != MPM_OK) return st;
     e->substeps = 0;
-    return load_states(e, soa26_host, true);
+    return load_states(e, soa26_host, init_rules);
 }
 
 // ------------------------------------------------------ learned step ----
@@ -630,8 +637,13 @@ mpm_status prepare_large(mpm_engine* e) {
     return MPM_OK;
 }
 
+// Advection blend of the large step: RATIO substeps under a constant
+// acceleration move a particle by RATIO DT (v_old + (RATIO + 1) / (2 RATIO)
+// (v_new - v_old)).
+float large_blend(const mpm_engine* e) { return (float)(e->ratio + 1) / (float)(2 * e->ratio); }
+
 // One substep of RATIO x DT from parity `par` into 1 - par (learn: the
-// learned or collection G2P; null: the uncorrected large step).
+// learned, collection or uncorrected large-step G2P).
 int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
     cudaStream_t st = e->stream;
     uint32_t* work = e->ctl + 2 * e->scenes;
@@ -640,8 +652,9 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
     launches += mpm::launch_bin_order(e->table, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart,
                                       e->cstart, e->pcell, e->prank, e->gidx, e->d_itemoff, work, st);
     launches += mpm::launch_p2g(e->table_large, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par],
-                                e->d_itemoff, work, e->accum, e->d_flags + 1, st);
-    launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, st);
+                                e->d_itemoff, work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm);
+    launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, st,
+                                        e->tune.grid_block);
     launches += mpm::launch_g2p(e->table_large, big, e->n, e->P[par], e->P[1 - par], e->gidx, e->sigma[par],
                                 e->sigma[1 - par], e->vgrid, e->sdf, e->pcell, e->prank, e->bins[1 - par], e->d_flags,
                                 st, learn);
@@ -1095,9 +1108,9 @@ extern "C" mpm_status mpm_step_learned(mpm_engine* e, int32_t nlarge, mpm_learne
     if ((s = learned_ready(e)) != MPM_OK) return s;
     for (int k = 0; k < nlarge; ++k) {
         const int par = e->parity;
-        mpm::LearnArgs la{e->mlp, nullptr, nullptr, e->d_stat};
+        mpm::LearnArgs la{e->mlp_set ? e->mlp : nullptr, nullptr, nullptr, e->d_stat, large_blend(e)};
         if (e->mlp_set) CK(e, cudaMemsetAsync(e->d_stat, 0, sizeof(float), e->stream));
-        e->kernel_launches += enqueue_large(e, par, e->mlp_set ? &la : nullptr);
+        e->kernel_launches += enqueue_large(e, par, &la);
         CK(e, cudaGetLastError());
         e->sort_src = par;
         bool accept = true;
@@ -1143,7 +1156,7 @@ extern "C" mpm_status mpm_corrector_collect(mpm_corrector* c, mpm_engine* e, int
     // The uncorrected large step, recording features and final velocities;
     // then back to its start state for RATIO plain substeps.
     const int par = e->parity;
-    mpm::LearnArgs la{nullptr, e->feat_all, e->vlarge, nullptr};
+    mpm::LearnArgs la{nullptr, e->feat_all, e->vlarge, nullptr, large_blend(e)};
     e->kernel_launches += enqueue_large(e, par, &la);
     CK(e, cudaGetLastError());
     if ((s = rebin(e, par)) != MPM_OK) return s;
@@ -1160,4 +1173,321 @@ extern "C" mpm_status mpm_corrector_collect(mpm_corrector* c, mpm_engine* e, int
     if ((s = export_positions(e)) != MPM_OK) return s;
     if ((s = sync_and_collect(e)) != MPM_OK) return s;
     return check_health(e);
+}
+
+// ---------------------------------------------------------- checkpoint ----
+namespace {
+
+constexpr char kCkptMagic[8] = {'M', 'P', 'M', 'C', 'K', 'P', 'T', '1'};
+constexpr uint32_t kCkptVersion = 1;
+constexpr uint32_t kCkptHeader = 128;
+
+uint32_t crc32_update(uint32_t crc, const void* data, size_t len) {
+    static uint32_t table[256];
+    static bool ready = false;
+    if (!ready) {
+        for (uint32_t i = 0; i < 256; ++i) {
+            uint32_t c = i;
+            for (int k = 0; k < 8; ++k) c = (c & 1u) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
+            table[i] = c;
+        }
+        ready = true;
+    }
+    const unsigned char* b = static_cast<const unsigned char*>(data);
+    crc = ~crc;
+    for (size_t i = 0; i < len; ++i) crc = table[(crc ^ b[i]) & 0xffu] ^ (crc >> 8);
+    return ~crc;
+}
+
+template <typename T>
+void put(std::vector<unsigned char>& h, size_t off, T v) {
+    std::memcpy(h.data() + off, &v, sizeof(T));
+}
+template <typename T>
+T get(const std::vector<unsigned char>& h, size_t off) {
+    T v;
+    std::memcpy(&v, h.data() + off, sizeof(T));
+    return v;
+}
+
+struct CkptHeader {
+    int64_t n = 0, substeps = 0;
+    mpm_config cfg{};
+    float pvol = 0.f, pmass = 0.f;
+    uint64_t note_bytes = 0;
+};
+
+bool parse_header(const std::vector<unsigned char>& h, CkptHeader* out, std::string& err) {
+    if (h.size() < kCkptHeader || std::memcmp(h.data(), kCkptMagic, 8) != 0) {
+        err = "not an MPM checkpoint (bad magic)";
+        return false;
+    }
+    if (get<uint32_t>(h, 8) != kCkptVersion || get<uint32_t>(h, 12) != kCkptHeader) {
+        err = "unsupported checkpoint version";
+        return false;
+    }
+    out->n = get<int64_t>(h, 16);
+    out->substeps = get<int64_t>(h, 24);
+    out->cfg.size_x = get<int32_t>(h, 32);
+    out->cfg.size_y = get<int32_t>(h, 36);
+    out->cfg.size_z = get<int32_t>(h, 40);
+    out->cfg.padding = get<int32_t>(h, 44);
+    out->cfg.gravity = get<float>(h, 48);
+    out->cfg.dt = get<float>(h, 52);
+    out->cfg.gamma = get<float>(h, 56);
+    out->cfg.compression = get<float>(h, 60);
+    out->cfg.resolution = get<float>(h, 64);
+    out->cfg.substeps = get<int32_t>(h, 68);
+    out->cfg.sdf_resolution = get<int32_t>(h, 72);
+    out->pvol = get<float>(h, 76);
+    out->pmass = get<float>(h, 80);
+    out->note_bytes = get<uint64_t>(h, 84);
+    if (out->n < 0 || out->n > 0x7fffffffLL - 64 || out->cfg.size_x <= 0 || out->cfg.size_y <= 0 ||
+        out->cfg.size_z <= 0 || out->note_bytes > (1u << 24)) {
+        err = "corrupt checkpoint header";
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" mpm_status mpm_checkpoint_save(mpm_engine* e, const char* path, const char* note) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!path) return record(e, MPM_ERR_INVALID_ARGUMENT, "path is NULL");
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (e->scenes != 1) return record(e, MPM_ERR_UNSUPPORTED, "checkpoints hold engines of one scene");
+    const long long n = e->n;
+    const long long g = e->g_total;
+    std::vector<float> state((size_t)MPM_PARTICLE_PLANES * n), sdf((size_t)g);
+    if (n > 0 && (s = mpm_get_state(e, state.data())) != MPM_OK) return s;
+    if ((s = mpm_get_sdf(e, sdf.data())) != MPM_OK) return s;
+    const std::string txt = note ? note : "";
+    std::vector<unsigned char> h(kCkptHeader, 0);
+    std::memcpy(h.data(), kCkptMagic, 8);
+    const mpm_config& c = e->cfg[0];
+    put<uint32_t>(h, 8, kCkptVersion);
+    put<uint32_t>(h, 12, kCkptHeader);
+    put<int64_t>(h, 16, n);
+    put<int64_t>(h, 24, e->substeps);
+    put<int32_t>(h, 32, c.size_x);
+    put<int32_t>(h, 36, c.size_y);
+    put<int32_t>(h, 40, c.size_z);
+    put<int32_t>(h, 44, c.padding);
+    put<float>(h, 48, c.gravity);
+    put<float>(h, 52, c.dt);
+    put<float>(h, 56, c.gamma);
+    put<float>(h, 60, c.compression);
+    put<float>(h, 64, c.resolution);
+    put<int32_t>(h, 68, c.substeps);
+    put<int32_t>(h, 72, c.sdf_resolution);
+    put<float>(h, 76, e->prm[0].pvol);
+    put<float>(h, 80, e->prm[0].pmass);
+    put<uint64_t>(h, 84, (uint64_t)txt.size());
+    const std::string tmp = std::string(path) + ".part";
+    FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return record(e, MPM_ERR_IO, std::string("cannot write ") + tmp);
+    uint32_t crc = 0;
+    auto write = [&](const void* d, size_t len) {
+        crc = crc32_update(crc, d, len);
+        return std::fwrite(d, 1, len, f) == len;
+    };
+    bool ok = write(h.data(), h.size()) && write(txt.data(), txt.size()) &&
+              write(state.data(), state.size() * sizeof(float)) && write(sdf.data(), sdf.size() * sizeof(float));
+    ok = ok && std::fwrite(&crc, 1, sizeof(crc), f) == sizeof(crc);
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok || std::rename(tmp.c_str(), path) != 0) {
+        std::remove(tmp.c_str());
+        return record(e, MPM_ERR_IO, std::string("cannot write checkpoint ") + path);
+    }
+    return MPM_OK;
+}
+
+namespace {
+mpm_status read_checkpoint(const char* path, CkptHeader* hd, std::string* note, std::vector<float>* state,
+                           std::vector<float>* sdf) {
+    if (!path) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "path is NULL");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return record(nullptr, MPM_ERR_IO, std::string("cannot open checkpoint ") + path);
+    std::vector<unsigned char> data;
+    unsigned char buf[1 << 16];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0) data.insert(data.end(), buf, buf + got);
+    std::fclose(f);
+    std::string err;
+    if (!parse_header(data, hd, err)) return record(nullptr, MPM_ERR_IO, err);
+    const size_t g = (size_t)hd->cfg.size_x * hd->cfg.size_y * hd->cfg.size_z;
+    const size_t sbytes = (size_t)MPM_PARTICLE_PLANES * hd->n * sizeof(float);
+    const size_t want = kCkptHeader + hd->note_bytes + sbytes + g * sizeof(float) + 4;
+    if (data.size() != want) return record(nullptr, MPM_ERR_IO, "checkpoint size does not match its header");
+    uint32_t crc;
+    std::memcpy(&crc, data.data() + want - 4, 4);
+    if (crc32_update(0, data.data(), want - 4) != crc) return record(nullptr, MPM_ERR_IO, "checkpoint CRC mismatch");
+    size_t off = kCkptHeader;
+    if (note) note->assign(reinterpret_cast<const char*>(data.data() + off), hd->note_bytes);
+    off += hd->note_bytes;
+    if (state) {
+        state->resize((size_t)MPM_PARTICLE_PLANES * hd->n);
+        std::memcpy(state->data(), data.data() + off, sbytes);
+    }
+    off += sbytes;
+    if (sdf) {
+        sdf->resize(g);
+        std::memcpy(sdf->data(), data.data() + off, g * sizeof(float));
+    }
+    return MPM_OK;
+}
+}  // namespace
+
+extern "C" mpm_status mpm_checkpoint_info(const char* path, mpm_config* cfg, int64_t* n, int64_t* substeps,
+                                          char* note, int32_t note_len) {
+    g_global_error.clear();
+    CkptHeader hd;
+    std::string txt;
+    mpm_status s = read_checkpoint(path, &hd, &txt, nullptr, nullptr);
+    if (s != MPM_OK) return s;
+    if (cfg) *cfg = hd.cfg;
+    if (n) *n = hd.n;
+    if (substeps) *substeps = hd.substeps;
+    if (note && note_len > 0) {
+        const size_t k = std::min((size_t)note_len - 1, txt.size());
+        std::memcpy(note, txt.data(), k);
+        note[k] = '\0';
+    }
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_checkpoint_load(const char* path, int32_t device, mpm_engine** out) {
+    g_global_error.clear();
+    if (!out) return record(nullptr, MPM_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    CkptHeader hd;
+    std::vector<float> state, sdf;
+    mpm_status s = read_checkpoint(path, &hd, nullptr, &state, &sdf);
+    if (s != MPM_OK) return s;
+    mpm_engine* e = nullptr;
+    if ((s = create_engine(&hd.cfg, 1, device, &e)) != MPM_OK) return s;
+    const int64_t n = hd.n;
+    const float* planes = state.data();
+    s = init_all(e, &n, &planes, false, &hd.pvol, &hd.pmass);
+    if (s == MPM_OK) {
+        cudaError_t err = cudaMemcpyAsync(e->sdf, sdf.data(), sdf.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                          e->stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+        if (err != cudaSuccess) s = cuda_fail(e, err, "checkpoint sdf upload");
+    }
+    if (s != MPM_OK) {
+        g_global_error = e->last_error;
+        mpm_destroy(e);
+        return s;
+    }
+    e->substeps = hd.substeps;
+    *out = e;
+    return MPM_OK;
+}
+
+// ------------------------------------------------------------ autotune ----
+namespace {
+bool valid_tuning(const mpm_tuning& t) {
+    return t.p2g_ctas_per_sm >= 1 && t.p2g_ctas_per_sm <= mpm::p2g_max_ctas_per_sm() &&
+           (t.g2p_block == 128 || t.g2p_block == 256) && (t.grid_block == 128 || t.grid_block == 256);
+}
+
+// Times stage `stage` of one substep from the current state and undoes the
+// substep (the state of the current parity is untouched by it; the counter
+// sets are rebuilt from it).
+mpm_status time_stage(mpm_engine* e, int stage, cudaEvent_t a, cudaEvent_t b, float* ms) {
+    const int par = e->parity;
+    e->kernel_launches += enqueue_substep(e, par, MPM_STAGE_SORT, stage - 1);
+    CK(e, cudaEventRecord(a, e->stream));
+    e->kernel_launches += enqueue_substep(e, par, stage, stage);
+    CK(e, cudaEventRecord(b, e->stream));
+    e->kernel_launches += enqueue_substep(e, par, stage + 1, MPM_STAGE_G2P);
+    CK(e, cudaGetLastError());
+    CK(e, cudaEventSynchronize(b));
+    CK(e, cudaEventElapsedTime(ms, a, b));
+    mpm_status s = rebin(e, par);
+    if (s != MPM_OK) return s;
+    return sync_and_collect(e);
+}
+}  // namespace
+
+extern "C" mpm_status mpm_set_tuning(mpm_engine* e, const mpm_tuning* t) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!t || !valid_tuning(*t)) return record(e, MPM_ERR_INVALID_ARGUMENT, "tuning out of range");
+    e->tune.p2g_ctas_per_sm = t->p2g_ctas_per_sm;
+    e->tune.g2p_block = t->g2p_block;
+    e->tune.grid_block = t->grid_block;
+    return e->initialized ? capture_graphs(e) : MPM_OK;
+}
+
+extern "C" mpm_status mpm_get_tuning(mpm_engine* e, mpm_tuning* t) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!t) return record(e, MPM_ERR_INVALID_ARGUMENT, "out is NULL");
+    *t = e->tune;
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* out) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (repeats < 1 || repeats > 100) return record(e, MPM_ERR_INVALID_ARGUMENT, "repeats must be in [1, 100]");
+    if (e->accum_dirty) {
+        CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->g_total * sizeof(float4), e->stream));
+        e->accum_dirty = false;
+    }
+    e->partial_stage = 0;
+    cudaEvent_t a = nullptr, b = nullptr;
+    CK(e, cudaEventCreate(&a));
+    if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return cuda_fail(e, cudaGetLastError(), "cudaEventCreate");
+    }
+    mpm_tuning best = e->tune;
+    auto median_time = [&](int stage, float* ms) -> mpm_status {
+        std::vector<float> t(repeats);
+        for (int r = 0; r < repeats; ++r) {
+            mpm_status st = time_stage(e, stage, a, b, &t[r]);
+            if (st != MPM_OK) return st;
+        }
+        std::sort(t.begin(), t.end());
+        *ms = t[repeats / 2];
+        return MPM_OK;
+    };
+    // Each stage is its own kernel: tune them one at a time.
+    const int max_p2g = mpm::p2g_max_ctas_per_sm();
+    float tbest = 1e30f, ms = 0.f;
+    for (int k : {4, 6, 8, 10, 12, 14, 16, 20, 24}) {
+        if (k > max_p2g) break;
+        e->tune.p2g_ctas_per_sm = k;
+        if ((s = median_time(MPM_STAGE_P2G, &ms)) != MPM_OK) break;
+        if (ms < tbest) tbest = ms, best.p2g_ctas_per_sm = k, best.p2g_ms = ms;
+    }
+    e->tune.p2g_ctas_per_sm = best.p2g_ctas_per_sm;
+    tbest = 1e30f;
+    for (int k : {128, 256}) {
+        if (s != MPM_OK) break;
+        e->tune.grid_block = k;
+        if ((s = median_time(MPM_STAGE_GRID, &ms)) != MPM_OK) break;
+        if (ms < tbest) tbest = ms, best.grid_block = k, best.grid_ms = ms;
+    }
+    e->tune.grid_block = best.grid_block;
+    tbest = 1e30f;
+    for (int k : {128, 256}) {
+        if (s != MPM_OK) break;
+        e->tune.g2p_block = k;
+        if ((s = median_time(MPM_STAGE_G2P, &ms)) != MPM_OK) break;
+        if (ms < tbest) tbest = ms, best.g2p_block = k, best.g2p_ms = ms;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    e->tune = best;
+    if (s != MPM_OK) return s;
+    if ((s = capture_graphs(e)) != MPM_OK) return s;
+    if (out) *out = best;
+    return MPM_OK;
 }

@@ -74,22 +74,27 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
                      int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
                      long long* itemoff, uint32_t* work, cudaStream_t st);
 // P2G over the items of `cur`; gidx maps slots of the new order to P.
+// ctas_per_sm: persistent single-warp CTAs per SM (0 = the default 12).
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
                const int32_t* cstart, const BinSet& cur, const long long* itemoff, uint32_t* work, float4* accum,
-               uint32_t* status, cudaStream_t st);
+               uint32_t* status, cudaStream_t st, int ctas_per_sm = 0);
+// Most P2G CTAs that fit on one SM.
+int p2g_max_ctas_per_sm();
 // p0: the parameters of scene 0, used directly when the table holds one scene.
 int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
-                       const float* sdf, cudaStream_t st);
-// Large-step G2P (one scene).  With mlp set: the corrector's correction is
-// added to each particle's velocity and stat[0] += sum over particles of
-// |1 / det(I + dt C) - 1| (the step's predicted relative density change).
-// With mlp null (collection probe): feat[orig] receives the 16 features and
-// vel[orig] the final velocity, by original index.
+                       const float* sdf, cudaStream_t st, int block = 256);
+// Large-step G2P (one scene): particles advect with v_old + blend (v_new -
+// v_old).  With mlp set: the corrector's correction is added to each
+// particle's velocity and stat[0] += sum over particles of |1 / det(I + dt C)
+// - 1| (the step's predicted relative density change).  With feat set
+// (collection probe): feat[orig] receives the 16 features and vel[orig] the
+// final velocity, by original index.  Neither: the uncorrected large step.
 struct LearnArgs {
     const MlpPacked* mlp;
     float* feat;
     float* vel;
     float* stat;
+    float blend;
 };
 
 // G2P: slot j of Pout = particle gidx[j] of Pin advanced one substep;
@@ -98,7 +103,7 @@ struct LearnArgs {
 int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const float* Pin, float* Pout,
                const int32_t* gidx, const int32_t* sig_in, int32_t* sig_out, const float4* vgrid, const float* sdf,
                int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st,
-               const LearnArgs* learn = nullptr);
+               const LearnArgs* learn = nullptr, int block = 256);
 
 // The kernels below take one scene's SimParams and pointers already offset to
 // that scene's part of the arrays.

@@ -591,12 +591,13 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
     const float* sdf = sdf_all + p.goff;
     const float4 a = accum[gi];
     float4 out = make_float4(a.x, 0.f, 0.f, 0.f);
+    const bool inside = __ldg(sdf + idx) < 0.0f;
     if (a.x > 1e-9f) {
         const int x = idx % p.sx, y = (idx / p.sx) % p.sy, z = idx / (p.sx * p.sy);
         float vx = a.y / a.x;
         float vy = a.z / a.x - p.gravity * p.dt;
         float vz = a.w / a.x;
-        if (__ldg(sdf + idx) < 0.0f) {
+        if (inside) {
             const float3 nrm = sdf_node_normal(p, sdf, x, y, z);
             const float vdn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
             if (vdn < 0.0f) {
@@ -614,6 +615,8 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
         if ((uint32_t)z > (uint32_t)p.sz - 1u - pad && vz > 0.f) vz = 0.f;
         out = make_float4(a.x, vx, vy, vz);
     }
+    // Sign bit of the mass: the node's SDF is negative (G2P's obstacle test).
+    if (inside) out.x = -out.x;
     vgrid[gi] = out;
     if (a.x != 0.f || a.y != 0.f || a.z != 0.f || a.w != 0.f) accum[gi] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
@@ -623,11 +626,13 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
 // slot gidx[j] of the old state and writes slot j of the new one, so the
 // state ends up ordered by cell.  It also files the new position into the
 // counter set of the next substep.
-// G2P modes: the plain substep; the learned large step (features -> MLP ->
-// velocity correction before advection); the collection probe (the large
-// step without correction, recording each particle's features and final
-// velocity by original index).
-enum G2PMode : int { kG2PPlain = 0, kG2PLearned = 1, kG2PCollect = 2 };
+// G2P modes: the plain substep; the uncorrected large step; the learned
+// large step (features -> MLP -> velocity correction before advection); the
+// collection probe (the uncorrected large step, recording each particle's
+// features and final velocity by original index).  Large steps advect with
+// v_old + blend (v_new - v_old), blend = (R + 1) / (2R) for R plain substeps:
+// R substeps under a constant acceleration move a particle by exactly that.
+enum G2PMode : int { kG2PPlain = 0, kG2PLearned = 1, kG2PCollect = 2, kG2PLarge = 3 };
 
 template <bool kBatch, int kMode>
 __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, long long n_total, const float* __restrict__ Pin,
@@ -657,6 +662,8 @@ __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, l
     const int src = __ldg(gidx + j);
     const float4* q = reinterpret_cast<const float4*>(Pin + (size_t)src * kAFloats);
     const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+    float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (kMode != kG2PPlain) qv = __ldg(q + 3);  // old velocity
     const float pos[3] = {q0.x, q0.y, q0.z};
     const float F[9] = {q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
 
@@ -669,29 +676,42 @@ __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, l
         wz[a] = bspline_weight(pos[2] - (float)(bz + a));
     }
     float tv[3] = {0.f, 0.f, 0.f}, tc[9], tm = 0.f;
+    // Set when a stencil node lies outside the grid or inside an obstacle:
+    // only then can the SDF at the new position be negative (see below).
+    uint32_t sdf_risk = 0u;
 #pragma unroll
     for (int k = 0; k < 9; ++k) tc[k] = 0.f;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const int z = bz + c;
-        if ((unsigned)z >= (unsigned)p.sz) continue;
+        if ((unsigned)z >= (unsigned)p.sz) {
+            sdf_risk = 1u;
+            continue;
+        }
         const float dzv = -(pos[2] - (float)z);
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
             const int y = by + b;
-            if ((unsigned)y >= (unsigned)p.sy) continue;
+            if ((unsigned)y >= (unsigned)p.sy) {
+                sdf_risk = 1u;
+                continue;
+            }
             const float dyv = -(pos[1] - (float)y);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 const int x = bx + a;
-                if ((unsigned)x >= (unsigned)p.sx) continue;
+                if ((unsigned)x >= (unsigned)p.sx) {
+                    sdf_risk = 1u;
+                    continue;
+                }
                 const float dxv = -(pos[0] - (float)x);
                 const float4 g = __ldg(vgrid + node_index(p, x, y, z));
+                sdf_risk |= __float_as_uint(g.x) >> 31;
                 const float w = wx[a] * wy[b] * wz[c];
                 tv[0] += w * g.y;
                 tv[1] += w * g.z;
                 tv[2] += w * g.w;
-                if constexpr (kMode != kG2PPlain) tm += w * g.x;
+                if constexpr (kMode != kG2PPlain) tm += w * fabsf(g.x);
                 const float term = 4.0f * w;
                 tc[0] += term * g.y * dxv;
                 tc[1] += term * g.y * dyv;
@@ -705,7 +725,7 @@ __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, l
             }
         }
     }
-    if constexpr (kMode != kG2PPlain) {
+    if constexpr (kMode == kG2PLearned || kMode == kG2PCollect) {
         float f[kMlpIn];
 #pragma unroll
         for (int k = 0; k < 9; ++k) f[k] = tc[k];
@@ -732,7 +752,7 @@ __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, l
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) dev += __shfl_xor_sync(0xffffffffu, dev, o);
             if ((threadIdx.x & 31) == 0) atomicAdd(la.stat, dev);
-        } else if (valid) {
+        } else if (valid) {  // collection probe: la.feat holds n rows
             float* fo = la.feat + (size_t)__ldg(sig_in + src) * kMlpIn;
 #pragma unroll
             for (int k = 0; k < kMlpIn; k += 4) *reinterpret_cast<float4*>(fo + k) = make_float4(f[k], f[k + 1], f[k + 2], f[k + 3]);
@@ -755,8 +775,21 @@ __global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, l
         for (int k = 0; k < 9; ++k) NF[k] *= scale;
     }
     // Advect, then push out of obstacles (kernels.cu:249-270).
-    float nx = pos[0] + tv[0] * p.dt, ny = pos[1] + tv[1] * p.dt, nz = pos[2] + tv[2] * p.dt;
-    const float dist = sdf_trilinear(p, sdf, nx, ny, nz);
+    float av[3] = {tv[0], tv[1], tv[2]};
+    if constexpr (kMode != kG2PPlain) {
+        av[0] = qv.x + la.blend * (tv[0] - qv.x);
+        av[1] = qv.y + la.blend * (tv[1] - qv.y);
+        av[2] = qv.z + la.blend * (tv[2] - qv.z);
+    }
+    const float sx = av[0] * p.dt, sy = av[1] * p.dt, sz = av[2] * p.dt;
+    float nx = pos[0] + sx, ny = pos[1] + sy, nz = pos[2] + sz;
+    // The stencil nodes are base..base+2 and pos - base lies in [0.5, 1.5):
+    // a move of at most 0.25 per axis keeps every corner of the new
+    // position's cell among them, so with no stencil node outside the grid or
+    // with a negative SDF the trilinear SDF there is a convex combination of
+    // non-negative values and the obstacle test below cannot fire.
+    const bool far = !sdf_risk && fabsf(sx) <= 0.25f && fabsf(sy) <= 0.25f && fabsf(sz) <= 0.25f;
+    const float dist = far ? 0.0f : sdf_trilinear(p, sdf, nx, ny, nz);
     if (dist < 0.0f) {
         const float3 nrm = sdf_gradient_dir(p, sdf, nx, ny, nz);
         nx -= nrm.x * dist;
@@ -876,7 +909,7 @@ __global__ void __launch_bounds__(256) grid_export_kernel(SimParams p, const flo
     if (i >= p.g) return;
     const float4 v = __ldg(grid + i);
     const long long g = p.g;
-    planes[i] = v.x;
+    planes[i] = fabsf(v.x);  // the sign bit of a velocity node's mass marks a negative SDF
     planes[g + i] = v.y;
     planes[2 * g + i] = v.z;
     planes[3 * g + i] = v.w;
@@ -916,44 +949,61 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
     return 3;
 }
 
+int p2g_max_ctas_per_sm() {
+    int k = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, p2g_kernel, 32, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return kP2GWarpsPerSM;
+    }
+    return k;
+}
+
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
                const int32_t* cstart, const BinSet& cur, const long long* itemoff, uint32_t* work, float4* accum,
-               uint32_t* status, cudaStream_t st) {
+               uint32_t* status, cudaStream_t st, int ctas_per_sm) {
     if (n <= 0) return 0;
-    const int warps = (int)std::min(bins_total * kBinZ, 148LL * kP2GWarpsPerSM);
+    const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : kP2GWarpsPerSM;
+    const int warps = (int)std::min(bins_total * kBinZ, 148LL * per_sm);
     p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, itemoff, work, accum, status);
     return 1;
 }
 
 int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
-                       const float* sdf, cudaStream_t st) {
+                       const float* sdf, cudaStream_t st, int block) {
     if (g_total <= 0) return 0;
+    const int b = (block == 128 || block == 256) ? block : 256;
     if (sc.count == 1)
-        grid_update_kernel<false><<<blocks_for(g_total, 256), 256, 0, st>>>(sc, p0, g_total, accum, vgrid, sdf);
+        grid_update_kernel<false><<<blocks_for(g_total, b), b, 0, st>>>(sc, p0, g_total, accum, vgrid, sdf);
     else
-        grid_update_kernel<true><<<blocks_for(g_total, 256), 256, 0, st>>>(sc, p0, g_total, accum, vgrid, sdf);
+        grid_update_kernel<true><<<blocks_for(g_total, b), b, 0, st>>>(sc, p0, g_total, accum, vgrid, sdf);
     return 1;
 }
 
 int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const float* Pin, float* Pout,
                const int32_t* gidx, const int32_t* sig_in, int32_t* sig_out, const float4* vgrid, const float* sdf,
                int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st,
-               const LearnArgs* learn) {
+               const LearnArgs* learn, int block) {
     if (n <= 0) return 0;
     const LearnArgs la = learn ? *learn : LearnArgs{};
     const unsigned grid = blocks_for(n, 256);
+    // Plain G2P: 128- or 256-thread CTAs (the learned modes stage 8 warps of
+    // MLP inputs and always run 256).
+    const int pb = (block == 128 || block == 256) ? block : 256;
     if (learn && sc.count == 1 && la.mlp)
         g2p_kernel<false, kG2PLearned><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
                                                              pcell, prank, next, health, la);
-    else if (learn && sc.count == 1)
+    else if (learn && sc.count == 1 && la.feat)
         g2p_kernel<false, kG2PCollect><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
                                                              pcell, prank, next, health, la);
-    else if (sc.count == 1)
-        g2p_kernel<false, kG2PPlain><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+    else if (learn && sc.count == 1)
+        g2p_kernel<false, kG2PLarge><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
                                                            pcell, prank, next, health, la);
+    else if (sc.count == 1)
+        g2p_kernel<false, kG2PPlain><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out,
+                                                                       vgrid, sdf, pcell, prank, next, health, la);
     else
-        g2p_kernel<true, kG2PPlain><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
-                                                          pcell, prank, next, health, la);
+        g2p_kernel<true, kG2PPlain><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out,
+                                                                      vgrid, sdf, pcell, prank, next, health, la);
     return 1;
 }
 

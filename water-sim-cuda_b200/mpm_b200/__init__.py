@@ -62,6 +62,11 @@ class _LearnedStats(ctypes.Structure):
                 ("last_density_change", ctypes.c_double)]
 
 
+class _Tuning(ctypes.Structure):
+    _fields_ = [("p2g_ctas_per_sm", ctypes.c_int32), ("g2p_block", ctypes.c_int32), ("grid_block", ctypes.c_int32),
+                ("p2g_ms", ctypes.c_float), ("g2p_ms", ctypes.c_float), ("grid_ms", ctypes.c_float)]
+
+
 class _Stats(ctypes.Structure):
     _fields_ = [("substeps", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
                 ("sort_passes", ctypes.c_int64), ("health", ctypes.c_uint32),
@@ -164,6 +169,42 @@ def _load() -> ctypes.CDLL:
         "mpm_scene_get_grid": (I32, [P, I32, P]),
         "mpm_scene_get_sdf": (I32, [P, I32, P]),
         "mpm_scene_get_sort": (I32, [P, I32, P, P]),
+        "mpm_scene_build": (I32, [ctypes.c_char_p, ctypes.c_char_p, I32, P]),
+        "mpm_scene_data_free": (None, [P]),
+        "mpm_scene_data_num_particles": (I64, [P]),
+        "mpm_scene_data_num_triangles": (I64, [P]),
+        "mpm_scene_data_state": (I32, [P, P]),
+        "mpm_scene_data_triangles": (I32, [P, P]),
+        "mpm_scene_data_log": (ctypes.c_char_p, [P]),
+        "mpm_scene_last_error": (ctypes.c_char_p, []),
+        "mpm_mesh_load_obj": (I32, [ctypes.c_char_p, P]),
+        "mpm_mesh_from_obj_text": (I32, [ctypes.c_char_p, P]),
+        "mpm_mesh_free": (None, [P]),
+        "mpm_mesh_num_vertices": (I64, [P]),
+        "mpm_mesh_num_triangles": (I64, [P]),
+        "mpm_mesh_get": (I32, [P, P, P, P]),
+        "mpm_voxelize": (I32, [P, ctypes.c_float, I32, P]),
+        "mpm_points_create": (I32, [P, I64, P]),
+        "mpm_points_count": (I64, [P]),
+        "mpm_points_get": (I32, [P, P]),
+        "mpm_points_free": (None, [P]),
+        "mpm_points_normalize": (I32, [P, ctypes.c_float, ctypes.c_float, P, I32, I32]),
+        "mpm_triangles_normalize": (I32, [P, P, ctypes.c_float, ctypes.c_float, P]),
+        "mpm_checkpoint_save": (I32, [P, ctypes.c_char_p, ctypes.c_char_p]),
+        "mpm_checkpoint_load": (I32, [ctypes.c_char_p, I32, P]),
+        "mpm_checkpoint_info": (I32, [ctypes.c_char_p, P, P, P, ctypes.c_char_p, I32]),
+        "mpm_render_params_default": (None, [P, I32, I32, I32]),
+        "mpm_renderer_create": (I32, [P, I32, P]),
+        "mpm_renderer_destroy": (None, [P]),
+        "mpm_renderer_last_error": (ctypes.c_char_p, [P]),
+        "mpm_renderer_set_background": (I32, [P, P]),
+        "mpm_render_points": (I32, [P, P, I64, P]),
+        "mpm_render_frame": (I32, [P, P]),
+        "mpm_renderer_get_depth": (I32, [P, I32, P]),
+        "mpm_renderer_get_image": (I32, [P, P, P]),
+        "mpm_autotune": (I32, [P, I32, P]),
+        "mpm_set_tuning": (I32, [P, P]),
+        "mpm_get_tuning": (I32, [P, P]),
         "mpm_set_corrector": (I32, [P, P, I32, ctypes.c_float]),
         "mpm_step_learned": (I32, [P, I32, P]),
         "mpm_corrector_create": (I32, [I32, I64, P]),
@@ -337,6 +378,38 @@ class Engine:
 
     def stream(self) -> int:
         return int(lib.mpm_stream(self._h) or 0)
+
+    # -- launch shapes --------------------------------------------------------
+    def autotune(self, repeats: int = 3) -> dict:
+        """Time the candidate launch shapes on the current particles; keep the fastest."""
+        t = _Tuning()
+        self._check(lib.mpm_autotune(self._h, int(repeats), ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in _Tuning._fields_}
+
+    def tuning(self) -> dict:
+        t = _Tuning()
+        self._check(lib.mpm_get_tuning(self._h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in _Tuning._fields_}
+
+    def set_tuning(self, p2g_ctas_per_sm: int = 12, g2p_block: int = 256, grid_block: int = 256):
+        t = _Tuning(int(p2g_ctas_per_sm), int(g2p_block), int(grid_block), 0.0, 0.0, 0.0)
+        self._check(lib.mpm_set_tuning(self._h, ctypes.byref(t)))
+
+    # -- checkpoints ----------------------------------------------------------
+    def save_checkpoint(self, path: str, note: str = ""):
+        """State (original order), SDF, config and substep count to one file."""
+        self._check(lib.mpm_checkpoint_save(self._h, path.encode(), note.encode()))
+
+    @classmethod
+    def load_checkpoint(cls, path: str, device: int = 0) -> "Engine":
+        info = checkpoint_info(path)
+        h = ctypes.c_void_p()
+        st = lib.mpm_checkpoint_load(path.encode(), int(device), ctypes.byref(h))
+        if st != 0:
+            raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
+        e = cls.__new__(cls)
+        e.cfg, e._h, e.n = info["config"], h, info["n"]
+        return e
 
     # -- learned large step ---------------------------------------------------
     def set_corrector(self, params: np.ndarray | None, ratio: int = 4, max_density_change: float = 0.02):
@@ -536,3 +609,182 @@ class Corrector:
         out = np.empty((len(f), CORRECTOR_OUTPUTS), np.float32)
         self._check(lib.mpm_corrector_forward(self._h, len(f), _ptr(f), _ptr(out)))
         return out
+
+
+# -- scene construction (Simulation::Simulation's WATER= / OBJECT= path) ----------
+def _scene_check(st: int):
+    if st != 0:
+        raise MpmError(st, lib.mpm_scene_last_error().decode(errors="replace"))
+
+
+class Mesh:
+    """An OBJ model: vertices and triangles (ObjLoader::loadObj + extractTriangles)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def load(cls, path: str) -> "Mesh":
+        h = ctypes.c_void_p()
+        _scene_check(lib.mpm_mesh_load_obj(path.encode(), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_text(cls, text: str) -> "Mesh":
+        h = ctypes.c_void_p()
+        _scene_check(lib.mpm_mesh_from_obj_text(text.encode(), ctypes.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.mpm_mesh_free(self._h)
+            self._h = None
+
+    def arrays(self):
+        """(vertices (nv, 3), faces (nt, 3) int32, triangles (nt, 9))."""
+        nv, nt = lib.mpm_mesh_num_vertices(self._h), lib.mpm_mesh_num_triangles(self._h)
+        v = np.empty((nv, 3), np.float32)
+        f = np.empty((nt, 3), np.int32)
+        t = np.empty((nt, 9), np.float32)
+        _scene_check(lib.mpm_mesh_get(self._h, _ptr(v), _ptr(f), _ptr(t)))
+        return v, f, t
+
+    def voxelize(self, resolution: float = 100.0, device: int = 0) -> np.ndarray:
+        """VoxelEngine::voxelize: (n, 3) voxel centres, z-major order."""
+        h = ctypes.c_void_p()
+        _scene_check(lib.mpm_voxelize(self._h, float(resolution), int(device), ctypes.byref(h)))
+        try:
+            return _points_array(h)
+        finally:
+            lib.mpm_points_free(h)
+
+
+def _points_array(h) -> np.ndarray:
+    n = lib.mpm_points_count(h)
+    out = np.empty((n, 3), np.float32)
+    _scene_check(lib.mpm_points_get(h, _ptr(out) if n else None))
+    return out
+
+
+def normalize_points(points: np.ndarray, normalize_size: float, scale: float, displacement, lattice_step: int,
+                     device: int = 0) -> np.ndarray:
+    """VoxelEngine::normalize(VoxelData&): centre, scale, displace, snap + 5^3 dilation."""
+    p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    d = np.ascontiguousarray(displacement, np.float32).reshape(3)
+    h = ctypes.c_void_p()
+    _scene_check(lib.mpm_points_create(_ptr(p) if len(p) else None, len(p), ctypes.byref(h)))
+    try:
+        _scene_check(lib.mpm_points_normalize(h, float(normalize_size), float(scale), _ptr(d), int(lattice_step),
+                                              int(device)))
+        return _points_array(h)
+    finally:
+        lib.mpm_points_free(h)
+
+
+def normalize_triangles(tris: np.ndarray, normalize_size: float, scale: float, displacement) -> np.ndarray:
+    """VoxelEngine::normalize(std::vector<Triangle>&): (t, 9) -> the kept, transformed triangles."""
+    t = np.ascontiguousarray(tris, np.float32).reshape(-1, 9).copy()
+    d = np.ascontiguousarray(displacement, np.float32).reshape(3)
+    n = ctypes.c_int64(len(t))
+    _scene_check(lib.mpm_triangles_normalize(_ptr(t) if len(t) else None, ctypes.byref(n), float(normalize_size),
+                                             float(scale), _ptr(d)))
+    return t[:n.value]
+
+
+def build_scene(config_text: str, base_dir: str = "", device: int = 0):
+    """Simulation::Simulation's scene part: (Config, state (26, n), triangles (t, 9), log)."""
+    cfg = parse_config_string(config_text)
+    h = ctypes.c_void_p()
+    _scene_check(lib.mpm_scene_build(config_text.encode(), base_dir.encode(), int(device), ctypes.byref(h)))
+    try:
+        n = lib.mpm_scene_data_num_particles(h)
+        t = lib.mpm_scene_data_num_triangles(h)
+        st = np.empty((PARTICLE_PLANES, n), np.float32)
+        tris = np.empty((t, 9), np.float32)
+        _scene_check(lib.mpm_scene_data_state(h, _ptr(st) if n else None))
+        _scene_check(lib.mpm_scene_data_triangles(h, _ptr(tris) if t else None))
+        log = lib.mpm_scene_data_log(h).decode(errors="replace")
+    finally:
+        lib.mpm_scene_data_free(h)
+    return cfg, st, tris, log
+
+
+def checkpoint_info(path: str) -> dict:
+    c = _Config()
+    n, sub = ctypes.c_int64(0), ctypes.c_int64(0)
+    note = ctypes.create_string_buffer(1 << 16)
+    st = lib.mpm_checkpoint_info(path.encode(), ctypes.byref(c), ctypes.byref(n), ctypes.byref(sub), note, len(note))
+    if st != 0:
+        raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
+    cfg = Config(c.size_x, c.size_y, c.size_z, c.padding, c.gravity, c.dt, c.gamma, c.compression,
+                 c.resolution, c.substeps, c.sdf_resolution)
+    return {"config": cfg, "n": n.value, "substeps": sub.value, "note": note.value.decode(errors="replace")}
+
+
+# -- headless screen-space fluid rendering ----------------------------------------
+class _RenderParams(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("grid", ctypes.c_int32 * 3),
+                ("fov_y_degrees", ctypes.c_float), ("near_clip", ctypes.c_float), ("far_clip", ctypes.c_float),
+                ("zoom_distance", ctypes.c_float), ("rotation", ctypes.c_float),
+                ("rotation_vertical", ctypes.c_float), ("radius", ctypes.c_float), ("filter_size", ctypes.c_float),
+                ("depth_falloff", ctypes.c_float), ("light_dir", ctypes.c_float * 3),
+                ("clear_color", ctypes.c_float * 3)]
+
+
+class Renderer:
+    """The reference's SSF passes (depth splat, bilateral blur, composite) on the GPU."""
+
+    def __init__(self, grid, width: int = 1920, height: int = 1600, device: int = 0, **overrides):
+        p = _RenderParams()
+        lib.mpm_render_params_default(ctypes.byref(p), int(grid[0]), int(grid[1]), int(grid[2]))
+        p.width, p.height = int(width), int(height)
+        for k, v in overrides.items():
+            if k in ("light_dir", "clear_color"):
+                getattr(p, k)[:] = [float(x) for x in v]
+            else:
+                setattr(p, k, v)
+        h = ctypes.c_void_p()
+        st = lib.mpm_renderer_create(ctypes.byref(p), int(device), ctypes.byref(h))
+        if st != 0:
+            raise MpmError(st, lib.mpm_global_last_error().decode(errors="replace"))
+        self._h, self.width, self.height = h, p.width, p.height
+
+    def _check(self, st):
+        if st != 0:
+            raise MpmError(st, lib.mpm_renderer_last_error(self._h).decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.mpm_renderer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_background(self, rgb8: np.ndarray):
+        a = np.ascontiguousarray(rgb8, np.uint8).reshape(self.height, self.width, 3)
+        self._check(lib.mpm_renderer_set_background(self._h, _ptr(a)))
+
+    def render_device(self, xyz_ptr: int, n: int, stream: int = 0):
+        self._check(lib.mpm_render_points(self._h, ctypes.c_void_p(xyz_ptr), int(n), ctypes.c_void_p(stream)))
+
+    def render_engine(self, engine: Engine):
+        self._check(lib.mpm_render_frame(self._h, engine._h))
+
+    def depth(self, which: int = 2) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        self._check(lib.mpm_renderer_get_depth(self._h, int(which), _ptr(out)))
+        return out
+
+    def image(self):
+        """(float RGB (h, w, 3), 8-bit RGB), row 0 at the bottom."""
+        f = np.empty((self.height, self.width, 3), np.float32)
+        b = np.empty((self.height, self.width, 3), np.uint8)
+        self._check(lib.mpm_renderer_get_image(self._h, _ptr(f), _ptr(b)))
+        return f, b

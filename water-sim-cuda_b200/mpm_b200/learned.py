@@ -144,16 +144,20 @@ def _timed(fn):
 
 
 def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_density_change: float = 0.02,
-             checkpoints=(100,)) -> dict:
+             checkpoints=(10, 25, 50, 100), perturb: float = 1e-4) -> dict:
     """Plain (ratio * nlarge substeps) vs learned (nlarge large steps) vs the
     uncorrected large step, from the same state; metrics at each checkpoint
-    (in large steps) and at the end."""
+    (in large steps) and at the end.  "perturbed" is the plain run from
+    positions moved by N(0, perturb) cells: its distance from the plain run
+    is the chaos floor of the scene, what no large step can undercut."""
     marks = sorted(set([c for c in checkpoints if c <= nlarge] + [nlarge]))
     res = {"ratio": ratio, "large_steps": nlarge, "max_density_change": max_density_change}
     runs = {}
-    for tag in ("plain", "learned", "uncorrected"):
+    st_p = st.copy()
+    st_p[0:3] += np.random.default_rng(99).normal(0, perturb, st_p[0:3].shape).astype(np.float32)
+    for tag in ("plain", "perturbed", "learned", "uncorrected"):
         with Engine(cfg) as e:
-            e.init(st)
+            e.init(st_p if tag == "perturbed" else st)
             e.init_sdf(tris)
             if tag == "learned":
                 e.set_corrector(params, ratio=ratio, max_density_change=max_density_change)
@@ -162,7 +166,7 @@ def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_densi
             pos, total, prev, stats = {}, 0.0, 0, {}
             for m in marks:
                 k = m - prev
-                if tag == "plain":
+                if tag in ("plain", "perturbed"):
                     _, dt = _timed(lambda: e.step(k * ratio))
                 else:
                     stats, dt = _timed(lambda: e.step_learned(k))
@@ -175,7 +179,7 @@ def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_densi
                         "particle_substeps_per_s": e.get_number() * nlarge * ratio / total}
             if tag == "learned":
                 res[tag].update(stats)
-    for tag in ("learned", "uncorrected"):
+    for tag in ("perturbed", "learned", "uncorrected"):
         for m in marks:
             res[tag][f"at_{m}"] = compare(cfg, runs[tag][m], runs["plain"][m])
     res["speedup_sim_time"] = res["learned"]["sim_time_per_s"] / res["plain"]["sim_time_per_s"]
@@ -183,7 +187,10 @@ def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_densi
 
 
 def save_params(path: str, params: np.ndarray, meta: dict):
+    """path (.npz: parameters and training record) and the raw little-endian
+    float32 parameters beside it (.bin, what `mpm_run --corrector` reads)."""
     np.savez_compressed(path, params=params.astype(np.float32), meta=json.dumps(meta))
+    params.astype("<f4").tofile(os.path.splitext(path)[0] + ".bin")
 
 
 def load_params(path: str = DEFAULT_PARAMS):
