@@ -361,21 +361,28 @@ def run_engine(args, rank, world, local):
         lib = mpm_b200.lib
         init2()  # warm the allocation path once
         if tuning:
-            eng2.set_tuning(tuning["p2g_ctas_per_sm"], tuning["g2p_block"], tuning["grid_block"])
+            eng2.set_tuning(tuning["p2g_ctas_per_sm"], tuning["g2p_block"], tuning["grid_block"],
+                            tuning["p2g_cell_cap"])
         eng2.step(sub)
         dist.barrier()
-        t0 = time.perf_counter()
+        marks = [time.perf_counter()]
         init2()
+        marks.append(time.perf_counter())
         for _ in range(args.steps):
             eng2.step(sub)
             read_positions()
-        t1 = time.perf_counter()
+            marks.append(time.perf_counter())
+        t0, t1 = marks[0], marks[-1]
         dist.barrier()
         e2e_s = dist.max(t1 - t0)
+        frames = [1e3 * (b - a) for a, b in zip(marks[1:-1], marks[2:])]
         e2e = {"value": world * n * sub * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(26 * 4 * n / args.steps), "d2h_bytes_per_step": 12 * n,
                "timed": "mpm_init_particles(pinned host state) + K x (mpm_step(SUBSTEPS) + "
-                        "mpm_get_positions(pinned)); host wall clock, max over ranks"}
+                        "mpm_get_positions(pinned)); host wall clock, max over ranks",
+               "init_ms": round(1e3 * (marks[1] - marks[0]), 3),
+               "frame_ms": {"min": round(min(frames), 3), "median": round(sorted(frames)[len(frames) // 2], 3),
+                            "max": round(max(frames), 3)}}
         eng2.close()
 
     cpu = None

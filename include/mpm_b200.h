@@ -495,8 +495,9 @@ mpm_status mpm_triangles_normalize(float* triangles9_host, int64_t* t, float nor
 /* ------------------------------------------------------------------ */
 /* Launch-shape tuning                                                   */
 /* ------------------------------------------------------------------ */
-/* The substep's launch shapes: persistent P2G CTAs per SM, and the CTA
- * sizes of the plain G2P and of the grid update.  mpm_autotune times each
+/* The substep's launch shapes: persistent P2G CTAs per SM and P2G's
+ * crowded-cell threshold, and the CTA sizes of the plain G2P and of the grid
+ * update.  mpm_autotune times each
  * candidate on the engine's current particles (each stage on its own, the
  * median of `repeats` runs; every timed substep is undone, so the state does
  * not advance) and keeps the fastest; results are identical for every shape
@@ -506,6 +507,8 @@ typedef struct mpm_tuning {
     int32_t g2p_block;        /* 128 or 256 (default 256) */
     int32_t grid_block;       /* 128 or 256 (default 256) */
     float p2g_ms, g2p_ms, grid_ms;  /* stage times of the chosen shapes (mpm_autotune) */
+    int32_t p2g_cell_cap;     /* 4 .. 64: particles of a cell one lane sums before the
+                               * cell is shared by the warp (default 12) */
 } mpm_tuning;
 mpm_status mpm_autotune(mpm_engine* engine, int32_t repeats, mpm_tuning* out);
 mpm_status mpm_set_tuning(mpm_engine* engine, const mpm_tuning* tuning);

@@ -106,6 +106,7 @@ def test_autotune_keeps_state_and_results(gpu_ok, mpm):
         before = [b.scene_buffer(k) for k in range(len(sc))]
         t = b.autotune(repeats=2)
         assert t["p2g_ctas_per_sm"] >= 1 and t["g2p_block"] in (128, 256) and t["grid_block"] in (128, 256)
+        assert t["p2g_cell_cap"] in (8, 12, 16, 24, 32)
         assert t["p2g_ms"] > 0 and t["g2p_ms"] > 0 and t["grid_ms"] > 0
         assert b.tuning()["p2g_ctas_per_sm"] == t["p2g_ctas_per_sm"]
         after = [b.scene_buffer(k) for k in range(len(sc))]
@@ -116,7 +117,7 @@ def test_autotune_keeps_state_and_results(gpu_ok, mpm):
         tuned = [b.scene_buffer(k) for k in range(len(sc))]
     with _batch(mpm, sc) as b:
         b.step(2)
-        b.set_tuning(4, 128, 128)
+        b.set_tuning(4, 128, 128, 32)
         b.step(3)
         other = [b.scene_buffer(k) for k in range(len(sc))]
         with pytest.raises(mpm.MpmError):

@@ -144,7 +144,7 @@ struct mpm_engine {
     double last_density_change = 0.0;
 
     // Launch shapes of the substep (mpm_autotune / mpm_set_tuning).
-    mpm_tuning tune{12, 256, 256, 0.f, 0.f, 0.f};
+    mpm_tuning tune{12, 256, 256, 0.f, 0.f, 0.f, 12};
 };
 
 namespace {
@@ -281,7 +281,8 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
     mark(1);
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
         launches += mpm::launch_p2g(sc, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par], e->d_itemoff,
-                                    work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm);
+                                    work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
+                                    e->tune.p2g_cell_cap);
     mark(2);
     if (from <= MPM_STAGE_GRID && upto >= MPM_STAGE_GRID)
         launches += mpm::launch_grid_update(sc, e->prm[0], e->g_total, e->accum, e->vgrid, e->sdf, st,
@@ -652,7 +653,8 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
     launches += mpm::launch_bin_order(e->table, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart,
                                       e->cstart, e->pcell, e->prank, e->gidx, e->d_itemoff, work, st);
     launches += mpm::launch_p2g(e->table_large, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par],
-                                e->d_itemoff, work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm);
+                                e->d_itemoff, work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
+                                e->tune.p2g_cell_cap);
     launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, st,
                                         e->tune.grid_block);
     launches += mpm::launch_g2p(e->table_large, big, e->n, e->P[par], e->P[1 - par], e->gidx, e->sigma[par],
@@ -1391,7 +1393,8 @@ extern "C" mpm_status mpm_checkpoint_load(const char* path, int32_t device, mpm_
 namespace {
 bool valid_tuning(const mpm_tuning& t) {
     return t.p2g_ctas_per_sm >= 1 && t.p2g_ctas_per_sm <= mpm::p2g_max_ctas_per_sm() &&
-           (t.g2p_block == 128 || t.g2p_block == 256) && (t.grid_block == 128 || t.grid_block == 256);
+           (t.g2p_block == 128 || t.g2p_block == 256) && (t.grid_block == 128 || t.grid_block == 256) &&
+           t.p2g_cell_cap >= 4 && t.p2g_cell_cap <= 64;
 }
 
 // Times stage `stage` of one substep from the current state and undoes the
@@ -1420,6 +1423,7 @@ extern "C" mpm_status mpm_set_tuning(mpm_engine* e, const mpm_tuning* t) {
     e->tune.p2g_ctas_per_sm = t->p2g_ctas_per_sm;
     e->tune.g2p_block = t->g2p_block;
     e->tune.grid_block = t->grid_block;
+    e->tune.p2g_cell_cap = t->p2g_cell_cap;
     return e->initialized ? capture_graphs(e) : MPM_OK;
 }
 
@@ -1468,6 +1472,14 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
         if (ms < tbest) tbest = ms, best.p2g_ctas_per_sm = k, best.p2g_ms = ms;
     }
     e->tune.p2g_ctas_per_sm = best.p2g_ctas_per_sm;
+    tbest = best.p2g_ms;
+    for (int k : {8, 16, 24, 32}) {
+        if (s != MPM_OK) break;
+        e->tune.p2g_cell_cap = k;
+        if ((s = median_time(MPM_STAGE_P2G, &ms)) != MPM_OK) break;
+        if (ms < tbest) tbest = ms, best.p2g_cell_cap = k, best.p2g_ms = ms;
+    }
+    e->tune.p2g_cell_cap = best.p2g_cell_cap;
     tbest = 1e30f;
     for (int k : {128, 256}) {
         if (s != MPM_OK) break;

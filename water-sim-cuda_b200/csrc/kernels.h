@@ -74,10 +74,12 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
                      int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
                      long long* itemoff, uint32_t* work, cudaStream_t st);
 // P2G over the items of `cur`; gidx maps slots of the new order to P.
-// ctas_per_sm: persistent single-warp CTAs per SM (0 = the default 12).
+// ctas_per_sm: persistent single-warp CTAs per SM (0 = the default 12);
+// cell_cap: particles of a cell its own lane sums before the cell is shared
+// by the whole warp (0 = the default 12).
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
                const int32_t* cstart, const BinSet& cur, const long long* itemoff, uint32_t* work, float4* accum,
-               uint32_t* status, cudaStream_t st, int ctas_per_sm = 0);
+               uint32_t* status, cudaStream_t st, int ctas_per_sm = 0, int cell_cap = 0);
 // Most P2G CTAs that fit on one SM.
 int p2g_max_ctas_per_sm();
 // p0: the parameters of scene 0, used directly when the table holds one scene.

@@ -119,7 +119,8 @@ struct SceneLookup {
 // lane then adds its 27 sums to the warp's footprint, the layer's 10 x 6 x 3
 // nodes in shared memory: the 32 cells of a layer are distinct, so for one
 // stencil offset the 32 nodes differ and a plain read-add-write per offset is
-// race-free.  A lane sums at most kCellCap particles of its cell; the rest of
+// race-free.  A lane sums at most `cap` particles of its cell (a launch
+// parameter, kCellCap by default); the rest of
 // a crowded cell (this Tait law resists only expansion, so compressed fluid
 // piles up) is shared by all 32 lanes and reduced across the warp.  The
 // footprint goes to global memory with one vector reduction per touched
@@ -181,7 +182,11 @@ __device__ __forceinline__ P2GParticle p2g_particle(const SimParams& p, float4 q
     // matrix C' = C + (4 DT V p / m) I (kernels.cu:20-35).
     float J = det3(F);
     J = fmaxf(0.9f, fminf(J, 1.1f));
-    float pressure = p.compression * (powf(J, p.gamma) - 1.0f);
+    // J^gamma - 1 > 0 only for J > 1 (gamma > 0) or J < 1 (gamma < 0); the
+    // clamp below zeroes every other case, so powf runs only where it counts.
+    float pressure = 0.0f;
+    if ((p.gamma > 0.0f && J > 1.0f) || (p.gamma < 0.0f && J < 1.0f))
+        pressure = p.compression * (powf(J, p.gamma) - 1.0f);
     if (pressure < 0.0f) pressure = 0.0f;
     const float multi = 4.0f * p.dt * (p.pvol * J) * pressure / p.pmass;
     C[0] += multi;
@@ -238,7 +243,7 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
                                                                   const long long* __restrict__ itemoff,
                                                                   uint32_t* __restrict__ work,
                                                                   float4* __restrict__ accum_all,
-                                                                  uint32_t* __restrict__ status) {
+                                                                  uint32_t* __restrict__ status, int cap) {
     __shared__ __align__(16) float4 s_ring[kRing][6][32];
     __shared__ float4 s_foot[kFootNodes];
     __shared__ int32_t s_gidx[kGidxStage];
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= nitems) return;
         // Items: kBinZ layers per listed bin, scene after scene.
-        const int scene = scene_of(itemoff, sc.count, item);
+        const int scene = sc.count == 1 ? 0 : scene_of(itemoff, sc.count, item);
         const SimParams p = sc.prm[scene];
         const int local = item - (int)__ldg(itemoff + scene);
         const int bin = __ldg(set.blist + p.boff + local / kBinZ), layer = local % kBinZ;
@@ -270,12 +275,12 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
         if (staged)
             for (int q = lane; q < l1 - l0; q += 32) s_gidx[q] = __ldg(gidx + l0 + q);
         __syncwarp();
-        // Pass 0: each lane its own cell's first kCellCap particles (slots
+        // Pass 0: each lane its own cell's first `cap` particles (slots
         // cs + s).  Pass k > 0: the k-th crowded cell's further particles,
-        // slot hcs + kCellCap + lane + 32 s, for every lane.  One loop body
+        // slot hcs + cap + lane + 32 s, for every lane.  One loop body
         // serves both; only the flush differs.
-        uint32_t crowded = __ballot_sync(0xffffffffu, full > kCellCap);
-        int first = cs, step = 1, cnt = min(full, kCellCap), target = lane;
+        uint32_t crowded = __ballot_sync(0xffffffffu, full > cap);
+        int first = cs, step = 1, cnt = min(full, cap), target = lane;
         for (;;) {
             float am[27], ax[27], ay[27], az[27];
             int maxc = cnt;
@@ -385,9 +390,9 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
             const int src = __ffs(crowded) - 1;
             crowded &= crowded - 1;
             const int hcnt = __shfl_sync(0xffffffffu, full, src);
-            first = __shfl_sync(0xffffffffu, cs, src) + kCellCap + lane;
+            first = __shfl_sync(0xffffffffu, cs, src) + cap + lane;
             step = 32;
-            cnt = max(0, (hcnt - kCellCap - lane + 31) / 32);
+            cnt = max(0, (hcnt - cap - lane + 31) / 32);
             target = src;
         }
         __syncwarp();
@@ -960,11 +965,12 @@ int p2g_max_ctas_per_sm() {
 
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
                const int32_t* cstart, const BinSet& cur, const long long* itemoff, uint32_t* work, float4* accum,
-               uint32_t* status, cudaStream_t st, int ctas_per_sm) {
+               uint32_t* status, cudaStream_t st, int ctas_per_sm, int cell_cap) {
     if (n <= 0) return 0;
     const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : kP2GWarpsPerSM;
+    const int cap = cell_cap > 0 ? cell_cap : kCellCap;
     const int warps = (int)std::min(bins_total * kBinZ, 148LL * per_sm);
-    p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, itemoff, work, accum, status);
+    p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, itemoff, work, accum, status, cap);
     return 1;
 }
 

@@ -219,6 +219,7 @@ def main(argv=None):
     ev.add_argument("--threshold", type=float, default=0.02)
     ev.add_argument("--physical", action="store_true")
     ev.add_argument("--seed", type=int, default=1235)
+    ev.add_argument("--alpha", type=float, default=1.0, help="scale of the applied correction")
     a = ap.parse_args(argv)
     if a.cmd == "train":
         seeds = list(range(a.first_seed, a.first_seed + a.variants))
@@ -238,11 +239,14 @@ def main(argv=None):
         print(json.dumps({k: v for k, v in meta.items() if k != "losses"} | {"final_loss": losses[-1]}))
     else:
         params, meta = load_params(a.params)
+        params = params.copy()
+        params[32:35] *= a.alpha  # output scale (MPM_CORRECTOR_PARAMS layout)
         cfg, st, tris = scenes.dam_break(seed=a.seed)
         if a.physical:
             cfg = physical_config(cfg)
         res = evaluate(cfg, st, tris, params, nlarge=a.large_steps, ratio=int(meta.get("ratio", 4)),
                        max_density_change=a.threshold)
+        res["alpha"] = a.alpha
         print(json.dumps(res))
 
 
