@@ -504,7 +504,8 @@ mpm_status mpm_triangles_normalize(float* triangles9_host, int64_t* t, float nor
  * up to the order of float sums. */
 typedef struct mpm_tuning {
     int32_t p2g_ctas_per_sm;  /* 1 .. the most that fit (default 12) */
-    int32_t g2p_block;        /* 128 or 256 (default 256) */
+    int32_t g2p_block;        /* 128 or 256 (default 256); 512 = 256-thread CTAs free to use up to
+                               * 255 registers (more loads in flight, fewer warps) */
     int32_t grid_block;       /* 128 or 256 (default 256) */
     float p2g_ms, g2p_ms, grid_ms;  /* stage times of the chosen shapes (mpm_autotune) */
     int32_t p2g_cell_cap;     /* 4 .. 64: particles of a cell one lane sums before the
@@ -526,7 +527,7 @@ mpm_status mpm_get_tuning(mpm_engine* engine, mpm_tuning* tuning);
  * (3), interpolated grid mass over the seeding density, minus 1 (1), and the
  * obstacle SDF folded into one vector n * phi * max(0, 1 - |phi| / 4) (3), all
  * gathered from the large step's grid at the particle's start position.
- * The plain substep is the fallback and the judge: a large step whose mean
+ * The plain substep is the fallback and the yardstick: a large step whose mean
  * predicted relative density change, mean over particles of
  * |1 / det(I + RATIO DT C) - 1|, exceeds max_density_change is undone and
  * replaced by RATIO plain substeps.  Engines of one scene only. */

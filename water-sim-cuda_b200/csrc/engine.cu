@@ -1393,7 +1393,8 @@ extern "C" mpm_status mpm_checkpoint_load(const char* path, int32_t device, mpm_
 namespace {
 bool valid_tuning(const mpm_tuning& t) {
     return t.p2g_ctas_per_sm >= 1 && t.p2g_ctas_per_sm <= mpm::p2g_max_ctas_per_sm() &&
-           (t.g2p_block == 128 || t.g2p_block == 256) && (t.grid_block == 128 || t.grid_block == 256) &&
+           (t.g2p_block == 128 || t.g2p_block == 256 || t.g2p_block == 512) &&
+           (t.grid_block == 128 || t.grid_block == 256) &&
            t.p2g_cell_cap >= 4 && t.p2g_cell_cap <= 64;
 }
 
@@ -1489,7 +1490,7 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
     }
     e->tune.grid_block = best.grid_block;
     tbest = 1e30f;
-    for (int k : {128, 256}) {
+    for (int k : {128, 256, 512}) {
         if (s != MPM_OK) break;
         e->tune.g2p_block = k;
         if ((s = median_time(MPM_STAGE_G2P, &ms)) != MPM_OK) break;

@@ -639,8 +639,11 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
 // R substeps under a constant acceleration move a particle by exactly that.
 enum G2PMode : int { kG2PPlain = 0, kG2PLearned = 1, kG2PCollect = 2, kG2PLarge = 3 };
 
-template <bool kBatch, int kMode>
-__global__ void __launch_bounds__(256) g2p_kernel(SceneTable sc, SimParams p0, long long n_total, const float* __restrict__ Pin,
+// kWide: 256-thread CTAs free to use up to 255 registers (one CTA per SM,
+// every node load of a particle in flight at once) instead of 64 registers
+// and four CTAs per SM; chosen by the autotuner.
+template <bool kBatch, int kMode, bool kWide = false>
+__global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch || kMode == 2) ? 3 : 4))) g2p_kernel(SceneTable sc, SimParams p0, long long n_total, const float* __restrict__ Pin,
                                                   float* __restrict__ Pout, const int32_t* __restrict__ gidx,
                                                   const int32_t* __restrict__ sig_in, int32_t* __restrict__ sig_out,
                                                   const float4* __restrict__ vgrid_all, const float* __restrict__ sdf_all,
@@ -992,9 +995,10 @@ int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const flo
     if (n <= 0) return 0;
     const LearnArgs la = learn ? *learn : LearnArgs{};
     const unsigned grid = blocks_for(n, 256);
-    // Plain G2P: 128- or 256-thread CTAs (the learned modes stage 8 warps of
-    // MLP inputs and always run 256).
-    const int pb = (block == 128 || block == 256) ? block : 256;
+    // Plain G2P: 128- or 256-thread CTAs, or 512 = the register-wide 256-thread
+    // variant (the learned modes stage 8 warps of MLP inputs and always run 256).
+    const bool wide = block == 512;
+    const int pb = wide ? 256 : ((block == 128 || block == 256) ? block : 256);
     if (learn && sc.count == 1 && la.mlp)
         g2p_kernel<false, kG2PLearned><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
                                                              pcell, prank, next, health, la);
@@ -1004,9 +1008,17 @@ int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const flo
     else if (learn && sc.count == 1)
         g2p_kernel<false, kG2PLarge><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
                                                            pcell, prank, next, health, la);
+    else if (sc.count == 1 && wide)
+        g2p_kernel<false, kG2PPlain, true><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in,
+                                                                             sig_out, vgrid, sdf, pcell, prank, next,
+                                                                             health, la);
     else if (sc.count == 1)
         g2p_kernel<false, kG2PPlain><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out,
                                                                        vgrid, sdf, pcell, prank, next, health, la);
+    else if (wide)
+        g2p_kernel<true, kG2PPlain, true><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in,
+                                                                            sig_out, vgrid, sdf, pcell, prank, next,
+                                                                            health, la);
     else
         g2p_kernel<true, kG2PPlain><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out,
                                                                       vgrid, sdf, pcell, prank, next, health, la);
