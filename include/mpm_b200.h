@@ -509,7 +509,8 @@ typedef struct mpm_tuning {
     int32_t grid_block;       /* 128 or 256 (default 256) */
     float p2g_ms, g2p_ms, grid_ms;  /* stage times of the chosen shapes (mpm_autotune) */
     int32_t p2g_cell_cap;     /* 4 .. 64: particles of a cell one lane sums before the
-                               * cell is shared by the warp (default 12) */
+                               * cell is shared by the warp; 0 (default): chosen per
+                               * work item from its cells' particle counts */
 } mpm_tuning;
 mpm_status mpm_autotune(mpm_engine* engine, int32_t repeats, mpm_tuning* out);
 mpm_status mpm_set_tuning(mpm_engine* engine, const mpm_tuning* tuning);
@@ -543,7 +544,8 @@ mpm_status mpm_get_tuning(mpm_engine* engine, mpm_tuning* tuning);
 typedef struct mpm_learned_stats {
     int64_t large_steps;         /* large steps accepted since creation */
     int64_t fallbacks;           /* large steps replaced by RATIO plain substeps */
-    double last_density_change;  /* the statistic of the last large step */
+    double last_density_change;  /* the statistic of the last large step that was checked
+                                  * (large steps are checked only when the fallback is on) */
 } mpm_learned_stats;
 
 /* Sets the corrector (params_host: MPM_CORRECTOR_PARAMS floats, or NULL for

@@ -144,7 +144,7 @@ struct mpm_engine {
     double last_density_change = 0.0;
 
     // Launch shapes of the substep (mpm_autotune / mpm_set_tuning).
-    mpm_tuning tune{12, 256, 256, 0.f, 0.f, 0.f, 12};
+    mpm_tuning tune{12, 256, 256, 0.f, 0.f, 0.f, 0};
 };
 
 namespace {
@@ -1111,17 +1111,20 @@ extern "C" mpm_status mpm_step_learned(mpm_engine* e, int32_t nlarge, mpm_learne
     for (int k = 0; k < nlarge; ++k) {
         const int par = e->parity;
         mpm::LearnArgs la{e->mlp_set ? e->mlp : nullptr, nullptr, nullptr, e->d_stat, large_blend(e)};
+        // The statistic is read back (a host sync per large step) only when
+        // it can trigger the fallback.
+        const bool judge = e->mlp_set && e->max_density_change >= 0.f;
         if (e->mlp_set) CK(e, cudaMemsetAsync(e->d_stat, 0, sizeof(float), e->stream));
         e->kernel_launches += enqueue_large(e, par, &la);
         CK(e, cudaGetLastError());
         e->sort_src = par;
         bool accept = true;
-        if (e->mlp_set) {
+        if (judge) {
             float sum = 0.f;
             CK(e, cudaMemcpyAsync(&sum, e->d_stat, sizeof(float), cudaMemcpyDeviceToHost, e->stream));
             CK(e, cudaStreamSynchronize(e->stream));
             e->last_density_change = e->n > 0 ? (double)sum / (double)e->n : 0.0;
-            accept = !(e->max_density_change >= 0.f) || e->last_density_change <= e->max_density_change;
+            accept = e->last_density_change <= e->max_density_change;
         }
         if (accept) {
             e->parity = 1 - par;
@@ -1395,7 +1398,7 @@ bool valid_tuning(const mpm_tuning& t) {
     return t.p2g_ctas_per_sm >= 1 && t.p2g_ctas_per_sm <= mpm::p2g_max_ctas_per_sm() &&
            (t.g2p_block == 128 || t.g2p_block == 256 || t.g2p_block == 512) &&
            (t.grid_block == 128 || t.grid_block == 256) &&
-           t.p2g_cell_cap >= 4 && t.p2g_cell_cap <= 64;
+           (t.p2g_cell_cap == 0 || (t.p2g_cell_cap >= 4 && t.p2g_cell_cap <= 64));
 }
 
 // Times stage `stage` of one substep from the current state and undoes the
@@ -1474,7 +1477,7 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
     }
     e->tune.p2g_ctas_per_sm = best.p2g_ctas_per_sm;
     tbest = best.p2g_ms;
-    for (int k : {8, 16, 24, 32}) {
+    for (int k : {12, 24, 32}) {
         if (s != MPM_OK) break;
         e->tune.p2g_cell_cap = k;
         if ((s = median_time(MPM_STAGE_P2G, &ms)) != MPM_OK) break;

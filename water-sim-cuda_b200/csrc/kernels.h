@@ -76,7 +76,7 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
 // P2G over the items of `cur`; gidx maps slots of the new order to P.
 // ctas_per_sm: persistent single-warp CTAs per SM (0 = the default 12);
 // cell_cap: particles of a cell its own lane sums before the cell is shared
-// by the whole warp (0 = the default 12).
+// by the whole warp (0 = chosen per work item from its cells' counts).
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
                const int32_t* cstart, const BinSet& cur, const long long* itemoff, uint32_t* work, float4* accum,
                uint32_t* status, cudaStream_t st, int ctas_per_sm = 0, int cell_cap = 0);

@@ -120,7 +120,7 @@ struct SceneLookup {
 // nodes in shared memory: the 32 cells of a layer are distinct, so for one
 // stencil offset the 32 nodes differ and a plain read-add-write per offset is
 // race-free.  A lane sums at most `cap` particles of its cell (a launch
-// parameter, kCellCap by default); the rest of
+// parameter; 0 = chosen per work item by item_cap); the rest of
 // a crowded cell (this Tait law resists only expansion, so compressed fluid
 // piles up) is shared by all 32 lanes and reduced across the warp.  The
 // footprint goes to global memory with one vector reduction per touched
@@ -237,6 +237,26 @@ __device__ __forceinline__ void p2g_stencil(const P2GParticle& r, Emit emit) {
     }
 }
 
+// The crowded-cell threshold of one work item, from the counts of its 32
+// cells (`full`, one per lane): for each candidate cap the loop costs
+// min(max count, cap) iterations with every lane, plus, per cell above the
+// cap, ceil((count - cap) / 32) iterations and one reduce-scatter (about 1.3
+// iterations); the cheapest candidate wins.  Every cap gives the same sums.
+__device__ __forceinline__ int item_cap(int full) {
+    const int maxc = __reduce_max_sync(0xffffffffu, (unsigned)full);
+    int best = kCellCap;
+    float best_cost = 1e30f;
+#pragma unroll
+    for (int cand : {8, 12, 16, 24, 32, 48, 64}) {
+        const int over = full > cand ? (full - cand + 31) / 32 : 0;
+        const int passes = (int)__reduce_add_sync(0xffffffffu, (unsigned)over);
+        const int cells = __popc(__ballot_sync(0xffffffffu, full > cand));
+        const float cost = (float)min(maxc, cand) + (float)passes + 1.3f * (float)cells;
+        if (cost < best_cost) best_cost = cost, best = cand;
+    }
+    return best;
+}
+
 __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, const float* __restrict__ P,
                                                                   const int32_t* __restrict__ gidx,
                                                                   const int32_t* __restrict__ cstart, BinSet set,
@@ -279,8 +299,9 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
         // cs + s).  Pass k > 0: the k-th crowded cell's further particles,
         // slot hcs + cap + lane + 32 s, for every lane.  One loop body
         // serves both; only the flush differs.
-        uint32_t crowded = __ballot_sync(0xffffffffu, full > cap);
-        int first = cs, step = 1, cnt = min(full, cap), target = lane;
+        const int icap = cap > 0 ? cap : item_cap(full);
+        uint32_t crowded = __ballot_sync(0xffffffffu, full > icap);
+        int first = cs, step = 1, cnt = min(full, icap), target = lane;
         for (;;) {
             float am[27], ax[27], ay[27], az[27];
             int maxc = cnt;
@@ -390,9 +411,9 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
             const int src = __ffs(crowded) - 1;
             crowded &= crowded - 1;
             const int hcnt = __shfl_sync(0xffffffffu, full, src);
-            first = __shfl_sync(0xffffffffu, cs, src) + cap + lane;
+            first = __shfl_sync(0xffffffffu, cs, src) + icap + lane;
             step = 32;
-            cnt = max(0, (hcnt - cap - lane + 31) / 32);
+            cnt = max(0, (hcnt - icap - lane + 31) / 32);
             target = src;
         }
         __syncwarp();
@@ -971,7 +992,7 @@ int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const fl
                uint32_t* status, cudaStream_t st, int ctas_per_sm, int cell_cap) {
     if (n <= 0) return 0;
     const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : kP2GWarpsPerSM;
-    const int cap = cell_cap > 0 ? cell_cap : kCellCap;
+    const int cap = cell_cap > 0 ? cell_cap : 0;
     const int warps = (int)std::min(bins_total * kBinZ, 148LL * per_sm);
     p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, itemoff, work, accum, status, cap);
     return 1;

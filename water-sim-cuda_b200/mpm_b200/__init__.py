@@ -393,7 +393,7 @@ class Engine:
         return {k: getattr(t, k) for k, _ in _Tuning._fields_}
 
     def set_tuning(self, p2g_ctas_per_sm: int = 12, g2p_block: int = 256, grid_block: int = 256,
-                   p2g_cell_cap: int = 12):
+                   p2g_cell_cap: int = 0):
         t = _Tuning(int(p2g_ctas_per_sm), int(g2p_block), int(grid_block), 0.0, 0.0, 0.0, int(p2g_cell_cap))
         self._check(lib.mpm_set_tuning(self._h, ctypes.byref(t)))
 

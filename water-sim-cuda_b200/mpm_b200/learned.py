@@ -34,6 +34,7 @@ from . import Corrector, Engine, scenes
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_PARAMS = os.path.join(HERE, "corrector_dam_break.npz")
+PHYSICAL_PARAMS = os.path.join(HERE, "corrector_dam_break_physical.npz")
 
 
 def dam_break_variant(seed: int, physical: bool = False):
