@@ -697,19 +697,20 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
     const float F[9] = {q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
 
     const int bx = stencil_base(pos[0]), by = stencil_base(pos[1]), bz = stencil_base(pos[2]);
+    // f = pos - base is exact, so f - o equals pos - (base + o) bit for bit
+    // and axis_weights gives bspline_weight's values.
+    const float fx = pos[0] - (float)bx, fy = pos[1] - (float)by, fz = pos[2] - (float)bz;
     float wx[3], wy[3], wz[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        wx[a] = bspline_weight(pos[0] - (float)(bx + a));
-        wy[a] = bspline_weight(pos[1] - (float)(by + a));
-        wz[a] = bspline_weight(pos[2] - (float)(bz + a));
-    }
+    axis_weights(fx, 1.0f, wx);
+    axis_weights(fy, 1.0f, wy);
+    axis_weights(fz, 1.0f, wz);
     float tv[3] = {0.f, 0.f, 0.f}, tc[9], tm = 0.f;
     // Set when a stencil node lies outside the grid or inside an obstacle:
     // only then can the SDF at the new position be negative (see below).
     uint32_t sdf_risk = 0u;
 #pragma unroll
     for (int k = 0; k < 9; ++k) tc[k] = 0.f;
+    const int plane = p.sx * p.sy;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const int z = bz + c;
@@ -717,7 +718,7 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
             sdf_risk = 1u;
             continue;
         }
-        const float dzv = -(pos[2] - (float)z);
+        const float dzv = -(fz - (float)c);
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
             const int y = by + b;
@@ -725,7 +726,8 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
                 sdf_risk = 1u;
                 continue;
             }
-            const float dyv = -(pos[1] - (float)y);
+            const float dyv = -(fy - (float)b);
+            const float4* row = vgrid + (z * plane + y * p.sx + bx);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 const int x = bx + a;
@@ -733,8 +735,8 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
                     sdf_risk = 1u;
                     continue;
                 }
-                const float dxv = -(pos[0] - (float)x);
-                const float4 g = __ldg(vgrid + node_index(p, x, y, z));
+                const float dxv = -(fx - (float)a);
+                const float4 g = __ldg(row + a);
                 sdf_risk |= __float_as_uint(g.x) >> 31;
                 const float w = wx[a] * wy[b] * wz[c];
                 tv[0] += w * g.y;
