@@ -553,6 +553,12 @@ typedef struct mpm_learned_stats {
  * fallback threshold (negative: never fall back). */
 mpm_status mpm_set_corrector(mpm_engine* engine, const float* params_host, int32_t ratio,
                              float max_density_change);
+/* Which tensor-core path evaluates the MLP inside the large step's G2P:
+ * tcgen05.mma with TMEM accumulators, 256 particles per CTA (default), or
+ * warp-level mma.sync (the same operands and roundings). */
+#define MPM_CORRECTOR_TCGEN05 0
+#define MPM_CORRECTOR_MMA_SYNC 1
+mpm_status mpm_set_corrector_kernel(mpm_engine* engine, int32_t kind);
 /* nlarge large steps (each RATIO x DT of simulated time); stats optional. */
 mpm_status mpm_step_learned(mpm_engine* engine, int32_t nlarge, mpm_learned_stats* stats);
 
@@ -589,8 +595,13 @@ mpm_status mpm_corrector_gradient(mpm_corrector* corrector, int64_t count, const
                                   float* grad_host, float* loss_host);
 mpm_status mpm_corrector_get_params(mpm_corrector* corrector, float* params_host);
 mpm_status mpm_corrector_set_params(mpm_corrector* corrector, const float* params_host);
-/* The tensor-core inference of the learned G2P on n feature rows. */
+/* The tensor-core inference of the learned G2P on n feature rows
+ * (warp-level mma.sync, bf16, fp32 accumulation). */
 mpm_status mpm_corrector_forward(mpm_corrector* corrector, int64_t n, const float* features_host, float* out_host);
+/* The same MLP on the 5th-generation tensor cores: tcgen05.mma with operands
+ * in shared memory and accumulators in tensor memory, 256 rows per CTA. */
+mpm_status mpm_corrector_forward_tc(mpm_corrector* corrector, int64_t n, const float* features_host,
+                                    float* out_host);
 
 #ifdef __cplusplus
 }

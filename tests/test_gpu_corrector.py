@@ -196,3 +196,41 @@ def test_collect_records_the_probe(gpu_ok, mpm):
     # density feature: interpolated mass over the seeding density, minus 1, is > -1
     assert (feats[:, 12] > -1).all()
     assert not feats[:, 13:16].any()  # no obstacle: the folded SDF is zero
+
+
+def test_forward_tcgen05_matches(gpu_ok, mpm):
+    """The tcgen05 / TMEM MLP against the torch reference and the mma.sync path
+    (both round the same operands to bf16; only fp32 summation order differs)."""
+    n = 4099  # 17 CTAs of 256 rows, the last one ragged
+    feats = _features(n, 11)
+    targs = np.random.default_rng(12).normal(0, 0.3, (n, 3)).astype(np.float32)
+    w = mlp_ref.random_params(13, feats, targs)
+    with mpm.Corrector(16) as c:
+        c.set_params(w)
+        tc = c.forward(feats, tcgen05=True)
+        ms = c.forward(feats)
+    want = mlp_ref.forward(torch.tensor(w), torch.tensor(feats)).detach().numpy()
+    scale = np.sqrt((want ** 2).mean(0))
+    assert (np.abs(tc - want).max(0) / scale < 2e-2).all()
+    assert (np.abs(tc - ms).max(0) / scale < 1e-2).all()
+
+
+def test_learned_step_tcgen05_matches_mma_sync(gpu_ok, mpm):
+    """The learned large step with the MLP on tcgen05 (default) and on
+    mma.sync: the same corrections up to fp32 summation order."""
+    cfg, st, tris = _small(mpm, n=5000, obstacle=True, seed=14)
+    feats = _features(2000, 15)
+    w = mlp_ref.random_params(16, feats)
+    mlp_ref.split(w)["out_std"][:] = 0.05
+    out = {}
+    for tc in (True, False):
+        with mpm.Engine(cfg) as e:
+            e.init(st)
+            e.init_sdf(tris)
+            e.set_corrector(w, ratio=4, max_density_change=-1.0)
+            e.set_corrector_kernel(tcgen05=tc)
+            e.step_learned(2)
+            out[tc] = e.get_buffer()
+    a, b = out[True], out[False]
+    assert np.abs(a[3:6] - b[3:6]).max() < 2e-3 * max(1.0, float(np.abs(b[3:6]).max()))
+    assert np.abs(a[0:3] - b[0:3]).max() < 2e-3

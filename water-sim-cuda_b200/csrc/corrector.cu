@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/mpm_b200.h"
+#include "corrector_tc.cuh"
 #include "kernels.h"
 
 namespace mpm {
@@ -60,6 +61,52 @@ __global__ void mlp_pack_kernel(const float* __restrict__ w, MlpPacked* __restri
         for (int k = 0; k < kMlpIn; ++k) m->in_mean[k] = w[kPInMean + k], m->in_inv_std[k] = w[kPInInvStd + k];
         for (int k = 0; k < 4; ++k) m->out_std[k] = k < kMlpOut ? w[kPOutStd + k] : 0.f;
     }
+}
+
+// params (fp32) -> the tcgen05 operand layout: one thread per weight entry.
+__global__ void mlp_pack_tc_kernel(const float* __restrict__ w, MlpTc* __restrict__ m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 64 * 16) {
+        const int r = i / 16, k = i % 16;
+        m->w1[canon_index(r, k, 16)] = __float2bfloat16_rn(w[kPW1 + i]);
+    } else if (i < 64 * 16 + 64 * 64) {
+        const int q = i - 64 * 16, r = q / 64, k = q % 64;
+        m->w2[canon_index(r, k, 64)] = __float2bfloat16_rn(w[kPW2 + q]);
+    } else if (i < 64 * 16 + 64 * 64 + 16 * 64) {
+        const int q = i - 64 * 16 - 64 * 64, r = q / 64, k = q % 64;
+        m->w3[canon_index(r, k, 64)] = __float2bfloat16_rn(r < kMlpOut ? w[kPW3 + r * 64 + k] : 0.f);
+    } else if (i == 64 * 16 + 64 * 64 + 16 * 64) {
+        for (int k = 0; k < 64; ++k) m->b1[k] = w[kPB1 + k], m->b2[k] = w[kPB2 + k];
+        for (int k = 0; k < 4; ++k) m->b3[k] = k < kMlpOut ? w[kPB3 + k] : 0.f;
+        for (int k = 0; k < kMlpIn; ++k) m->in_mean[k] = w[kPInMean + k], m->in_inv_std[k] = w[kPInInvStd + k];
+        for (int k = 0; k < 4; ++k) m->out_std[k] = k < kMlpOut ? w[kPOutStd + k] : 0.f;
+    }
+}
+
+// Stand-alone tcgen05 inference: 256 rows per CTA (the routine of the
+// learned G2P's tcgen05 mode).
+__global__ void __launch_bounds__(kTcThreads) mlp_infer_tc_kernel(const MlpTc* __restrict__ mlp,
+                                                                  const float* __restrict__ feat, long long n,
+                                                                  float* __restrict__ out, uint32_t* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    MlpTcSmem& s = *reinterpret_cast<MlpTcSmem*>(smem_raw);
+    const uint4* src = reinterpret_cast<const uint4*>(mlp);
+    uint4* dst = reinterpret_cast<uint4*>(&s.w);
+    for (int i = threadIdx.x; i < (int)(sizeof(MlpTc) / 16); i += blockDim.x) dst[i] = __ldg(src + i);
+    mlp_tc_begin(s);
+    const long long jj = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long j = jj < n ? jj : n - 1;
+    float x[kMlpIn], y[3];
+#pragma unroll
+    for (int k = 0; k < kMlpIn; ++k) x[k] = __ldg(feat + j * kMlpIn + k);
+    mlp_forward_tc(s, x, y);
+    mlp_tc_end(s);
+    if (s.failed) {
+        if (threadIdx.x == 0) atomicOr(status, kStatusTimeout);
+        return;
+    }
+    if (jj < n)
+        for (int o = 0; o < 3; ++o) out[j * 3 + o] = y[o];
 }
 
 // Stand-alone tensor-core inference (the same warp routine as the learned G2P).
@@ -362,6 +409,18 @@ int launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t st) {
     return 1;
 }
 
+int launch_mlp_pack_tc(const float* params, MlpTc* out, cudaStream_t st) {
+    mlp_pack_tc_kernel<<<blocks_of(64 * 16 + 64 * 64 + 16 * 64 + 1, 256), 256, 0, st>>>(params, out);
+    return 1;
+}
+
+int launch_mlp_infer_tc(const MlpTc* mlp, const float* feat, long long n, float* out, uint32_t* status,
+                        cudaStream_t st) {
+    if (n <= 0) return 0;
+    mlp_infer_tc_kernel<<<blocks_of(n, kTcThreads), kTcThreads, sizeof(MlpTcSmem), st>>>(mlp, feat, n, out, status);
+    return 1;
+}
+
 int launch_mlp_infer(const MlpPacked* mlp, const float* feat, long long n, float* out, cudaStream_t st) {
     if (n <= 0) return 0;
     mlp_infer_kernel<<<blocks_of(n, 256), 256, 0, st>>>(mlp, feat, n, out);
@@ -393,6 +452,8 @@ struct mpm_corrector {
     long long* idx = nullptr;  // explicit batch indices (gradient checks)
     long long idx_cap = 0;
     mpm::MlpPacked* packed = nullptr;
+    mpm::MlpTc* packed_tc = nullptr;
+    uint32_t* status = nullptr;
     float* io = nullptr;     // stand-alone inference staging
     long long io_cap = 0;
     int adam_t = 0;
@@ -491,6 +552,9 @@ mpm_status mpm_corrector_create(int32_t device, int64_t capacity, mpm_corrector*
     CA(cudaMalloc(&c->loss, sizeof(float)));
     CA(cudaMalloc(&c->mom, 2 * (mpm::kMlpIn + mpm::kMlpOut) * sizeof(double)));
     CA(cudaMalloc(&c->packed, sizeof(mpm::MlpPacked)));
+    CA(cudaMalloc(&c->packed_tc, sizeof(mpm::MlpTc)));
+    CA(cudaMalloc(&c->status, sizeof(uint32_t)));
+    CA(cudaMemsetAsync(c->status, 0, sizeof(uint32_t), c->stream));
     CA(cudaMemsetAsync(c->w, 0, mpm::kPCount * sizeof(float), c->stream));
     CA(cudaMemsetAsync(c->grad, 0, mpm::kPCount * sizeof(float), c->stream));
     CA(cudaMemsetAsync(c->m1, 0, mpm::kPCount * sizeof(float), c->stream));
@@ -508,7 +572,8 @@ void mpm_corrector_destroy(mpm_corrector* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (void* p : {(void*)c->feat, (void*)c->targ, (void*)c->w, (void*)c->grad, (void*)c->m1, (void*)c->m2,
-                    (void*)c->loss, (void*)c->mom, (void*)c->idx, (void*)c->packed, (void*)c->io})
+                    (void*)c->loss, (void*)c->mom, (void*)c->idx, (void*)c->packed, (void*)c->io,
+                    (void*)c->packed_tc, (void*)c->status})
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -685,6 +750,34 @@ mpm_status mpm_corrector_gradient(mpm_corrector* c, int64_t count, const int64_t
     if (loss_host) CC(c, cudaMemcpyAsync(loss_host, c->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CC(c, cudaMemsetAsync(c->grad, 0, mpm::kPCount * sizeof(float), c->stream));
     CC(c, cudaStreamSynchronize(c->stream));
+    return MPM_OK;
+}
+
+mpm_status mpm_corrector_forward_tc(mpm_corrector* c, int64_t n, const float* features_host, float* out_host) {
+    mpm_status st = center(c);
+    if (st != MPM_OK) return st;
+    if (n < 0 || (n > 0 && (!features_host || !out_host))) return cbad(c, "bad forward arguments");
+    if (n == 0) return MPM_OK;
+    st = ensure_io(c, n * (mpm::kMlpIn + mpm::kMlpOut));
+    if (st != MPM_OK) return st;
+    float* d_in = c->io;
+    float* d_out = c->io + n * mpm::kMlpIn;
+    mpm::launch_mlp_pack_tc(c->w, c->packed_tc, c->stream);
+    CC(c, cudaGetLastError());
+    CC(c, cudaMemcpyAsync(d_in, features_host, (size_t)n * mpm::kMlpIn * sizeof(float), cudaMemcpyHostToDevice,
+                          c->stream));
+    CC(c, cudaMemsetAsync(c->status, 0, sizeof(uint32_t), c->stream));
+    mpm::launch_mlp_infer_tc(c->packed_tc, d_in, n, d_out, c->status, c->stream);
+    CC(c, cudaGetLastError());
+    CC(c, cudaMemcpyAsync(out_host, d_out, (size_t)n * mpm::kMlpOut * sizeof(float), cudaMemcpyDeviceToHost,
+                          c->stream));
+    uint32_t flag = 0;
+    CC(c, cudaMemcpyAsync(&flag, c->status, sizeof(flag), cudaMemcpyDeviceToHost, c->stream));
+    CC(c, cudaStreamSynchronize(c->stream));
+    if (flag) {
+        c->last_error = "a bounded wait of the tcgen05 MLP gave up";
+        return MPM_ERR_TIMEOUT;
+    }
     return MPM_OK;
 }
 

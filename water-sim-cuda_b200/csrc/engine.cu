@@ -134,6 +134,8 @@ struct mpm_engine {
     SimParams* d_prm_large = nullptr;
     mpm::SceneTable table_large{};
     mpm::MlpPacked* mlp = nullptr;
+    mpm::MlpTc* mlp_tc = nullptr;
+    int corrector_kernel = MPM_CORRECTOR_TCGEN05;
     float* d_params = nullptr;
     float* d_stat = nullptr;
     float* feat_all = nullptr;  // [n][16]
@@ -747,6 +749,7 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->staging);
     free_dev(e->d_prm_large);
     free_dev(e->mlp);
+    free_dev(e->mlp_tc);
     free_dev(e->d_params);
     free_dev(e->d_stat);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -1075,6 +1078,7 @@ namespace mpm {
 mpm_status corrector_append(mpm_corrector* c, const float* feat_all, const float* vplain, const float* vlarge,
                             long long n, long long samples, unsigned long long seed, cudaStream_t st);
 int launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t st);
+int launch_mlp_pack_tc(const float* params, MlpTc* out, cudaStream_t st);
 int launch_velocity_export(const float* P, const int32_t* sigma, long long n, float* out, cudaStream_t st);
 }  // namespace mpm
 
@@ -1089,11 +1093,13 @@ extern "C" mpm_status mpm_set_corrector(mpm_engine* e, const float* params_host,
             if (!std::isfinite(params_host[i])) return record(e, MPM_ERR_INVALID_ARGUMENT, "a parameter is not finite");
         if (!e->mlp) {
             CK(e, cudaMalloc(&e->mlp, sizeof(mpm::MlpPacked)));
+            CK(e, cudaMalloc(&e->mlp_tc, sizeof(mpm::MlpTc)));
             CK(e, cudaMalloc(&e->d_params, MPM_CORRECTOR_PARAMS * sizeof(float)));
         }
         CK(e, cudaMemcpyAsync(e->d_params, params_host, MPM_CORRECTOR_PARAMS * sizeof(float), cudaMemcpyHostToDevice,
                               e->stream));
         e->kernel_launches += mpm::launch_mlp_pack(e->d_params, e->mlp, e->stream);
+        e->kernel_launches += mpm::launch_mlp_pack_tc(e->d_params, e->mlp_tc, e->stream);
         CK(e, cudaGetLastError());
         CK(e, cudaStreamSynchronize(e->stream));
     }
@@ -1110,7 +1116,9 @@ extern "C" mpm_status mpm_step_learned(mpm_engine* e, int32_t nlarge, mpm_learne
     if ((s = learned_ready(e)) != MPM_OK) return s;
     for (int k = 0; k < nlarge; ++k) {
         const int par = e->parity;
-        mpm::LearnArgs la{e->mlp_set ? e->mlp : nullptr, nullptr, nullptr, e->d_stat, large_blend(e)};
+        const bool tc = e->mlp_set && e->corrector_kernel == MPM_CORRECTOR_TCGEN05;
+        mpm::LearnArgs la{e->mlp_set ? e->mlp : nullptr, nullptr, nullptr, e->d_stat, large_blend(e),
+                          tc ? e->mlp_tc : nullptr, e->d_flags + 1};
         // The statistic is read back (a host sync per large step) only when
         // it can trigger the fallback.
         const bool judge = e->mlp_set && e->max_density_change >= 0.f;
@@ -1161,7 +1169,7 @@ extern "C" mpm_status mpm_corrector_collect(mpm_corrector* c, mpm_engine* e, int
     // The uncorrected large step, recording features and final velocities;
     // then back to its start state for RATIO plain substeps.
     const int par = e->parity;
-    mpm::LearnArgs la{nullptr, e->feat_all, e->vlarge, nullptr, large_blend(e)};
+    mpm::LearnArgs la{nullptr, e->feat_all, e->vlarge, nullptr, large_blend(e), nullptr, nullptr};
     e->kernel_launches += enqueue_large(e, par, &la);
     CK(e, cudaGetLastError());
     if ((s = rebin(e, par)) != MPM_OK) return s;
@@ -1505,5 +1513,14 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
     if (s != MPM_OK) return s;
     if ((s = capture_graphs(e)) != MPM_OK) return s;
     if (out) *out = best;
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_set_corrector_kernel(mpm_engine* e, int32_t kind) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (kind != MPM_CORRECTOR_TCGEN05 && kind != MPM_CORRECTOR_MMA_SYNC)
+        return record(e, MPM_ERR_INVALID_ARGUMENT, "unknown corrector kernel");
+    e->corrector_kernel = kind;
     return MPM_OK;
 }

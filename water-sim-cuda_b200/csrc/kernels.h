@@ -9,6 +9,7 @@
 #include <string>
 
 #include "corrector.cuh"
+#include "corrector_tc.cuh"
 #include "device_math.cuh"
 
 namespace mpm {
@@ -97,6 +98,8 @@ struct LearnArgs {
     float* vel;
     float* stat;
     float blend;
+    const MlpTc* mlp_tc;  // set: the MLP runs on tcgen05 (mlp unused)
+    uint32_t* status;     // kStatusTimeout when a tcgen05 wait gives up
 };
 
 // G2P: slot j of Pout = particle gidx[j] of Pin advanced one substep;

@@ -658,13 +658,13 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
 // features and final velocity by original index).  Large steps advect with
 // v_old + blend (v_new - v_old), blend = (R + 1) / (2R) for R plain substeps:
 // R substeps under a constant acceleration move a particle by exactly that.
-enum G2PMode : int { kG2PPlain = 0, kG2PLearned = 1, kG2PCollect = 2, kG2PLarge = 3 };
+enum G2PMode : int { kG2PPlain = 0, kG2PLearned = 1, kG2PCollect = 2, kG2PLarge = 3, kG2PLearnedTc = 4 };
 
 // kWide: 256-thread CTAs free to use up to 255 registers (one CTA per SM,
 // every node load of a particle in flight at once) instead of 64 registers
 // and four CTAs per SM; chosen by the autotuner.
 template <bool kBatch, int kMode, bool kWide = false>
-__global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch || kMode == 2) ? 3 : 4))) g2p_kernel(SceneTable sc, SimParams p0, long long n_total, const float* __restrict__ Pin,
+__global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch || kMode == 2 || kMode == 4) ? 3 : 4))) g2p_kernel(SceneTable sc, SimParams p0, long long n_total, const float* __restrict__ Pin,
                                                   float* __restrict__ Pout, const int32_t* __restrict__ gidx,
                                                   const int32_t* __restrict__ sig_in, int32_t* __restrict__ sig_out,
                                                   const float4* __restrict__ vgrid_all, const float* __restrict__ sdf_all,
@@ -674,11 +674,19 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
     __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
     __shared__ __align__(16) unsigned char s_mlp_raw[kMode == kG2PLearned ? sizeof(MlpPacked) : 16];
     __shared__ uint32_t s_stage[kMode == kG2PLearned ? 8 * 32 * kMlpStageStride : 1];
+    extern __shared__ __align__(1024) unsigned char s_dyn[];  // MlpTcSmem in the tcgen05 mode
     if constexpr (kMode == kG2PLearned) {
         const uint4* src = reinterpret_cast<const uint4*>(la.mlp);
         uint4* dst = reinterpret_cast<uint4*>(s_mlp_raw);
         for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) dst[i] = __ldg(src + i);
         __syncthreads();
+    }
+    if constexpr (kMode == kG2PLearnedTc) {
+        MlpTcSmem& ts = *reinterpret_cast<MlpTcSmem*>(s_dyn);
+        const uint4* src = reinterpret_cast<const uint4*>(la.mlp_tc);
+        uint4* dst = reinterpret_cast<uint4*>(&ts.w);
+        for (int i = threadIdx.x; i < (int)(sizeof(MlpTc) / 16); i += blockDim.x) dst[i] = __ldg(src + i);
+        mlp_tc_begin(ts);  // TMEM columns and the mbarrier; synchronises the CTA
     }
     const SceneLookup<kBatch> look(sc, sc.poff, s_prm, s_first);
     const long long jj = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -756,7 +764,7 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
             }
         }
     }
-    if constexpr (kMode == kG2PLearned || kMode == kG2PCollect) {
+    if constexpr (kMode == kG2PLearned || kMode == kG2PCollect || kMode == kG2PLearnedTc) {
         float f[kMlpIn];
 #pragma unroll
         for (int k = 0; k < 9; ++k) f[k] = tc[k];
@@ -769,10 +777,17 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
             const float s = phi * (1.0f - fabsf(phi) * 0.25f);
             f[13] = nrm.x * s, f[14] = nrm.y * s, f[15] = nrm.z * s;
         }
-        if constexpr (kMode == kG2PLearned) {
+        if constexpr (kMode == kG2PLearned || kMode == kG2PLearnedTc) {
             float dv[3];
-            mlp_forward_warp(*reinterpret_cast<const MlpPacked*>(s_mlp_raw), s_stage + (threadIdx.x >> 5) * 32 * kMlpStageStride,
-                             f, dv);
+            if constexpr (kMode == kG2PLearned) {
+                mlp_forward_warp(*reinterpret_cast<const MlpPacked*>(s_mlp_raw),
+                                 s_stage + (threadIdx.x >> 5) * 32 * kMlpStageStride, f, dv);
+            } else {
+                MlpTcSmem& ts = *reinterpret_cast<MlpTcSmem*>(s_dyn);
+                mlp_forward_tc(ts, f, dv);
+                mlp_tc_end(ts);  // TMEM freed before the rest of the particle update
+                if (ts.failed && threadIdx.x == 0) atomicOr(la.status, kStatusTimeout);
+            }
             tv[0] += dv[0], tv[1] += dv[1], tv[2] += dv[2];
             // Predicted relative density change of the step: 1 / det(I + dt C) - 1.
             float T[9];
@@ -1018,6 +1033,11 @@ int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const flo
     if (n <= 0) return 0;
     const LearnArgs la = learn ? *learn : LearnArgs{};
     const unsigned grid = blocks_for(n, 256);
+    if (learn && sc.count == 1 && la.mlp_tc) {
+        g2p_kernel<false, kG2PLearnedTc><<<grid, 256, sizeof(MlpTcSmem), st>>>(
+            sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, prank, next, health, la);
+        return 1;
+    }
     // Plain G2P: 128- or 256-thread CTAs, or 512 = the register-wide 256-thread
     // variant (the learned modes stage 8 warps of MLP inputs and always run 256).
     const bool wide = block == 512;

@@ -208,6 +208,7 @@ def _load() -> ctypes.CDLL:
         "mpm_get_tuning": (I32, [P, P]),
         "mpm_set_corrector": (I32, [P, P, I32, ctypes.c_float]),
         "mpm_step_learned": (I32, [P, I32, P]),
+        "mpm_set_corrector_kernel": (I32, [P, I32]),
         "mpm_corrector_create": (I32, [I32, I64, P]),
         "mpm_corrector_destroy": (None, [P]),
         "mpm_corrector_last_error": (ctypes.c_char_p, [P]),
@@ -222,6 +223,7 @@ def _load() -> ctypes.CDLL:
         "mpm_corrector_get_params": (I32, [P, P]),
         "mpm_corrector_set_params": (I32, [P, P]),
         "mpm_corrector_forward": (I32, [P, I64, P, P]),
+        "mpm_corrector_forward_tc": (I32, [P, I64, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -424,6 +426,10 @@ class Engine:
             raise ValueError(f"expected {CORRECTOR_PARAMS} parameters, got {w.size}")
         self._check(lib.mpm_set_corrector(self._h, _ptr(w), int(ratio), float(max_density_change)))
 
+    def set_corrector_kernel(self, tcgen05: bool = True):
+        """The MLP inside the learned G2P: tcgen05 + TMEM (default) or mma.sync."""
+        self._check(lib.mpm_set_corrector_kernel(self._h, 0 if tcgen05 else 1))
+
     def step_learned(self, nlarge: int = 1) -> dict:
         """nlarge large steps of RATIO x DT; returns the running learned-step counters."""
         s = _LearnedStats()
@@ -605,11 +611,12 @@ class Corrector:
             raise ValueError(f"expected {CORRECTOR_PARAMS} parameters")
         self._check(lib.mpm_corrector_set_params(self._h, _ptr(w)))
 
-    def forward(self, features: np.ndarray) -> np.ndarray:
-        """The tensor-core inference of the learned G2P."""
+    def forward(self, features: np.ndarray, tcgen05: bool = False) -> np.ndarray:
+        """The tensor-core inference of the learned G2P (mma.sync, or tcgen05 with TMEM)."""
         f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, CORRECTOR_FEATURES)
         out = np.empty((len(f), CORRECTOR_OUTPUTS), np.float32)
-        self._check(lib.mpm_corrector_forward(self._h, len(f), _ptr(f), _ptr(out)))
+        fn = lib.mpm_corrector_forward_tc if tcgen05 else lib.mpm_corrector_forward
+        self._check(fn(self._h, len(f), _ptr(f), _ptr(out)))
         return out
 
 
