@@ -198,7 +198,7 @@ __device__ __forceinline__ void mlp_tc_hidden(MlpTcSmem& s, const float* bias) {
     const int row = threadIdx.x, tile = row >> 7, r = row & 127;
     __nv_bfloat16* a = s.a + tile * 128 * 64;
     const uint32_t taddr = mlp_tc_taddr(s);
-#pragma unroll 1
+#pragma unroll
     for (int c0 = 0; c0 < 64; c0 += 16) {
         float v[16];
         tmem_ld16(taddr + (uint32_t)c0, v);
