@@ -247,6 +247,14 @@ const float* mpm_positions_device(mpm_engine* engine);
 
 /* mpm_positions_device + a device-to-host copy of 3*n floats. */
 mpm_status mpm_get_positions(mpm_engine* engine, float* xyz_host);
+/* As mpm_get_positions, without waiting: the copy runs on the engine's copy
+ * stream, after the export it reads and alongside the substeps that follow,
+ * and xyz_host holds the positions once mpm_positions_wait returns.  Exports
+ * alternate between two device buffers, and an export waits for the read-back
+ * of its buffer, so one frame can be read while the next computes.  Pinned
+ * host memory makes the copy asynchronous. */
+mpm_status mpm_get_positions_async(mpm_engine* engine, float* xyz_host);
+mpm_status mpm_positions_wait(mpm_engine* engine);
 
 /* Replaces Engine::getGrid (engine.h:22) + a copy of its 4 planes (4*G
  * floats, plane order MPM_GRID_*).  After a substep: mass from P2G and the

@@ -148,3 +148,29 @@ def test_scale_256_invariants(gpu_ok, mpm):
     assert np.isfinite(after[0:24]).all()
     assert np.array_equal(keys, morton_reference(before[0:3]))
     assert np.array_equal(perm, stable_sort_reference(keys))
+
+
+def test_async_positions_double_buffered(gpu_ok, mpm):
+    """mpm_get_positions_async: frame k's read-back overlaps frame k + 1 and
+    still returns frame k's positions."""
+    import torch
+    from mpm_b200 import scenes
+    cfg, st, tris = scenes.small_scene(20000, (48, 48, 48), seed=31)
+    with mpm.Engine(cfg) as e:
+        e.init(st)
+        e.init_sdf(tris)
+        want = []
+        for _ in range(3):
+            e.step(2)
+            want.append(e.get_positions().copy())
+    bufs = [torch.empty((20000, 3), dtype=torch.float32).pin_memory().numpy() for _ in range(3)]
+    with mpm.Engine(cfg) as e:
+        e.init(st)
+        e.init_sdf(tris)
+        for k in range(3):
+            e.step_async(2)
+            e.get_positions_async(bufs[k])
+        e.synchronize()
+        e.positions_wait()
+    for k in range(3):
+        assert np.abs(bufs[k] - want[k]).max() < 1e-4, k

@@ -83,7 +83,15 @@ struct mpm_engine {
     int32_t* ref_keys = nullptr;             // mpm_get_sort: keys in original order (one scene)
     int32_t* ref_perm = nullptr;             // mpm_get_sort: stable sort permutation
     void* sort_mem = nullptr;
-    float* pos_out = nullptr;  // float3 positions, all scenes, original order
+    // float3 positions, all scenes, original order: two buffers written by
+    // alternate exports, so that the host can read one back on copy_stream
+    // while the next frame computes (pos_ready: export done; copy_done: the
+    // read-back of that buffer done).
+    float* pos_buf[2] = {nullptr, nullptr};
+    int pos_cur = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pos_ready[2] = {nullptr, nullptr};
+    cudaEvent_t copy_done[2] = {nullptr, nullptr};
 
     float4* accum = nullptr;
     float4* vgrid = nullptr;
@@ -192,7 +200,8 @@ void free_particles(mpm_engine* e) {
     free_dev(e->ref_keys);
     free_dev(e->ref_perm);
     free_dev(e->sort_mem);
-    free_dev(e->pos_out);
+    free_dev(e->pos_buf[0]);
+    free_dev(e->pos_buf[1]);
     free_dev(e->feat_all);
     free_dev(e->vlarge);
     free_dev(e->vplain);
@@ -225,7 +234,8 @@ mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_by
     CK(e, cudaMalloc(&e->ref_keys, sbytes));
     CK(e, cudaMalloc(&e->ref_perm, sbytes));
     CK(e, cudaMalloc(&e->sort_mem, sort_bytes));
-    CK(e, cudaMalloc(&e->pos_out, cap * 3 * sizeof(float)));
+    CK(e, cudaMalloc(&e->pos_buf[0], cap * 3 * sizeof(float)));
+    CK(e, cudaMalloc(&e->pos_buf[1], cap * 3 * sizeof(float)));
     return MPM_OK;
 }
 
@@ -383,6 +393,8 @@ bool finite_cfg(const mpm_config* c) {
            std::isfinite(c->compression) && std::isfinite(c->resolution);
 }
 
+mpm_status export_positions(mpm_engine* e);
+
 // Uploads each scene's 26-plane host state and imports it (init_rules:
 // Engine::init), then files all particles into counter set 0.
 mpm_status load_states(mpm_engine* e, const float* const* soa26_host, bool init_rules) {
@@ -411,13 +423,9 @@ mpm_status load_states(mpm_engine* e, const float* const* soa26_host, bool init_
     e->accum_dirty = false;
     e->grid_view = GridView::kVelocity;
     e->health = 0;
-    for (int s = 0; s < e->scenes; ++s) {
-        const SimParams& p = e->prm[s];
-        e->kernel_launches += mpm::launch_positions_export(p, e->P[0] + p.poff * mpm::kAFloats, e->sigma[0] + p.poff,
-                                                           e->pos_out + p.poff * 3, e->stream);
-    }
-    CK(e, cudaGetLastError());
-    mpm_status st = capture_graphs(e);
+    mpm_status st = export_positions(e);
+    if (st != MPM_OK) return st;
+    st = capture_graphs(e);
     if (st != MPM_OK) return st;
     e->initialized = true;
     return sync_and_collect(e);
@@ -437,14 +445,20 @@ mpm_status enter_scene(mpm_engine* e, int32_t scene) {
     return MPM_OK;
 }
 
+// Exports the current positions into the other position buffer, once any
+// read-back of that buffer has finished, and makes it the current one.
 mpm_status export_positions(mpm_engine* e) {
+    const int b = 1 - e->pos_cur;
+    CK(e, cudaStreamWaitEvent(e->stream, e->copy_done[b], 0));
     for (int sc = 0; sc < e->scenes; ++sc) {
         const SimParams& p = e->prm[sc];
         e->kernel_launches += mpm::launch_positions_export(p, e->P[e->parity] + p.poff * mpm::kAFloats,
-                                                           e->sigma[e->parity] + p.poff, e->pos_out + p.poff * 3,
+                                                           e->sigma[e->parity] + p.poff, e->pos_buf[b] + p.poff * 3,
                                                            e->stream);
     }
     CK(e, cudaGetLastError());
+    CK(e, cudaEventRecord(e->pos_ready[b], e->stream));
+    e->pos_cur = b;
     return MPM_OK;
 }
 
@@ -549,8 +563,13 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
         return s;
     };
     if (cudaSetDevice(device) != cudaSuccess) return fail(cuda_fail(e, cudaGetLastError(), "cudaSetDevice"));
-    if ((err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    if ((err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (err = cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
         return fail(cuda_fail(e, err, "cudaStreamCreate"));
+    for (int k = 0; k < 2; ++k)
+        if ((err = cudaEventCreateWithFlags(&e->pos_ready[k], cudaEventDisableTiming)) != cudaSuccess ||
+            (err = cudaEventCreateWithFlags(&e->copy_done[k], cudaEventDisableTiming)) != cudaSuccess)
+            return fail(cuda_fail(e, err, "cudaEventCreate"));
     if ((err = cudaMalloc(&e->accum, (size_t)g_total * sizeof(float4))) != cudaSuccess ||
         (err = cudaMalloc(&e->vgrid, (size_t)g_total * sizeof(float4))) != cudaSuccess ||
         (err = cudaMalloc(&e->sdf, (size_t)g_total * sizeof(float))) != cudaSuccess ||
@@ -752,6 +771,12 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->mlp_tc);
     free_dev(e->d_params);
     free_dev(e->d_stat);
+    if (e->copy_stream) cudaStreamSynchronize(e->copy_stream);
+    for (int k = 0; k < 2; ++k) {
+        if (e->pos_ready[k]) cudaEventDestroy(e->pos_ready[k]);
+        if (e->copy_done[k]) cudaEventDestroy(e->copy_done[k]);
+    }
+    if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -912,7 +937,38 @@ extern "C" mpm_status mpm_get_state(mpm_engine* e, float* out) { return mpm_scen
 
 extern "C" const float* mpm_scene_positions_device(mpm_engine* e, int32_t scene) {
     if (!e || !e->initialized || scene < 0 || scene >= e->scenes) return nullptr;
-    return e->pos_out + e->prm[scene].poff * 3;
+    return e->pos_buf[e->pos_cur] + e->prm[scene].poff * 3;
+}
+
+namespace {
+// Enqueues the read-back of the current positions of `scene` (-1: all
+// scenes) on the copy stream, after the export that wrote them.
+mpm_status enqueue_positions_copy(mpm_engine* e, int32_t scene, float* xyz) {
+    const int b = e->pos_cur;
+    const long long first = scene < 0 ? 0 : e->prm[scene].poff;
+    const long long count = scene < 0 ? e->n : e->prm[scene].n;
+    CK(e, cudaStreamWaitEvent(e->copy_stream, e->pos_ready[b], 0));
+    if (count > 0)
+        CK(e, cudaMemcpyAsync(xyz, e->pos_buf[b] + first * 3, (size_t)count * 3 * sizeof(float),
+                              cudaMemcpyDeviceToHost, e->copy_stream));
+    CK(e, cudaEventRecord(e->copy_done[b], e->copy_stream));
+    return MPM_OK;
+}
+}  // namespace
+
+extern "C" mpm_status mpm_get_positions_async(mpm_engine* e, float* xyz) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
+    if (e->n > 0 && !xyz) return record(e, MPM_ERR_INVALID_ARGUMENT, "xyz_host is NULL");
+    return enqueue_positions_copy(e, -1, xyz);
+}
+
+extern "C" mpm_status mpm_positions_wait(mpm_engine* e) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    CK(e, cudaStreamSynchronize(e->copy_stream));
+    return MPM_OK;
 }
 
 extern "C" const float* mpm_positions_device(mpm_engine* e) { return mpm_scene_positions_device(e, 0); }
@@ -924,9 +980,8 @@ extern "C" mpm_status mpm_scene_get_positions(mpm_engine* e, int32_t scene, floa
     const SimParams& p = e->prm[scene];
     if (p.n == 0) return MPM_OK;
     if (!xyz) return record(e, MPM_ERR_INVALID_ARGUMENT, "xyz_host is NULL");
-    CK(e, cudaMemcpyAsync(xyz, e->pos_out + p.poff * 3, (size_t)p.n * 3 * sizeof(float), cudaMemcpyDeviceToHost,
-                          e->stream));
-    CK(e, cudaStreamSynchronize(e->stream));
+    if ((s = enqueue_positions_copy(e, scene, xyz)) != MPM_OK) return s;
+    CK(e, cudaStreamSynchronize(e->copy_stream));
     return MPM_OK;
 }
 

@@ -148,6 +148,8 @@ def _load() -> ctypes.CDLL:
         "mpm_set_state": (I32, [P, I64, P]),
         "mpm_positions_device": (P, [P]),
         "mpm_get_positions": (I32, [P, P]),
+        "mpm_get_positions_async": (I32, [P, P]),
+        "mpm_positions_wait": (I32, [P]),
         "mpm_get_grid": (I32, [P, P]),
         "mpm_get_sdf": (I32, [P, P]),
         "mpm_get_sort": (I32, [P, P, P]),
@@ -351,6 +353,13 @@ class Engine:
             out = np.empty((self.n, 3), np.float32)
         self._check(lib.mpm_get_positions(self._h, _ptr(out)))
         return out
+
+    def get_positions_async(self, out: np.ndarray):
+        """Start reading the current positions into `out` (pinned for overlap); see positions_wait."""
+        self._check(lib.mpm_get_positions_async(self._h, _ptr(out)))
+
+    def positions_wait(self):
+        self._check(lib.mpm_positions_wait(self._h))
 
     def positions_device_ptr(self) -> int:
         return int(lib.mpm_positions_device(self._h) or 0)

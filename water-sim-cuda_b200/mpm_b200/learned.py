@@ -59,25 +59,32 @@ def physical_config(cfg):
 
 
 def collect(corr: Corrector, seeds, substeps: int, probe_every: int, samples: int, ratio: int = 4,
-            physical: bool = False, log=print):
-    """Plain trajectories of `substeps` substeps on dam_break_variant(seed),
-    with the collection probe every `probe_every` substeps."""
+            physical: bool = False, log=print, policy=None):
+    """Trajectories of `substeps` substeps on dam_break_variant(seed), with the
+    collection probe every `probe_every` substeps.  Between probes the
+    trajectory advances with plain substeps, or, given `policy` parameters,
+    with learned large steps (no fallback): the probes then sample the states
+    a learned rollout visits (dataset aggregation)."""
     for k, seed in enumerate(seeds):
         cfg, st, tris = dam_break_variant(seed, physical)
         with Engine(cfg) as e:
             e.init(st)
             e.init_sdf(tris)
-            e.set_corrector(None, ratio=ratio)
             done = 0
             probe = 0
             while done + ratio <= substeps:
                 if done % probe_every == 0:
+                    e.set_corrector(None, ratio=ratio)
                     corr.collect(e, samples, seed=seed * 100003 + probe)
                     probe += 1
                     done += ratio
                 else:
                     step = min(probe_every - done % probe_every, substeps - done)
-                    e.step(step)
+                    if policy is not None and step % ratio == 0:
+                        e.set_corrector(policy, ratio=ratio, max_density_change=-1.0)
+                        e.step_learned(step // ratio)
+                    else:
+                        e.step(step)
                     done += step
         log(f"variant {k + 1}/{len(seeds)} seed {seed}: {corr.size} samples")
 
@@ -214,6 +221,8 @@ def main(argv=None):
     t.add_argument("--ratio", type=int, default=4)
     t.add_argument("--physical", action="store_true")
     t.add_argument("--out", default=DEFAULT_PARAMS)
+    t.add_argument("--dagger", default=None, help="parameters whose learned rollouts add probes")
+    t.add_argument("--dagger-variants", type=int, default=100)
     ev = sub.add_parser("evaluate")
     ev.add_argument("--params", default=DEFAULT_PARAMS)
     ev.add_argument("--large-steps", type=int, default=250)
@@ -225,16 +234,22 @@ def main(argv=None):
     if a.cmd == "train":
         seeds = list(range(a.first_seed, a.first_seed + a.variants))
         probes = a.substeps // a.probe_every
-        cap = a.variants * (probes + 1) * a.samples
+        extra = a.dagger_variants if a.dagger else 0
+        cap = (a.variants + extra) * (probes + 1) * a.samples
         t0 = time.perf_counter()
         with Corrector(cap) as c:
             collect(c, seeds, a.substeps, a.probe_every, a.samples, a.ratio, a.physical)
+            if a.dagger:
+                policy, _ = load_params(a.dagger)
+                dseeds = list(range(a.first_seed + 100000, a.first_seed + 100000 + extra))
+                collect(c, dseeds, a.substeps, a.probe_every, a.samples, a.ratio, a.physical, policy=policy)
             t_collect = time.perf_counter() - t0
             losses, t_train = train(c, a.steps, a.batch, a.lr)
             params = c.get_params()
             meta = {"variants": a.variants, "first_seed": a.first_seed, "substeps": a.substeps,
                     "probe_every": a.probe_every, "samples_per_probe": a.samples, "dataset": c.size,
                     "steps": a.steps, "batch": a.batch, "lr": a.lr, "ratio": a.ratio, "physical": a.physical,
+                    "dagger": os.path.basename(a.dagger) if a.dagger else None, "dagger_variants": extra,
                     "losses": losses, "collect_s": t_collect, "train_s": t_train}
         save_params(a.out, params, meta)
         print(json.dumps({k: v for k, v in meta.items() if k != "losses"} | {"final_loss": losses[-1]}))
