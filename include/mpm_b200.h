@@ -505,7 +505,7 @@ mpm_status mpm_triangles_normalize(float* triangles9_host, int64_t* t, float nor
 /* ------------------------------------------------------------------ */
 /* The substep's launch shapes: persistent P2G CTAs per SM and P2G's
  * crowded-cell threshold, and the CTA sizes of the plain G2P and of the grid
- * update.  mpm_autotune times each
+ * update.  mpm_autotune leaves the threshold to P2G's per-item choice (0).  mpm_autotune times each
  * candidate on the engine's current particles (each stage on its own, the
  * median of `repeats` runs; every timed substep is undone, so the state does
  * not advance) and keeps the fastest; results are identical for every shape

@@ -1519,6 +1519,7 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
         return cuda_fail(e, cudaGetLastError(), "cudaEventCreate");
     }
     mpm_tuning best = e->tune;
+    best.p2g_cell_cap = e->tune.p2g_cell_cap = 0;
     auto median_time = [&](int stage, float* ms) -> mpm_status {
         std::vector<float> t(repeats);
         for (int r = 0; r < repeats; ++r) {
@@ -1539,14 +1540,9 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
         if (ms < tbest) tbest = ms, best.p2g_ctas_per_sm = k, best.p2g_ms = ms;
     }
     e->tune.p2g_ctas_per_sm = best.p2g_ctas_per_sm;
-    tbest = best.p2g_ms;
-    for (int k : {12, 24, 32}) {
-        if (s != MPM_OK) break;
-        e->tune.p2g_cell_cap = k;
-        if ((s = median_time(MPM_STAGE_P2G, &ms)) != MPM_OK) break;
-        if (ms < tbest) tbest = ms, best.p2g_cell_cap = k, best.p2g_ms = ms;
-    }
-    e->tune.p2g_cell_cap = best.p2g_cell_cap;
+    // The crowded-cell threshold is not tuned here: P2G chooses it per work
+    // item from the counts it sees, which follows the state as it evolves,
+    // while a fixed value timed on one state can cost far more later.
     tbest = 1e30f;
     for (int k : {128, 256}) {
         if (s != MPM_OK) break;

@@ -719,48 +719,64 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
 #pragma unroll
     for (int k = 0; k < 9; ++k) tc[k] = 0.f;
     const int plane = p.sx * p.sy;
+    // One node of the stencil, offsets (a, b, c), `row` = node (base x, y, z).
+    auto gather = [&](int a, int b, int c, const float4* row) {
+        const float dxv = -(fx - (float)a), dyv = -(fy - (float)b), dzv = -(fz - (float)c);
+        const float4 g = __ldg(row + a);
+        sdf_risk |= __float_as_uint(g.x) >> 31;
+        const float w = wx[a] * wy[b] * wz[c];
+        tv[0] += w * g.y;
+        tv[1] += w * g.z;
+        tv[2] += w * g.w;
+        if constexpr (kMode != kG2PPlain) tm += w * fabsf(g.x);
+        const float term = 4.0f * w;
+        tc[0] += term * g.y * dxv;
+        tc[1] += term * g.y * dyv;
+        tc[2] += term * g.y * dzv;
+        tc[3] += term * g.z * dxv;
+        tc[4] += term * g.z * dyv;
+        tc[5] += term * g.z * dzv;
+        tc[6] += term * g.w * dxv;
+        tc[7] += term * g.w * dyv;
+        tc[8] += term * g.w * dzv;
+    };
+    // Whole stencil inside the grid (almost every particle): no per-node
+    // bounds tests.  Both branches add the nodes in the same order.
+    const bool inside = p.sx >= 3 && p.sy >= 3 && p.sz >= 3 && (unsigned)bx <= (unsigned)(p.sx - 3) &&
+                        (unsigned)by <= (unsigned)(p.sy - 3) && (unsigned)bz <= (unsigned)(p.sz - 3);
+    if (inside) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        const int z = bz + c;
-        if ((unsigned)z >= (unsigned)p.sz) {
-            sdf_risk = 1u;
-            continue;
-        }
-        const float dzv = -(fz - (float)c);
+        for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
-            const int y = by + b;
-            if ((unsigned)y >= (unsigned)p.sy) {
+            for (int b = 0; b < 3; ++b) {
+                const float4* row = vgrid + ((bz + c) * plane + (by + b) * p.sx + bx);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) gather(a, b, c, row);
+            }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int z = bz + c;
+            if ((unsigned)z >= (unsigned)p.sz) {
                 sdf_risk = 1u;
                 continue;
             }
-            const float dyv = -(fy - (float)b);
-            const float4* row = vgrid + (z * plane + y * p.sx + bx);
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                const int x = bx + a;
-                if ((unsigned)x >= (unsigned)p.sx) {
+            for (int b = 0; b < 3; ++b) {
+                const int y = by + b;
+                if ((unsigned)y >= (unsigned)p.sy) {
                     sdf_risk = 1u;
                     continue;
                 }
-                const float dxv = -(fx - (float)a);
-                const float4 g = __ldg(row + a);
-                sdf_risk |= __float_as_uint(g.x) >> 31;
-                const float w = wx[a] * wy[b] * wz[c];
-                tv[0] += w * g.y;
-                tv[1] += w * g.z;
-                tv[2] += w * g.w;
-                if constexpr (kMode != kG2PPlain) tm += w * fabsf(g.x);
-                const float term = 4.0f * w;
-                tc[0] += term * g.y * dxv;
-                tc[1] += term * g.y * dyv;
-                tc[2] += term * g.y * dzv;
-                tc[3] += term * g.z * dxv;
-                tc[4] += term * g.z * dyv;
-                tc[5] += term * g.z * dzv;
-                tc[6] += term * g.w * dxv;
-                tc[7] += term * g.w * dyv;
-                tc[8] += term * g.w * dzv;
+                const float4* row = vgrid + (z * plane + y * p.sx + bx);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    if ((unsigned)(bx + a) >= (unsigned)p.sx) {
+                        sdf_risk = 1u;
+                        continue;
+                    }
+                    gather(a, b, c, row);
+                }
             }
         }
     }
