@@ -601,6 +601,14 @@ mpm_status mpm_corrector_train(mpm_corrector* corrector, int32_t steps, int32_t 
  * of 64) at the current parameters, without a step. */
 mpm_status mpm_corrector_gradient(mpm_corrector* corrector, int64_t count, const int64_t* idx_host,
                                   float* grad_host, float* loss_host);
+/* Which kernel computes the training gradient: tcgen05.mma with TMEM
+ * accumulators, 128 samples per tile, every GEMM of the forward and backward
+ * pass on the tensor cores with bf16 operands (default); or FP32 on the CUDA
+ * cores with the forward roundings of the inference.  A bounded wait of the
+ * tcgen05 kernel that gives up is reported as MPM_ERR_TIMEOUT. */
+#define MPM_TRAIN_TCGEN05 0
+#define MPM_TRAIN_FP32 1
+mpm_status mpm_corrector_set_train_kernel(mpm_corrector* corrector, int32_t kind);
 mpm_status mpm_corrector_get_params(mpm_corrector* corrector, float* params_host);
 mpm_status mpm_corrector_set_params(mpm_corrector* corrector, const float* params_host);
 /* The tensor-core inference of the learned G2P on n feature rows

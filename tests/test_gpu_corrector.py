@@ -48,16 +48,21 @@ def test_forward_matches_torch(gpu_ok, mpm):
     assert np.abs(got2[::-1] - got).max() <= 1e-6 * np.abs(got).max()
 
 
-def test_gradient_matches_autograd(gpu_ok, mpm):
-    n = 1024
-    feats = _features(n, 4)
+@pytest.mark.parametrize("kernel", ["tcgen05", "fp32"])
+@pytest.mark.parametrize("n", [1024, 64, 192])
+def test_gradient_matches_autograd(gpu_ok, mpm, kernel, n):
+    """1024 samples: 8 full tiles of the tcgen05 kernel; 64 and 192: a
+    half-filled last tile (its rows beyond the batch are masked)."""
+    feats = _features(1024, 4)
     targs = (np.tanh(feats[:, 9:12]) * 0.5 + 0.1 * feats[:, 0:3]).astype(np.float32)
     w = mlp_ref.random_params(5, feats, targs)
-    with mpm.Corrector(n) as c:
+    idx = np.random.default_rng(n).permutation(1024)[:n]
+    with mpm.Corrector(1024) as c:
         c.add_data(feats, targs)
         c.set_params(w)
-        g, loss = c.gradient(np.arange(n))
-    want_loss, want_g = mlp_ref.loss_and_grad(w, feats, targs)
+        c.set_train_kernel(kernel)
+        g, loss = c.gradient(idx)
+    want_loss, want_g = mlp_ref.loss_and_grad(w, feats[idx], targs[idx])
     assert abs(loss - want_loss) <= 1e-2 * want_loss
     for name in ("W1", "b1", "W2", "b2", "W3", "b3"):
         o, k = mlp_ref.OFF[name]
@@ -66,6 +71,26 @@ def test_gradient_matches_autograd(gpu_ok, mpm):
         assert rel < 2e-2, (name, rel)
     # normalisation entries are not trained
     assert not g[:35].any()
+
+
+def test_train_kernels_agree(gpu_ok, mpm):
+    """The same Adam steps with either gradient kernel end at nearby parameters."""
+    n = 50_000
+    feats = _features(n, 8)
+    targs = (np.tanh(feats[:, 9:12]) + 0.3 * feats[:, 0:3]).astype(np.float32)
+    out = {}
+    for kernel in ("tcgen05", "fp32"):
+        with mpm.Corrector(n) as c:
+            c.add_data(feats, targs)
+            c.init(seed=3)
+            c.set_train_kernel(kernel)
+            out[kernel] = (c.train(40, batch=8192, lr=1e-3, seed=4), c.get_params())
+    (la, wa), (lb, wb) = out["tcgen05"], out["fp32"]
+    assert abs(la - lb) <= 2e-2 * lb, (la, lb)
+    for name in ("W1", "W2", "W3"):
+        o, k = mlp_ref.OFF[name]
+        rel = np.linalg.norm(wa[o:o + k] - wb[o:o + k]) / np.linalg.norm(wb[o:o + k])
+        assert rel < 2e-2, (name, rel)
 
 
 def test_training_fits_a_smooth_map(gpu_ok, mpm):

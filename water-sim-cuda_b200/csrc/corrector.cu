@@ -15,7 +15,7 @@
 #include <vector>
 
 #include "../../include/mpm_b200.h"
-#include "corrector_tc.cuh"
+#include "corrector_tc_train.cuh"
 #include "kernels.h"
 
 namespace mpm {
@@ -400,6 +400,237 @@ __global__ void adam_kernel(float* __restrict__ w, float* __restrict__ grad, flo
     w[i] -= lr * (a / bc1) / (sqrtf(b / bc2) + eps);
 }
 
+// The training gradient on tcgen05 (corrector_tc_train.cuh): the loss and
+// batch of mlp_train_kernel, tiles of 128 samples, rows at or beyond `batch`
+// masked by dY = 0.  A bounded wait that gives up sets kStatusTimeout in
+// *status and the CTA adds nothing to the gradient.
+__global__ void __launch_bounds__(kTrThreads, 1) mlp_train_tc_kernel(
+    const float* __restrict__ w, const float* __restrict__ feat, const float* __restrict__ targ, long long size,
+    const long long* __restrict__ idx_list, int batch, unsigned long long seed, int step, float* __restrict__ grad,
+    float* __restrict__ loss, uint32_t* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    MlpTrainSmem& s = *reinterpret_cast<MlpTrainSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, wq = (tid >> 5) & 3, ch = 32 * (tid >> 7);
+    const int srow = 32 * wq + lane;  // this thread's sample row in the epilogues
+    // Weights, their transposed copies, and the zero padding of dY and dZ^T.
+    for (int i = tid; i < 64 * 16; i += kTrThreads)
+        s.w.w1[canon_index(i / 16, i % 16, 16)] = __float2bfloat16_rn(w[kPW1 + i]);
+    for (int i = tid; i < 64 * 64; i += kTrThreads) {
+        const int u = i / 64, k = i % 64;
+        const __nv_bfloat16 v = __float2bfloat16_rn(w[kPW2 + i]);
+        s.w.w2[canon_index(u, k, 64)] = v;
+        s.w.w2t[canon_index(k, u, 64)] = v;
+    }
+    for (int i = tid; i < 16 * 64; i += kTrThreads) {
+        const int o = i / 64, k = i % 64;
+        const __nv_bfloat16 v = __float2bfloat16_rn(o < kMlpOut ? w[kPW3 + o * 64 + k] : 0.f);
+        s.w.w3[canon_index(o, k, 64)] = v;
+        s.w.w3t[canon_index(k, o, 16)] = v;
+    }
+    if (tid < 64) s.w.b1[tid] = w[kPB1 + tid], s.w.b2[tid] = w[kPB2 + tid];
+    if (tid < 4) s.w.b3[tid] = tid < kMlpOut ? w[kPB3 + tid] : 0.f;
+    for (int i = tid; i < (int)(sizeof(s.dy) / 16); i += kTrThreads) reinterpret_cast<uint4*>(s.dy)[i] = uint4{0, 0, 0, 0};
+    for (int i = tid; i < (int)(sizeof(s.dzt) / 16); i += kTrThreads)
+        reinterpret_cast<uint4*>(s.dzt)[i] = uint4{0, 0, 0, 0};
+    if (tid < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem)),
+                     "r"(kTrTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(&s.mbar, 1);
+        s.failed = 0u;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tm = s.tmem;
+    const uint32_t trow = tm + ((uint32_t)(32 * wq) << 16);  // this warp's TMEM lanes
+    const float inv_count = 1.0f / ((float)batch * kMlpOut);
+    float gW3 = 0.f, gB3 = 0.f, gB2 = 0.f, gB1 = 0.f, lsum = 0.f;
+    uint32_t phase = 0;
+    bool any = false;
+    const int ntiles = (batch + kTrTile - 1) / kTrTile;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        if (tid < kTrTile) {
+            const long long i = (long long)tile * kTrTile + tid;
+            long long j = 0;
+            if (i < batch) j = idx_list ? idx_list[i] : sample_index(seed, 0x7A11ull + (unsigned long long)step, i, size);
+            s.sidx[tid] = j;
+        }
+        __syncthreads();
+        for (int e = tid; e < kTrTile * kMlpIn; e += kTrThreads) {
+            const int r = e >> 4, k = e & 15;
+            const __nv_bfloat16 v =
+                __float2bfloat16_rn((feat[s.sidx[r] * kMlpIn + k] - w[kPInMean + k]) * w[kPInInvStd + k]);
+            s.x[canon_index(r, k, 16)] = v;
+            s.xt[canon_index(k, r, kTrTile)] = v;
+        }
+        for (int e = tid; e < kTrTile * kMlpOut; e += kTrThreads) {
+            const int r = e / kMlpOut, o = e % kMlpOut;
+            s.dyf[r * 4 + o] = targ[s.sidx[r] * kMlpOut + o] / w[kPOutStd + o];
+        }
+        // Z1 = X W1^T.
+        mlp_tr_publish();
+        if (tid == 0) {
+            mlp_tr_mma(tm + kTrColZ1, s.x, s.w.w1, 64, 16, false);
+            umma_commit(&s.mbar);
+        }
+        if (!mlp_tr_wait(s, phase)) break;
+        float g1[32], g2[32];
+        {
+            float v[32];
+            tmem_ld32(trow + kTrColZ1 + (uint32_t)ch, v);
+#pragma unroll
+            for (int j = 0; j < 32; j += 2) {
+                const int u = ch + j;
+                const float z0 = v[j] + s.w.b1[u], z1 = v[j + 1] + s.w.b1[u + 1];
+                g1[j] = gelu_tanh_grad(z0);
+                g1[j + 1] = gelu_tanh_grad(z1);
+                const __nv_bfloat162 h = __floats2bfloat162_rn(gelu_tanh(z0), gelu_tanh(z1));
+                *reinterpret_cast<__nv_bfloat162*>(s.h1 + canon_index(srow, u, 64)) = h;
+                s.h1t[canon_index(u, srow, kTrTile)] = h.x;
+                s.h1t[canon_index(u + 1, srow, kTrTile)] = h.y;
+            }
+        }
+        // Z2 = H1 W2^T.
+        mlp_tr_publish();
+        if (tid == 0) {
+            mlp_tr_mma(tm + kTrColZ2, s.h1, s.w.w2, 64, 64, false);
+            umma_commit(&s.mbar);
+        }
+        if (!mlp_tr_wait(s, phase)) break;
+        {
+            float v[32];
+            tmem_ld32(trow + kTrColZ2 + (uint32_t)ch, v);
+#pragma unroll
+            for (int j = 0; j < 32; j += 2) {
+                const int u = ch + j;
+                const float z0 = v[j] + s.w.b2[u], z1 = v[j + 1] + s.w.b2[u + 1];
+                g2[j] = gelu_tanh_grad(z0);
+                g2[j + 1] = gelu_tanh_grad(z1);
+                *reinterpret_cast<__nv_bfloat162*>(s.h2 + canon_index(srow, u, 64)) =
+                    __floats2bfloat162_rn(gelu_tanh(z0), gelu_tanh(z1));
+            }
+        }
+        // Y = H2 W3^T; the loss and dY.
+        mlp_tr_publish();
+        if (tid == 0) {
+            mlp_tr_mma(tm + kTrColY, s.h2, s.w.w3, 16, 64, false);
+            umma_commit(&s.mbar);
+        }
+        if (!mlp_tr_wait(s, phase)) break;
+        if (ch == 0) {
+            float v[16];
+            tmem_ld16(trow + kTrColY, v);
+            const bool valid = (long long)tile * kTrTile + srow < batch;
+#pragma unroll
+            for (int o = 0; o < kMlpOut; ++o) {
+                const float d = v[o] + s.w.b3[o] - s.dyf[srow * 4 + o];
+                const float dy = valid ? 2.0f * d * inv_count : 0.f;
+                if (valid) lsum += d * d;
+                s.dyf[srow * 4 + o] = dy;
+                s.dy[canon_index(srow, o, 16)] = __float2bfloat16_rn(dy);
+            }
+        }
+        // dH2 = dY W3 on the tensor cores while the CUDA cores sum the
+        // output layer's gradients.
+        mlp_tr_publish();
+        if (tid == 0) {
+            mlp_tr_mma(tm + kTrColZ1, s.dy, s.w.w3t, 64, 16, false);
+            umma_commit(&s.mbar);
+        }
+        if (tid < kMlpOut * 64) {
+            const int o = tid >> 6, k = tid & 63;
+            float acc = 0.f;
+            for (int r = 0; r < kTrTile; ++r) acc += s.dyf[r * 4 + o] * __bfloat162float(s.h2[canon_index(r, k, 64)]);
+            gW3 += acc;
+        } else if (tid < kMlpOut * 64 + kMlpOut) {
+            const int o = tid - kMlpOut * 64;
+            float acc = 0.f;
+            for (int r = 0; r < kTrTile; ++r) acc += s.dyf[r * 4 + o];
+            gB3 += acc;
+        }
+        if (!mlp_tr_wait(s, phase)) break;
+        {
+            float v[32];
+            tmem_ld32(trow + kTrColZ1 + (uint32_t)ch, v);
+#pragma unroll
+            for (int j = 0; j < 32; j += 2) {
+                const int u = ch + j;
+                v[j] *= g2[j];
+                v[j + 1] *= g2[j + 1];
+                const __nv_bfloat162 d = __floats2bfloat162_rn(v[j], v[j + 1]);
+                *reinterpret_cast<__nv_bfloat162*>(s.dz + canon_index(srow, u, 64)) = d;
+                s.dzt[canon_index(u, srow, kTrTile)] = d.x;
+                s.dzt[canon_index(u + 1, srow, kTrTile)] = d.y;
+            }
+            gB2 += warp_column_sums(v);
+        }
+        // dH1 = dZ2 W2 and dW2 += dZ2^T H1.
+        mlp_tr_publish();
+        if (tid == 0) {
+            mlp_tr_mma(tm + kTrColZ2, s.dz, s.w.w2t, 64, 64, false);
+            mlp_tr_mma(tm + kTrColDW2, s.dzt, s.h1t, 64, kTrTile, any);
+            umma_commit(&s.mbar);
+        }
+        if (!mlp_tr_wait(s, phase)) break;
+        {
+            float v[32];
+            tmem_ld32(trow + kTrColZ2 + (uint32_t)ch, v);
+#pragma unroll
+            for (int j = 0; j < 32; j += 2) {
+                const int u = ch + j;
+                v[j] *= g1[j];
+                v[j + 1] *= g1[j + 1];
+                const __nv_bfloat162 d = __floats2bfloat162_rn(v[j], v[j + 1]);
+                s.dzt[canon_index(u, srow, kTrTile)] = d.x;
+                s.dzt[canon_index(u + 1, srow, kTrTile)] = d.y;
+            }
+            gB1 += warp_column_sums(v);
+        }
+        // dW1 += dZ1^T X.
+        mlp_tr_publish();
+        if (tid == 0) {
+            mlp_tr_mma(tm + kTrColDW1, s.dzt, s.xt, 16, kTrTile, any);
+            umma_commit(&s.mbar);
+        }
+        if (!mlp_tr_wait(s, phase)) break;
+        any = true;
+    }
+    if (s.failed) {
+        if (tid == 0) atomicOr(status, kStatusTimeout);
+    } else if (any) {
+        if (wq < 2) {  // TMEM lanes 0..63: the hidden units
+            const int u = srow;
+            float v[32];
+            tmem_ld32(trow + kTrColDW2 + (uint32_t)ch, v);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) atomicAdd(grad + kPW2 + u * 64 + ch + j, v[j]);
+            if (ch == 0) {
+                float v16[16];
+                tmem_ld16(trow + kTrColDW1, v16);
+#pragma unroll
+                for (int i = 0; i < kMlpIn; ++i) atomicAdd(grad + kPW1 + u * kMlpIn + i, v16[i]);
+            }
+        }
+        atomicAdd(grad + kPB2 + ch + lane, gB2);
+        atomicAdd(grad + kPB1 + ch + lane, gB1);
+        if (tid < kMlpOut * 64) atomicAdd(grad + kPW3 + tid, gW3);
+        else if (tid < kMlpOut * 64 + kMlpOut) atomicAdd(grad + kPB3 + tid - kMlpOut * 64, gB3);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        if (lane == 0 && ch == 0) atomicAdd(loss, lsum * inv_count);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(kTrTmemCols) : "memory");
+}
+
 inline int blocks_of(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
@@ -457,6 +688,7 @@ struct mpm_corrector {
     float* io = nullptr;     // stand-alone inference staging
     long long io_cap = 0;
     int adam_t = 0;
+    int train_kind = MPM_TRAIN_TCGEN05;
     std::string last_error;
 };
 
@@ -561,6 +793,8 @@ mpm_status mpm_corrector_create(int32_t device, int64_t capacity, mpm_corrector*
     CA(cudaMemsetAsync(c->m2, 0, mpm::kPCount * sizeof(float), c->stream));
     CA(cudaFuncSetAttribute(mpm::mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)mpm::kTrainSmem));
+    CA(cudaFuncSetAttribute(mpm::mlp_train_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(mpm::MlpTrainSmem)));
     CA(cudaStreamSynchronize(c->stream));
 #undef CA
     *out = c;
@@ -685,17 +919,33 @@ mpm_status mpm_corrector_set_params(mpm_corrector* c, const float* params_host) 
 
 namespace {
 mpm_status launch_train(mpm_corrector* c, int batch, const long long* idx, unsigned long long seed, int step) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    if (c->train_kind == MPM_TRAIN_TCGEN05) {
+        const int tiles = (batch + mpm::kTrTile - 1) / mpm::kTrTile;
+        const int grid = std::max(1, std::min(tiles, sms));
+        mpm::mlp_train_tc_kernel<<<grid, mpm::kTrThreads, sizeof(mpm::MlpTrainSmem), c->stream>>>(
+            c->w, c->feat, c->targ, c->size, idx, batch, seed, step, c->grad, c->loss, c->status);
+        CC(c, cudaGetLastError());
+        return MPM_OK;
+    }
     const int tiles = batch / mpm::kTile;
     int per_sm = 0;
     CC(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mpm::mlp_train_kernel, mpm::kTrainThreads,
                                                          mpm::kTrainSmem));
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     const int grid = std::max(1, std::min(tiles, sms * std::max(per_sm, 1)));
     mpm::mlp_train_kernel<<<grid, mpm::kTrainThreads, mpm::kTrainSmem, c->stream>>>(
         c->w, c->feat, c->targ, c->size, idx, batch, seed, step, c->grad, c->loss);
     CC(c, cudaGetLastError());
     return MPM_OK;
+}
+
+// The status word the tcgen05 kernels set when a bounded wait gave up (read
+// back by the caller together with its results).
+mpm_status check_status(mpm_corrector* c, uint32_t flag) {
+    if (!flag) return MPM_OK;
+    c->last_error = "a bounded wait of a tcgen05 kernel gave up";
+    return MPM_ERR_TIMEOUT;
 }
 }  // namespace
 
@@ -707,6 +957,7 @@ mpm_status mpm_corrector_train(mpm_corrector* c, int32_t steps, int32_t batch, f
     if (c->size < 1) return cbad(c, "the dataset is empty");
     if (!(lr > 0.f)) return cbad(c, "lr must be positive");
     CC(c, cudaMemsetAsync(c->loss, 0, sizeof(float), c->stream));
+    CC(c, cudaMemsetAsync(c->status, 0, sizeof(uint32_t), c->stream));
     const float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
     const int ntrain = mpm::kPCount - mpm::kPTrainFirst;
     for (int i = 0; i < steps; ++i) {
@@ -720,10 +971,12 @@ mpm_status mpm_corrector_train(mpm_corrector* c, int32_t steps, int32_t batch, f
         CC(c, cudaGetLastError());
     }
     float loss = 0.f;
+    uint32_t flag = 0;
     CC(c, cudaMemcpyAsync(&loss, c->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CC(c, cudaMemcpyAsync(&flag, c->status, sizeof(flag), cudaMemcpyDeviceToHost, c->stream));
     CC(c, cudaStreamSynchronize(c->stream));
     if (mean_loss) *mean_loss = steps > 0 ? loss / (float)steps : 0.f;
-    return MPM_OK;
+    return check_status(c, flag);
 }
 
 mpm_status mpm_corrector_gradient(mpm_corrector* c, int64_t count, const int64_t* idx_host, float* grad_host,
@@ -743,13 +996,24 @@ mpm_status mpm_corrector_gradient(mpm_corrector* c, int64_t count, const int64_t
     CC(c, cudaMemcpyAsync(c->idx, idx_host, (size_t)count * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
     CC(c, cudaMemsetAsync(c->grad, 0, mpm::kPCount * sizeof(float), c->stream));
     CC(c, cudaMemsetAsync(c->loss, 0, sizeof(float), c->stream));
+    CC(c, cudaMemsetAsync(c->status, 0, sizeof(uint32_t), c->stream));
     st = launch_train(c, (int)count, c->idx, 0, 0);
     if (st != MPM_OK) return st;
     if (grad_host)
         CC(c, cudaMemcpyAsync(grad_host, c->grad, mpm::kPCount * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     if (loss_host) CC(c, cudaMemcpyAsync(loss_host, c->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    uint32_t flag = 0;
+    CC(c, cudaMemcpyAsync(&flag, c->status, sizeof(flag), cudaMemcpyDeviceToHost, c->stream));
     CC(c, cudaMemsetAsync(c->grad, 0, mpm::kPCount * sizeof(float), c->stream));
     CC(c, cudaStreamSynchronize(c->stream));
+    return check_status(c, flag);
+}
+
+mpm_status mpm_corrector_set_train_kernel(mpm_corrector* c, int32_t kind) {
+    mpm_status st = center(c);
+    if (st != MPM_OK) return st;
+    if (kind != MPM_TRAIN_TCGEN05 && kind != MPM_TRAIN_FP32) return cbad(c, "unknown training kernel");
+    c->train_kind = kind;
     return MPM_OK;
 }
 

@@ -222,6 +222,7 @@ def _load() -> ctypes.CDLL:
         "mpm_corrector_init": (I32, [P, ctypes.c_uint64]),
         "mpm_corrector_train": (I32, [P, I32, I32, ctypes.c_float, ctypes.c_uint64, P]),
         "mpm_corrector_gradient": (I32, [P, I64, P, P, P]),
+        "mpm_corrector_set_train_kernel": (I32, [P, I32]),
         "mpm_corrector_get_params": (I32, [P, P]),
         "mpm_corrector_set_params": (I32, [P, P]),
         "mpm_corrector_forward": (I32, [P, I64, P, P]),
@@ -608,6 +609,13 @@ class Corrector:
         loss = np.zeros(1, np.float32)
         self._check(lib.mpm_corrector_gradient(self._h, len(i), _ptr(i), _ptr(g), _ptr(loss)))
         return g, float(loss[0])
+
+    def set_train_kernel(self, kind: str):
+        """'tcgen05' (every GEMM on the 5th-generation tensor cores, the default) or 'fp32'."""
+        kinds = {"tcgen05": 0, "fp32": 1}
+        if kind not in kinds:
+            raise ValueError(f"unknown training kernel {kind!r}")
+        self._check(lib.mpm_corrector_set_train_kernel(self._h, kinds[kind]))
 
     def get_params(self) -> np.ndarray:
         w = np.empty(CORRECTOR_PARAMS, np.float32)
