@@ -103,6 +103,8 @@ struct mpm_engine {
     mpm::BinSet bins[2] = {};
     int32_t* bstart = nullptr;
     int32_t* cstart = nullptr;
+    int32_t* bpart = nullptr;  // chunk sums of the bin scan: scenes x scan_chunks
+    int scan_chunks = 1;
     uint32_t* ctl = nullptr;
     uint32_t* d_flags = nullptr;  // [0] health bits, [1] kernel status bits
 
@@ -289,7 +291,8 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
     mark(0);
     if (from <= MPM_STAGE_SORT && upto >= MPM_STAGE_SORT)
         launches += mpm::launch_bin_order(sc, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart, e->cstart,
-                                          e->pcell, e->prank, e->gidx, e->d_itemoff, work, st);
+                                          e->pcell, e->prank, e->gidx, e->d_itemoff, work, e->bpart,
+                                          e->scan_chunks, st);
     mark(1);
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
         launches += mpm::launch_p2g(sc, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par], e->d_itemoff,
@@ -556,6 +559,7 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
     e->cells_total = cells_total;
     e->bins_total = bins_total;
     e->bins_scan = bins_total - count;
+    for (const SimParams& p : prm) e->scan_chunks = std::max(e->scan_chunks, mpm::bin_scan_chunks(p.nb + 1));
 
     auto fail = [&](mpm_status s) {
         g_global_error = e->last_error;
@@ -577,6 +581,7 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
         (err = cudaMalloc(&e->ctl, (2 * count + 2) * sizeof(uint32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->bins_mem, bins_bytes(e))) != cudaSuccess ||
         (err = cudaMalloc(&e->bstart, (size_t)bins_total * sizeof(int32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->bpart, (size_t)count * e->scan_chunks * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->cstart, (size_t)cells_total * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->d_prm, count * sizeof(SimParams))) != cudaSuccess ||
         (err = cudaMalloc(&e->d_poff, (count + 1) * sizeof(long long))) != cudaSuccess ||
@@ -672,7 +677,8 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
     const SimParams big = large_params(e, 0);
     int launches = 0;
     launches += mpm::launch_bin_order(e->table, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart,
-                                      e->cstart, e->pcell, e->prank, e->gidx, e->d_itemoff, work, st);
+                                      e->cstart, e->pcell, e->prank, e->gidx, e->d_itemoff, work, e->bpart,
+                                          e->scan_chunks, st);
     launches += mpm::launch_p2g(e->table_large, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par],
                                 e->d_itemoff, work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
                                 e->tune.p2g_cell_cap);
@@ -758,6 +764,7 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->sdf);
     free_dev(e->bins_mem);
     free_dev(e->bstart);
+    free_dev(e->bpart);
     free_dev(e->cstart);
     free_dev(e->ctl);
     free_dev(e->d_prm);

@@ -70,10 +70,13 @@ int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t*
 // (first slot of every cell of a listed bin), gidx[new slot] = old slot, and
 // itemoff (the P2G work items of each scene: kBinZ per listed bin, prefix,
 // S + 1 entries); clears `other` and the work counters work[0..1].
-// bins_total: sum over scenes of nb + 1.
+// bins_total: sum over scenes of nb + 1.  bpart: scenes x scan_chunks ints of
+// scratch; scan_chunks = bin_scan_chunks(largest nb + 1).
 int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
                      int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
-                     long long* itemoff, uint32_t* work, cudaStream_t st);
+                     long long* itemoff, uint32_t* work, int32_t* bpart, int scan_chunks, cudaStream_t st);
+// Chunks of the bin scan for a scene of `bins` scanned bins.
+int bin_scan_chunks(long long bins);
 // P2G over the items of `cur`; gidx maps slots of the new order to P.
 // ctas_per_sm: persistent single-warp CTAs per SM (0 = the default 12);
 // cell_cap: particles of a cell its own lane sums before the cell is shared

@@ -453,84 +453,119 @@ __global__ void __launch_bounds__(256) bin_count_kernel(SceneTable sc, long long
     }
 }
 
-// One CTA per scene: bstart[i] = poff + sum of bcount[0..i) over the scene's
-// nbins = nb + 1 bins, bstart[nbins] = poff + its particle count (global
-// slots).  Also zeroes the scene's bin counters of the other set, and CTA 0
-// the P2G and G2P work counters.  In chunks of kScanChunk counters: coalesced
-// loads into shared memory, a contiguous run of kScanPer counters per thread,
-// a block scan of the run sums, coalesced stores.
-constexpr int kScanThreads = 1024;
+// Bin starts in two launches over (scene, chunk of kScanChunk bins) CTAs, no
+// CTA waiting on another: bin_sum_kernel writes each chunk's count sum to
+// bpart[scene * chunks + chunk]; bin_scan_kernel adds the sums of the
+// scene's earlier chunks to poff and scans its own chunk, so that
+// bstart[i] = poff + sum of bcount[0..i) over the scene's nbins = nb + 1
+// bins and bstart[nbins] = poff + its particle count (global slots).  The
+// scan also zeroes the chunk's bin counters of the other set, and CTA (0, 0)
+// the P2G and G2P work counters.  Per chunk: coalesced loads into shared
+// memory, a contiguous run of kScanPer counters per thread, a block scan of
+// the run sums, coalesced stores.
+constexpr int kScanThreads = 256;
+constexpr int kScanWarps = kScanThreads / 32;
 constexpr int kScanPer = 8;
 constexpr int kScanChunk = kScanThreads * kScanPer;
+
+// Sum of v over the CTA, returned to every thread (s_red: kScanWarps ints).
+__device__ __forceinline__ int scan_block_sum(int v, int* s_red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    int total = 0;
+#pragma unroll
+    for (int w = 0; w < kScanWarps; ++w) total += s_red[w];
+    return total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) bin_sum_kernel(SceneTable sc, const uint32_t* __restrict__ bcount_all,
+                                                               int32_t* __restrict__ bpart) {
+    __shared__ int s_red[kScanWarps];
+    const int scene = blockIdx.x, chunk = blockIdx.y;
+    const int nbins = sc.prm[scene].nb + 1;
+    const int c0 = chunk * kScanChunk;
+    if (c0 >= nbins) return;
+    const uint32_t* bcount = bcount_all + sc.prm[scene].boff + c0;
+    const int m = min(kScanChunk, nbins - c0);
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const int i = k * kScanThreads + threadIdx.x;
+        if (i < m) sum += (int)bcount[i];
+    }
+    sum = scan_block_sum(sum, s_red);
+    if (threadIdx.x == 0) bpart[(long long)scene * gridDim.y + chunk] = sum;
+}
+
 __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(SceneTable sc, const uint32_t* __restrict__ bcount_all,
                                                                 uint32_t* __restrict__ bclear_all,
+                                                                const int32_t* __restrict__ bpart,
                                                                 int32_t* __restrict__ bstart_all,
                                                                 uint32_t* __restrict__ work) {
     __shared__ int s_val[kScanChunk];
-    __shared__ int s_warp[kScanThreads / 32];
+    __shared__ int s_red[kScanWarps];
+    __shared__ int s_warp[kScanWarps];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const SimParams p = sc.prm[blockIdx.x];
-    const uint32_t* bcount = bcount_all + p.boff;
-    uint32_t* bclear = bclear_all + p.boff;
-    int32_t* bstart = bstart_all + p.boff;
+    const int scene = blockIdx.x, chunk = blockIdx.y;
+    if (scene == 0 && chunk == 0 && t == 0) {
+        work[0] = 0u;  // P2G items
+        work[1] = 0u;  // G2P items
+    }
+    const SimParams& p = sc.prm[scene];
     const int nbins = p.nb + 1;
-    int carry = (int)p.poff;
-    for (int c0 = 0; c0 < nbins; c0 += kScanChunk) {
-        const int m = min(kScanChunk, nbins - c0);
+    const int c0 = chunk * kScanChunk;
+    if (c0 >= nbins) return;
+    const long long boff = p.boff;
+    const uint32_t* bcount = bcount_all + boff + c0;
+    uint32_t* bclear = bclear_all + boff + c0;
+    int32_t* bstart = bstart_all + boff + c0;
+    const int m = min(kScanChunk, nbins - c0);
+    // Particles of the scene's earlier chunks.
+    int pre = 0;
+    for (int i = t; i < chunk; i += kScanThreads) pre += bpart[(long long)scene * gridDim.y + i];
 #pragma unroll
-        for (int k = 0; k < kScanPer; ++k) {
-            const int i = k * kScanThreads + t;
-            s_val[i] = i < m ? (int)bcount[c0 + i] : 0;
-            if (i < m) bclear[c0 + i] = 0u;
-        }
-        __syncthreads();
-        int v[kScanPer], sum = 0;
-#pragma unroll
-        for (int k = 0; k < kScanPer; ++k) {
-            v[k] = s_val[t * kScanPer + k];
-            sum += v[k];
-        }
-        int incl = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) s_warp[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            int w = s_warp[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += y;
-            }
-            s_warp[lane] = w;
-        }
-        __syncthreads();
-        int run = carry + incl - sum + (warp > 0 ? s_warp[warp - 1] : 0);
-#pragma unroll
-        for (int k = 0; k < kScanPer; ++k) {
-            s_val[t * kScanPer + k] = run;
-            run += v[k];
-        }
-        const int total = s_warp[31];
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < kScanPer; ++k) {
-            const int i = k * kScanThreads + t;
-            if (i < m) bstart[c0 + i] = s_val[i];
-        }
-        carry += total;
-        __syncthreads();
+    for (int k = 0; k < kScanPer; ++k) {
+        const int i = k * kScanThreads + t;
+        s_val[i] = i < m ? (int)bcount[i] : 0;
+        if (i < m) bclear[i] = 0u;
     }
-    if (t == 0) {
-        bstart[nbins] = carry;
-        if (blockIdx.x == 0) {
-            work[0] = 0u;  // P2G items
-            work[1] = 0u;  // G2P items
-        }
+    const int carry = (int)p.poff + scan_block_sum(pre, s_red);  // its barrier also publishes s_val
+    int v[kScanPer], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        v[k] = s_val[t * kScanPer + k];
+        sum += v[k];
     }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    int before = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kScanWarps; ++w) {
+        const int x = s_warp[w];
+        before += w < warp ? x : 0;
+        total += x;
+    }
+    int run = carry + before + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        s_val[t * kScanPer + k] = run;
+        run += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const int i = k * kScanThreads + t;
+        if (i < m) bstart[i] = s_val[i];
+    }
+    if (t == 0 && c0 + m == nbins) bstart[m] = carry + total;
 }
 
 // One warp per listed bin of each scene: cstart of its 128 cells = bstart of
@@ -999,16 +1034,20 @@ int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t*
     return 1;
 }
 
+int bin_scan_chunks(long long bins) { return (int)std::max(1LL, (bins + kScanChunk - 1) / kScanChunk); }
+
 int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
                      int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
-                     long long* itemoff, uint32_t* work, cudaStream_t st) {
+                     long long* itemoff, uint32_t* work, int32_t* bpart, int scan_chunks, cudaStream_t st) {
     if (n <= 0) return 0;
-    bin_scan_kernel<<<sc.count, kScanThreads, 0, st>>>(sc, cur.bcount, other.bcount, bstart, work);
+    const dim3 scan_grid((unsigned)sc.count, (unsigned)scan_chunks);
+    bin_sum_kernel<<<scan_grid, kScanThreads, 0, st>>>(sc, cur.bcount, bpart);
+    bin_scan_kernel<<<scan_grid, kScanThreads, 0, st>>>(sc, cur.bcount, other.bcount, bpart, bstart, work);
     const int ctas = (int)std::max(1LL, std::min((long long)blocks_for(bins_total * 32, 128), 148LL * 8));
     cell_scan_kernel<<<ctas, 128, 0, st>>>(sc, cur, bstart, cstart, other);
     bin_scatter_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, sc.count, pcell, prank, cstart, gidx, cur.nlist, itemoff,
                                                          other.nlist);
-    return 3;
+    return 4;
 }
 
 int p2g_max_ctas_per_sm() {
