@@ -19,7 +19,8 @@ Engine arm (default): `value` is device time (CUDA events on the engine's
 stream) of K frames with the state resident in HBM; `e2e` is the whole job
 through the C ABI with host buffers: upload of the scene from pinned memory
 (mpm_init_particles), then K x (mpm_step + positions read back to pinned
-memory), host wall time.  A second, instrumented pass records CUDA events
+memory), host wall time.  A second, instrumented pass of the same K frames,
+restarted from the state the timed frames started from, records CUDA events
 between the stages of every substep for the per-kernel roofline.  Rank 0 at
 N=1 also times the FP32 OpenMP CPU restatement on a bounded sample.
 Under torchrun each rank simulates an independent replica of the scene on its
@@ -304,6 +305,10 @@ def run_engine(args, rank, world, local):
     # does not advance the state).
     tuning = None if args.no_autotune else eng.autotune(3)
 
+    # The state the timed frames start from: the instrumented repeat below
+    # restarts from it, so that its stage times cover the same frames.
+    snap = [eng.scene_buffer(k) for k in range(len(cfgs))] if batched else eng.get_buffer()
+
     # Timed region: K frames, device time on the engine's stream.
     launches0 = eng.stats()["kernel_launches"]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -321,7 +326,13 @@ def run_engine(args, rank, world, local):
     ms = dist.max(e0.elapsed_time(e1))
     value = world * n * sub * args.steps / (ms / 1e3)
 
-    # Instrumented repeat: CUDA events between the stages of every substep.
+    # Instrumented repeat of the same K frames from the same starting state:
+    # CUDA events between the stages of every substep.
+    if batched:
+        eng.init_all(snap)
+    else:
+        eng.set_state(snap)
+    del snap
     eng.set_stage_timing(args.steps * sub)
     for _ in range(args.steps):
         eng.step_async(sub)
