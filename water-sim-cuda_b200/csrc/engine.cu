@@ -70,6 +70,7 @@ struct mpm_engine {
     long long* d_poff = nullptr;     // S + 1 first slots
     long long* d_goff = nullptr;     // S + 1 first nodes
     long long* d_itemoff = nullptr;  // S + 1 first P2G items
+    long long* d_clroff = nullptr;   // S + 1 first listed bins of the set being cleared
     mpm::SceneTable table{};
 
     bool initialized = false;
@@ -103,6 +104,7 @@ struct mpm_engine {
     mpm::BinSet bins[2] = {};
     int32_t* bstart = nullptr;
     int32_t* cstart = nullptr;
+    uint8_t* corder = nullptr;  // P2G's order of each listed bin's cells
     int32_t* bpart = nullptr;  // chunk sums of the bin scan: scenes x scan_chunks
     int scan_chunks = 1;
     uint32_t* ctl = nullptr;
@@ -291,11 +293,11 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
     mark(0);
     if (from <= MPM_STAGE_SORT && upto >= MPM_STAGE_SORT)
         launches += mpm::launch_bin_order(sc, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart, e->cstart,
-                                          e->pcell, e->prank, e->gidx, e->d_itemoff, work, e->bpart,
+                                          e->pcell, e->prank, e->gidx, e->corder, e->d_itemoff, e->d_clroff, work, e->bpart,
                                           e->scan_chunks, st);
     mark(1);
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
-        launches += mpm::launch_p2g(sc, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par], e->d_itemoff,
+        launches += mpm::launch_p2g(sc, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par], e->corder, e->d_itemoff,
                                     work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
                                     e->tune.p2g_cell_cap);
     mark(2);
@@ -583,10 +585,12 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
         (err = cudaMalloc(&e->bstart, (size_t)bins_total * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->bpart, (size_t)count * e->scan_chunks * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->cstart, (size_t)cells_total * sizeof(int32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->corder, (size_t)cells_total)) != cudaSuccess ||
         (err = cudaMalloc(&e->d_prm, count * sizeof(SimParams))) != cudaSuccess ||
         (err = cudaMalloc(&e->d_poff, (count + 1) * sizeof(long long))) != cudaSuccess ||
         (err = cudaMalloc(&e->d_goff, (count + 1) * sizeof(long long))) != cudaSuccess ||
-        (err = cudaMalloc(&e->d_itemoff, (count + 1) * sizeof(long long))) != cudaSuccess)
+        (err = cudaMalloc(&e->d_itemoff, (count + 1) * sizeof(long long))) != cudaSuccess ||
+        (err = cudaMalloc(&e->d_clroff, (count + 1) * sizeof(long long))) != cudaSuccess)
         return fail(cuda_fail(e, err, "cudaMalloc(grid)"));
     carve_bins(e);
     e->table.prm = e->d_prm;
@@ -677,10 +681,10 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
     const SimParams big = large_params(e, 0);
     int launches = 0;
     launches += mpm::launch_bin_order(e->table, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart,
-                                      e->cstart, e->pcell, e->prank, e->gidx, e->d_itemoff, work, e->bpart,
+                                      e->cstart, e->pcell, e->prank, e->gidx, e->corder, e->d_itemoff, e->d_clroff, work, e->bpart,
                                           e->scan_chunks, st);
     launches += mpm::launch_p2g(e->table_large, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par],
-                                e->d_itemoff, work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
+                                e->corder, e->d_itemoff, work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
                                 e->tune.p2g_cell_cap);
     launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, st,
                                         e->tune.grid_block);
@@ -765,12 +769,14 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->bins_mem);
     free_dev(e->bstart);
     free_dev(e->bpart);
+    free_dev(e->corder);
     free_dev(e->cstart);
     free_dev(e->ctl);
     free_dev(e->d_prm);
     free_dev(e->d_poff);
     free_dev(e->d_goff);
     free_dev(e->d_itemoff);
+    free_dev(e->d_clroff);
     free_dev(e->d_flags);
     free_dev(e->staging);
     free_dev(e->d_prm_large);

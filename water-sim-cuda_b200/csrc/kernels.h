@@ -67,14 +67,17 @@ struct BinSet {
 int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t* pcell, int32_t* prank,
                      const BinSet& set, cudaStream_t st);
 // Order by cell from set `cur`: bstart (global first slots of every bin), cstart
-// (first slot of every cell of a listed bin), gidx[new slot] = old slot, and
-// itemoff (the P2G work items of each scene: kBinZ per listed bin, prefix,
-// S + 1 entries); clears `other` and the work counters work[0..1].
+// (first slot of every cell of a listed bin), corder (P2G's order of each
+// listed bin's cells, one byte per cell, indexed like the cells), gidx[new
+// slot] = old slot, itemoff (the P2G work items of each scene: kBinZ per
+// listed bin, prefix, S + 1 entries) and clroff (the same prefix of `other`'s
+// listed bins, one per bin); clears `other` and the work counters work[0..1].
 // bins_total: sum over scenes of nb + 1.  bpart: scenes x scan_chunks ints of
 // scratch; scan_chunks = bin_scan_chunks(largest nb + 1).
 int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
                      int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
-                     long long* itemoff, uint32_t* work, int32_t* bpart, int scan_chunks, cudaStream_t st);
+                     uint8_t* corder, long long* itemoff, long long* clroff, uint32_t* work, int32_t* bpart,
+                     int scan_chunks, cudaStream_t st);
 // Chunks of the bin scan for a scene of `bins` scanned bins.
 int bin_scan_chunks(long long bins);
 // P2G over the items of `cur`; gidx maps slots of the new order to P.
@@ -82,8 +85,9 @@ int bin_scan_chunks(long long bins);
 // cell_cap: particles of a cell its own lane sums before the cell is shared
 // by the whole warp (0 = chosen per work item from its cells' counts).
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
-               const int32_t* cstart, const BinSet& cur, const long long* itemoff, uint32_t* work, float4* accum,
-               uint32_t* status, cudaStream_t st, int ctas_per_sm = 0, int cell_cap = 0);
+               const int32_t* cstart, const BinSet& cur, const uint8_t* corder, const long long* itemoff,
+               uint32_t* work, float4* accum, uint32_t* status, cudaStream_t st, int ctas_per_sm = 0,
+               int cell_cap = 0);
 // Most P2G CTAs that fit on one SM.
 int p2g_max_ctas_per_sm();
 // p0: the parameters of scene 0, used directly when the table holds one scene.

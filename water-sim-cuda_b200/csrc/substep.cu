@@ -110,29 +110,32 @@ struct SceneLookup {
 
 // ------------------------------------------------------------------ P2G ----
 // P2G (p2GTransferScatter, kernels.cu:6-142).  Persistent single-warp CTAs
-// take work items from a counter; an item is one z-layer (8 x 4 base cells)
-// of a bin that holds particles.  The cells of a layer are consecutive in the
-// particle order, so its particles are one slot range.  Lane = cell: all
-// particles of a cell scatter to the same 27 nodes, so the lane sums them in
-// registers, reading them through a ring of kRing particles fetched ahead with
-// 16-byte cp.async copies (the gather through gidx costs no registers).  The
-// lane then adds its 27 sums to the warp's footprint, the layer's 10 x 6 x 3
-// nodes in shared memory: the 32 cells of a layer are distinct, so for one
-// stencil offset the 32 nodes differ and a plain read-add-write per offset is
-// race-free.  A lane sums at most `cap` particles of its cell (a launch
-// parameter; 0 = chosen per work item by item_cap); the rest of
-// a crowded cell (this Tait law resists only expansion, so compressed fluid
+// take work items from a counter; a listed bin (8 x 4 x 4 base cells) has
+// kBinZ items, and item g takes positions 32 g .. 32 g + 31 of the bin's cell
+// order (cell_order: occupied cells by count class, largest first), so the
+// lanes of a warp hold cells of similar counts and no empty ones.  Lane =
+// cell: all particles of a cell scatter to the same 27 nodes, so the lane sums
+// them in registers, reading them through a ring of kRing particles fetched
+// ahead with 16-byte cp.async copies (the gather through gidx costs no
+// registers).  The lane then adds its 27 sums to the warp's footprint, the
+// bin's 10 x 6 x 6 nodes in shared memory: the lanes' cells are distinct, so
+// for one stencil offset their nodes differ and a plain read-add-write per
+// offset is race-free.  A lane sums at most `cap` particles of its cell (a
+// launch parameter; 0 = chosen per work item by item_cap); the rest of a
+// crowded cell (this Tait law resists only expansion, so compressed fluid
 // piles up) is shared by all 32 lanes and reduced across the warp.  The
-// footprint goes to global memory with one vector reduction per touched
-// node.  Unlike the reference, no partial sum is dropped (it drops
-// shared-tile cells whose partial mass is <= 1e-9, kernels.cu:132).
+// footprint's z-planes that the item reached go to global memory with one
+// vector reduction per touched node.  Unlike the reference, no partial sum
+// is dropped (it drops shared-tile cells whose partial mass is <= 1e-9,
+// kernels.cu:132).
 constexpr int kP2GWarpsPerSM = 12;
 constexpr int kRing = 2;
-constexpr int kGidxStage = 256;   // gather indices of a layer staged in shared memory
+constexpr int kGidxStage = 256;   // gather indices of a bin staged in shared memory
 constexpr int kCellCap = 12;      // particles of a cell its own lane sums; the rest: whole warp
 constexpr int kTX = kBinX + 2, kTY = kBinY + 2;
-constexpr int kFootNodes = kTX * kTY * 3;  // 180: one layer's stencil footprint
-static_assert(kBinX * kBinY == 32, "one warp covers one z-layer of a bin");
+constexpr int kFootPlane = kTX * kTY;              // 60 nodes of one z-plane
+constexpr int kFootNodes = kFootPlane * (kBinZ + 2);  // 360: a bin's stencil footprint
+static_assert(kBinX * kBinY == 32 && kBinZ == 4, "a bin is 128 cells: four items of 32");
 
 // Spline weights of nodes 0, 1, 2 of one axis at fractional offset f = pos -
 // base, times m.  For f in [0.5, 1.5) (every particle at pos >= 0.5) the
@@ -247,7 +250,7 @@ __device__ __forceinline__ int item_cap(int full) {
     int best = kCellCap;
     float best_cost = 1e30f;
 #pragma unroll
-    for (int cand : {8, 12, 16, 24, 32, 48, 64}) {
+    for (int cand : {8, 12, 16, 24, 32, 48, 64, 96, 128}) {
         const int over = full > cand ? (full - cand + 31) / 32 : 0;
         const int passes = (int)__reduce_add_sync(0xffffffffu, (unsigned)over);
         const int cells = __popc(__ballot_sync(0xffffffffu, full > cand));
@@ -260,6 +263,7 @@ __device__ __forceinline__ int item_cap(int full) {
 __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, const float* __restrict__ P,
                                                                   const int32_t* __restrict__ gidx,
                                                                   const int32_t* __restrict__ cstart, BinSet set,
+                                                                  const uint8_t* __restrict__ corder,
                                                                   const long long* __restrict__ itemoff,
                                                                   uint32_t* __restrict__ work,
                                                                   float4* __restrict__ accum_all,
@@ -279,18 +283,22 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
         const int scene = sc.count == 1 ? 0 : scene_of(itemoff, sc.count, item);
         const SimParams p = sc.prm[scene];
         const int local = item - (int)__ldg(itemoff + scene);
-        const int bin = __ldg(set.blist + p.boff + local / kBinZ), layer = local % kBinZ;
+        const int bin = __ldg(set.blist + p.boff + local / kBinZ), group = local % kBinZ;
         if (bin >= p.nb) continue;  // the overflow bin reaches no node
         float4* accum = accum_all + p.goff;
         const int bxi = bin % p.nbx, byi = (bin / p.nbx) % p.nby, bzi = bin / (p.nbx * p.nby);
-        // Node origin of the footprint = base cell of lane 0 of this layer.
-        const int ox = bxi * kBinX - 2, oy = byi * kBinY - 2, oz = bzi * kBinZ - 2 + layer;
-        const int cell = (int)p.coff + bin * kBinCells + layer * 32 + lane;
-        const int cs = __ldg(cstart + cell);
-        const int full = (int)__ldg(set.ccount + cell);
-        const int l0 = __shfl_sync(0xffffffffu, cs, 0);
-        const int l1 = __shfl_sync(0xffffffffu, cs + full, 31);
-        if (l1 == l0) continue;
+        // Node origin of the footprint = base cell of the bin's first cell.
+        const int ox = bxi * kBinX - 2, oy = byi * kBinY - 2, oz = bzi * kBinZ - 2;
+        const size_t cb = (size_t)p.coff + (size_t)bin * kBinCells;
+        // This lane's cell (z * 32 + y * 8 + x in the bin), 0xFF for none.
+        const int tcell = __ldg(corder + cb + group * 32 + lane);
+        if (__ballot_sync(0xffffffffu, tcell != 0xFF) == 0u) continue;
+        const bool own = tcell != 0xFF;
+        const int cs = own ? __ldg(cstart + cb + tcell) : 0;
+        const int full = own ? (int)__ldg(set.ccount + cb + tcell) : 0;
+        // The bin's slots (its cells are consecutive in the particle order).
+        const int l0 = __ldg(cstart + cb);
+        const int l1 = __ldg(cstart + cb + kBinCells - 1) + (int)__ldg(set.ccount + cb + kBinCells - 1);
         const bool staged = l1 - l0 <= kGidxStage;
         if (staged)
             for (int q = lane; q < l1 - l0; q += 32) s_gidx[q] = __ldg(gidx + l0 + q);
@@ -301,7 +309,7 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
         // serves both; only the flush differs.
         const int icap = cap > 0 ? cap : item_cap(full);
         uint32_t crowded = __ballot_sync(0xffffffffu, full > icap);
-        int first = cs, step = 1, cnt = min(full, icap), target = lane;
+        int first = cs, step = 1, cnt = min(full, icap), target = tcell;
         for (;;) {
             float am[27], ax[27], ay[27], az[27];
             int maxc = cnt;
@@ -339,7 +347,8 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
                                                        s_ring[sl][3][lane], s_ring[sl][4][lane], s_ring[sl][5][lane]);
                     // Filed under a cell of this layer by construction; a
                     // mismatch is recorded, never scattered to a wrong node.
-                    if (r.bx - ox != target % kBinX || r.by - oy != target / kBinX || r.bz != oz) {
+                    if (r.bx - ox != target % kBinX || r.by - oy != (target / kBinX) % kBinY ||
+                        r.bz - oz != target / 32) {
                         atomicOr(status, kStatusBinning);
                     } else {
                         p2g_stencil(r, [&](int k, int, int, int, float m, float mx, float my, float mz) {
@@ -355,7 +364,7 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
             cp_async_wait<0>();
             if (step == 1) {
                 // One lane per cell: distinct nodes for each stencil offset.
-                const int tx = lane % kBinX, ty = lane / kBinX;
+                const int tx = tcell % kBinX, ty = (tcell / kBinX) % kBinY, tz = (tcell / 32) & (kBinZ - 1);
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -363,14 +372,16 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
 #pragma unroll
                         for (int a = 0; a < 3; ++a) {
                             const int k = (c * 3 + b) * 3 + a;
-                            float4* d = &s_foot[(c * kTY + ty + b) * kTX + tx + a];
+                            float4* d = &s_foot[((tz + c) * kTY + ty + b) * kTX + tx + a];
                             __syncwarp();
-                            float4 v = *d;
-                            v.x += am[k];
-                            v.y += ax[k];
-                            v.z += ay[k];
-                            v.w += az[k];
-                            *d = v;
+                            if (own) {
+                                float4 v = *d;
+                                v.x += am[k];
+                                v.y += ax[k];
+                                v.z += ay[k];
+                                v.w += az[k];
+                                *d = v;
+                            }
                         }
             } else {
                 // A crowded cell's pass: reduce-scatter the 32 lanes' partial
@@ -396,8 +407,8 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
                 }
                 if (lane < 27) {
                     const int a = lane % 3, b = (lane / 3) % 3, c = lane / 9;
-                    const int tx = target % kBinX, ty = target / kBinX;
-                    float4* d = &s_foot[(c * kTY + ty + b) * kTX + tx + a];
+                    const int tx = target % kBinX, ty = (target / kBinX) % kBinY, tz = target / 32;
+                    float4* d = &s_foot[((tz + c) * kTY + ty + b) * kTX + tx + a];
                     float4 u = *d;
                     u.x += v[0];
                     u.y += v[1];
@@ -414,11 +425,14 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
             first = __shfl_sync(0xffffffffu, cs, src) + icap + lane;
             step = 32;
             cnt = max(0, (hcnt - icap - lane + 31) / 32);
-            target = src;
+            target = __shfl_sync(0xffffffffu, tcell, src);
         }
         __syncwarp();
-        for (int q = lane; q < kFootNodes; q += 32) {
-            const int x = ox + q % kTX, y = oy + (q / kTX) % kTY, z = oz + q / (kTX * kTY);
+        // The z-planes the group's cells reach: zmin .. zmax + 2.
+        const int zmin = (int)__reduce_min_sync(0xffffffffu, own ? (unsigned)(tcell / 32) : 0xFFu);
+        const int zmax = (int)__reduce_max_sync(0xffffffffu, own ? (unsigned)(tcell / 32) : 0u);
+        for (int q = zmin * kFootPlane + lane; q < (zmax + 3) * kFootPlane; q += 32) {
+            const int x = ox + q % kTX, y = oy + (q / kTX) % kTY, z = oz + q / kFootPlane;
             const float4 v = s_foot[q];
             s_foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (node_in_grid(p, x, y, z) && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))  // NaN counts
@@ -460,7 +474,9 @@ __global__ void __launch_bounds__(256) bin_count_kernel(SceneTable sc, long long
 // bstart[i] = poff + sum of bcount[0..i) over the scene's nbins = nb + 1
 // bins and bstart[nbins] = poff + its particle count (global slots).  The
 // scan also zeroes the chunk's bin counters of the other set, and CTA (0, 0)
-// the P2G and G2P work counters.  Per chunk: coalesced loads into shared
+// the P2G and G2P work counters and writes the per-scene prefixes of the
+// listed bins (itemoff, in P2G items, for the current set; clroff for the set
+// to clear).  Per chunk: coalesced loads into shared
 // memory, a contiguous run of kScanPer counters per thread, a block scan of
 // the run sums, coalesced stores.
 constexpr int kScanThreads = 256;
@@ -503,7 +519,11 @@ __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(SceneTable sc, c
                                                                 uint32_t* __restrict__ bclear_all,
                                                                 const int32_t* __restrict__ bpart,
                                                                 int32_t* __restrict__ bstart_all,
-                                                                uint32_t* __restrict__ work) {
+                                                                uint32_t* __restrict__ work,
+                                                                const uint32_t* __restrict__ cur_nlist,
+                                                                const uint32_t* __restrict__ clear_nlist,
+                                                                long long* __restrict__ itemoff,
+                                                                long long* __restrict__ clroff) {
     __shared__ int s_val[kScanChunk];
     __shared__ int s_red[kScanWarps];
     __shared__ int s_warp[kScanWarps];
@@ -512,6 +532,17 @@ __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(SceneTable sc, c
     if (scene == 0 && chunk == 0 && t == 0) {
         work[0] = 0u;  // P2G items
         work[1] = 0u;  // G2P items
+        // Per-scene prefixes: P2G items (kBinZ per listed bin of the current
+        // set) and the listed bins of the set to clear.
+        long long run = 0, runc = 0;
+        for (int s2 = 0; s2 < sc.count; ++s2) {
+            itemoff[s2] = run;
+            clroff[s2] = runc;
+            run += (long long)cur_nlist[s2] * kBinZ;
+            runc += (long long)clear_nlist[s2];
+        }
+        itemoff[sc.count] = run;
+        clroff[sc.count] = runc;
     }
     const SimParams& p = sc.prm[scene];
     const int nbins = p.nb + 1;
@@ -568,66 +599,109 @@ __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(SceneTable sc, c
     if (t == 0 && c0 + m == nbins) bstart[m] = carry + total;
 }
 
+// The P2G order of a bin's cells (one warp; lane holds the counts of cells
+// 4 lane .. 4 lane + 3): occupied cells by count class (floor(log2 count),
+// 7 for 128 and more), largest class first, by cell index within a class;
+// order[p] = the cell at position p, 0xFF past the occupied cells.  P2G's
+// item g of the bin takes positions 32 g .. 32 g + 31, so a warp's lanes hold
+// cells of similar counts.  Class counts travel as the bytes of two words
+// (classes 0..3 and 4..7; a byte holds at most 128): one warp scan gives the
+// cells of each class in lower lanes, and multiplying the totals by
+// 0x01010101 gives byte-wise running sums, hence each class's first position.
+__device__ __forceinline__ void cell_order(uint4 c, uint8_t* __restrict__ order) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t cnt[4] = {c.x, c.y, c.z, c.w};
+    int cls[4];
+    uint32_t lo = 0u, hi = 0u;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        cls[j] = cnt[j] == 0u ? -1 : min(7, 31 - __clz((int)cnt[j]));
+        const uint32_t one = cls[j] < 0 ? 0u : 1u << (8 * (cls[j] & 3));
+        if (cls[j] < 4) lo += one;
+        else hi += one;
+    }
+    uint32_t ilo = lo, ihi = hi;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t a = __shfl_up_sync(0xffffffffu, ilo, o), b = __shfl_up_sync(0xffffffffu, ihi, o);
+        if (lane >= o) ilo += a, ihi += b;
+    }
+    const uint32_t clo = __shfl_sync(0xffffffffu, ilo, 31) * 0x01010101u;  // byte k: cells of classes <= k
+    const uint32_t chi = __shfl_sync(0xffffffffu, ihi, 31) * 0x01010101u + (clo >> 24) * 0x01010101u;
+    const int total = (int)(chi >> 24);
+    uint32_t seen_lo = ilo - lo, seen_hi = ihi - hi;  // cells of each class in lower lanes, then earlier here
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (cls[j] < 0) continue;
+        const int sh = 8 * (cls[j] & 3);
+        const bool h = cls[j] >= 4;
+        const int upto = (int)(((h ? chi : clo) >> sh) & 0xFFu);  // cells of classes <= cls
+        const int ex = (int)(((h ? seen_hi : seen_lo) >> sh) & 0xFFu);
+        // First position of the class = cells of larger classes = total - upto.
+        order[total - upto + ex] = (uint8_t)(4 * lane + j);
+        if (h) seen_hi += 1u << sh;
+        else seen_lo += 1u << sh;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (4 * lane + j >= total) order[4 * lane + j] = 0xFFu;
+}
+
 // One warp per listed bin of each scene: cstart of its 128 cells = bstart of
 // the bin + the exclusive scan of their counts.  Then clears the cell
 // counters of the other set for the bins on that set's lists (the cells it
 // last filled).
 __global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet set, const int32_t* __restrict__ bstart,
-                                                        int32_t* __restrict__ cstart, BinSet clear) {
+                                                        int32_t* __restrict__ cstart, uint8_t* __restrict__ corder,
+                                                        BinSet clear, const long long* __restrict__ itemoff,
+                                                        const long long* __restrict__ clroff) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int scene = 0; scene < sc.count; ++scene) {
+    // Listed bins of all scenes, one after another (itemoff counts kBinZ items per bin).
+    const long long nbins = itemoff[sc.count] / kBinZ;
+    for (long long it = gw; it < nbins; it += nw) {
+        const int scene = sc.count == 1 ? 0 : scene_of(itemoff, sc.count, it * kBinZ);
         const long long coff = sc.prm[scene].coff, boff = sc.prm[scene].boff;
-        const int nlist = (int)set.nlist[scene];
-        for (int item = gw; item < nlist; item += nw) {
-            const int bin = set.blist[boff + item];
-            const size_t c0 = (size_t)coff + (size_t)bin * kBinCells + lane * 4;
-            const uint4 c = *reinterpret_cast<const uint4*>(set.ccount + c0);
-            const int sum = (int)(c.x + c.y + c.z + c.w);
-            int incl = sum;
+        const int bin = set.blist[boff + it - itemoff[scene] / kBinZ];
+        const size_t c0 = (size_t)coff + (size_t)bin * kBinCells + lane * 4;
+        const uint4 c = *reinterpret_cast<const uint4*>(set.ccount + c0);
+        const int sum = (int)(c.x + c.y + c.z + c.w);
+        int incl = sum;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const int e0 = bstart[boff + bin] + incl - sum;
-            int4 st;
-            st.x = e0;
-            st.y = e0 + (int)c.x;
-            st.z = st.y + (int)c.y;
-            st.w = st.z + (int)c.z;
-            *reinterpret_cast<int4*>(cstart + c0) = st;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
         }
-        const int nclear = (int)clear.nlist[scene];
-        for (int item = gw; item < nclear; item += nw) {
-            const int bin = clear.blist[boff + item];
-            *reinterpret_cast<uint4*>(clear.ccount + (size_t)coff + (size_t)bin * kBinCells + lane * 4) =
-                make_uint4(0u, 0u, 0u, 0u);
-        }
+        const int e0 = bstart[boff + bin] + incl - sum;
+        int4 st;
+        st.x = e0;
+        st.y = e0 + (int)c.x;
+        st.z = st.y + (int)c.y;
+        st.w = st.z + (int)c.z;
+        *reinterpret_cast<int4*>(cstart + c0) = st;
+        cell_order(c, corder + (size_t)coff + (size_t)bin * kBinCells);
+    }
+    const long long nclear = clroff[sc.count];
+    for (long long it = gw; it < nclear; it += nw) {
+        const int scene = sc.count == 1 ? 0 : scene_of(clroff, sc.count, it);
+        const long long coff = sc.prm[scene].coff, boff = sc.prm[scene].boff;
+        const int bin = clear.blist[boff + it - clroff[scene]];
+        *reinterpret_cast<uint4*>(clear.ccount + (size_t)coff + (size_t)bin * kBinCells + lane * 4) =
+            make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
 // gidx[cstart[cell[j]] + rank[j]] = j: the order by cell.  Thread 0 also
-// writes the P2G item offsets (kBinZ items per listed bin, scene after
-// scene) and resets the other set's lists, which cell_scan_kernel has just
-// cleared.
+// resets the other set's lists, which cell_scan_kernel has just cleared.
 __global__ void __launch_bounds__(256) bin_scatter_kernel(long long n, int scenes, const int32_t* __restrict__ pcell,
                                                           const int32_t* __restrict__ prank,
                                                           const int32_t* __restrict__ cstart,
-                                                          int32_t* __restrict__ gidx, const uint32_t* __restrict__ cur_nlist,
-                                                          long long* __restrict__ itemoff,
+                                                          int32_t* __restrict__ gidx,
                                                           uint32_t* __restrict__ clear_nlist) {
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (j == 0) {
-        long long run = 0;
-        for (int s2 = 0; s2 < scenes; ++s2) {
-            itemoff[s2] = run;
-            run += (long long)cur_nlist[s2] * kBinZ;
-            clear_nlist[s2] = 0u;
-        }
-        itemoff[scenes] = run;
-    }
+    if (j == 0)
+        for (int s2 = 0; s2 < scenes; ++s2) clear_nlist[s2] = 0u;
     if (j >= n) return;
     gidx[__ldg(cstart + __ldg(pcell + j)) + __ldg(prank + j)] = (int32_t)j;
 }
@@ -1038,15 +1112,16 @@ int bin_scan_chunks(long long bins) { return (int)std::max(1LL, (bins + kScanChu
 
 int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
                      int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
-                     long long* itemoff, uint32_t* work, int32_t* bpart, int scan_chunks, cudaStream_t st) {
+                     uint8_t* corder, long long* itemoff, long long* clroff, uint32_t* work, int32_t* bpart,
+                     int scan_chunks, cudaStream_t st) {
     if (n <= 0) return 0;
     const dim3 scan_grid((unsigned)sc.count, (unsigned)scan_chunks);
     bin_sum_kernel<<<scan_grid, kScanThreads, 0, st>>>(sc, cur.bcount, bpart);
-    bin_scan_kernel<<<scan_grid, kScanThreads, 0, st>>>(sc, cur.bcount, other.bcount, bpart, bstart, work);
+    bin_scan_kernel<<<scan_grid, kScanThreads, 0, st>>>(sc, cur.bcount, other.bcount, bpart, bstart, work, cur.nlist,
+                                                       other.nlist, itemoff, clroff);
     const int ctas = (int)std::max(1LL, std::min((long long)blocks_for(bins_total * 32, 128), 148LL * 8));
-    cell_scan_kernel<<<ctas, 128, 0, st>>>(sc, cur, bstart, cstart, other);
-    bin_scatter_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, sc.count, pcell, prank, cstart, gidx, cur.nlist, itemoff,
-                                                         other.nlist);
+    cell_scan_kernel<<<ctas, 128, 0, st>>>(sc, cur, bstart, cstart, corder, other, itemoff, clroff);
+    bin_scatter_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, sc.count, pcell, prank, cstart, gidx, other.nlist);
     return 4;
 }
 
@@ -1060,13 +1135,13 @@ int p2g_max_ctas_per_sm() {
 }
 
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
-               const int32_t* cstart, const BinSet& cur, const long long* itemoff, uint32_t* work, float4* accum,
-               uint32_t* status, cudaStream_t st, int ctas_per_sm, int cell_cap) {
+               const int32_t* cstart, const BinSet& cur, const uint8_t* corder, const long long* itemoff,
+               uint32_t* work, float4* accum, uint32_t* status, cudaStream_t st, int ctas_per_sm, int cell_cap) {
     if (n <= 0) return 0;
     const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : kP2GWarpsPerSM;
     const int cap = cell_cap > 0 ? cell_cap : 0;
     const int warps = (int)std::min(bins_total * kBinZ, 148LL * per_sm);
-    p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, itemoff, work, accum, status, cap);
+    p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, corder, itemoff, work, accum, status, cap);
     return 1;
 }
 
