@@ -79,6 +79,8 @@ struct mpm_engine {
     float* P[2] = {nullptr, nullptr};        // particle-major state, 24 floats per particle
     int32_t* sigma[2] = {nullptr, nullptr};  // slot -> original slot (global)
     int32_t* gidx = nullptr;                 // new slot -> old slot of the current binning
+    int4* crowd = nullptr;                   // P2G's crowded-cell list
+    int crowd_cap = 0;
     int32_t* pcell = nullptr;                // global cell of each slot of P[parity]
     int32_t* prank = nullptr;                // rank within its cell
     int32_t* ref_keys = nullptr;             // mpm_get_sort: keys in original order (one scene)
@@ -99,7 +101,8 @@ struct mpm_engine {
     float* sdf = nullptr;
     // Binning: two counter sets (cell counts, bin counts, bin lists) in one
     // allocation, the bin and cell starts of the current order, and ctl =
-    // {list lengths of set 0 (S), of set 1 (S), P2G work, G2P work}.
+    // {list lengths of set 0 (S), of set 1 (S), P2G work, G2P work, crowded-cell
+    // list length, crowded-cell entries taken}.
     void* bins_mem = nullptr;
     mpm::BinSet bins[2] = {};
     int32_t* bstart = nullptr;
@@ -199,6 +202,7 @@ void free_particles(mpm_engine* e) {
         e->graph_kernels[k] = 0;
     }
     free_dev(e->gidx);
+    free_dev(e->crowd);
     free_dev(e->pcell);
     free_dev(e->prank);
     free_dev(e->ref_keys);
@@ -232,6 +236,10 @@ mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_by
         CK(e, cudaMalloc(&e->sigma[k], ibytes));
     }
     CK(e, cudaMalloc(&e->gidx, ibytes));
+    // A crowded-cell entry holds at least one particle beyond a cap of 8 or
+    // more, and a cell yields one entry per 256 of them: fewer than n / 8.
+    e->crowd_cap = (int)std::min<long long>(cap / 8 + 64, 0x7fffffffLL);
+    CK(e, cudaMalloc(&e->crowd, (size_t)e->crowd_cap * sizeof(int4)));
     CK(e, cudaMalloc(&e->pcell, ibytes));
     CK(e, cudaMalloc(&e->prank, ibytes));
     const size_t sbytes = (size_t)std::max(max_n, 1) * sizeof(int32_t);
@@ -298,7 +306,7 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
     mark(1);
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
         launches += mpm::launch_p2g(sc, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par], e->corder, e->d_itemoff,
-                                    work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
+                                    work, e->accum, e->crowd, e->crowd_cap, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
                                     e->tune.p2g_cell_cap);
     mark(2);
     if (from <= MPM_STAGE_GRID && upto >= MPM_STAGE_GRID)
@@ -375,10 +383,12 @@ mpm_status sync_and_collect(mpm_engine* e) {
     CK(e, cudaMemcpyAsync(flags, e->d_flags, sizeof(flags), cudaMemcpyDeviceToHost, e->stream));
     CK(e, cudaStreamSynchronize(e->stream));
     e->health |= flags[0];
-    if (flags[1] & (mpm::kStatusTimeout | mpm::kStatusBinning)) {
+    if (flags[1] & (mpm::kStatusTimeout | mpm::kStatusBinning | mpm::kStatusCrowdList)) {
         CK(e, cudaMemsetAsync(e->d_flags + 1, 0, sizeof(uint32_t), e->stream));
         if (flags[1] & mpm::kStatusBinning)
             return record(e, MPM_ERR_CUDA, "internal error: a particle was not in the cell it was filed under");
+        if (flags[1] & mpm::kStatusCrowdList)
+            return record(e, MPM_ERR_CUDA, "internal error: the crowded-cell list of P2G overflowed");
         return record(e, MPM_ERR_TIMEOUT, "a bounded device-side wait gave up");
     }
     return MPM_OK;
@@ -416,7 +426,7 @@ mpm_status load_states(mpm_engine* e, const float* const* soa26_host, bool init_
     }
     // Both counter sets empty, then the imported particles filed into set 0.
     CK(e, cudaMemsetAsync(e->bins_mem, 0, bins_bytes(e), e->stream));
-    CK(e, cudaMemsetAsync(e->ctl, 0, (2 * e->scenes + 2) * sizeof(uint32_t), e->stream));
+    CK(e, cudaMemsetAsync(e->ctl, 0, (2 * e->scenes + 4) * sizeof(uint32_t), e->stream));
     e->kernel_launches += mpm::launch_bin_count(e->table, e->n, e->P[0], e->pcell, e->prank, e->bins[0], e->stream);
     CK(e, cudaGetLastError());
     e->parity = 0;
@@ -580,7 +590,7 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
         (err = cudaMalloc(&e->vgrid, (size_t)g_total * sizeof(float4))) != cudaSuccess ||
         (err = cudaMalloc(&e->sdf, (size_t)g_total * sizeof(float))) != cudaSuccess ||
         (err = cudaMalloc(&e->d_flags, 2 * sizeof(uint32_t))) != cudaSuccess ||
-        (err = cudaMalloc(&e->ctl, (2 * count + 2) * sizeof(uint32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->ctl, (2 * count + 4) * sizeof(uint32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->bins_mem, bins_bytes(e))) != cudaSuccess ||
         (err = cudaMalloc(&e->bstart, (size_t)bins_total * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->bpart, (size_t)count * e->scan_chunks * sizeof(int32_t))) != cudaSuccess ||
@@ -684,7 +694,7 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
                                       e->cstart, e->pcell, e->prank, e->gidx, e->corder, e->d_itemoff, e->d_clroff, work, e->bpart,
                                           e->scan_chunks, st);
     launches += mpm::launch_p2g(e->table_large, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par],
-                                e->corder, e->d_itemoff, work, e->accum, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
+                                e->corder, e->d_itemoff, work, e->accum, e->crowd, e->crowd_cap, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
                                 e->tune.p2g_cell_cap);
     launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, st,
                                         e->tune.grid_block);
@@ -698,7 +708,7 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
 // emptied first): the state of parity `par` becomes the current one again.
 mpm_status rebin(mpm_engine* e, int par) {
     CK(e, cudaMemsetAsync(e->bins_mem, 0, bins_bytes(e), e->stream));
-    CK(e, cudaMemsetAsync(e->ctl, 0, (2 * e->scenes + 2) * sizeof(uint32_t), e->stream));
+    CK(e, cudaMemsetAsync(e->ctl, 0, (2 * e->scenes + 4) * sizeof(uint32_t), e->stream));
     e->kernel_launches += mpm::launch_bin_count(e->table, e->n, e->P[par], e->pcell, e->prank, e->bins[par], e->stream);
     CK(e, cudaGetLastError());
     e->parity = par;

@@ -80,14 +80,16 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
                      int scan_chunks, cudaStream_t st);
 // Chunks of the bin scan for a scene of `bins` scanned bins.
 int bin_scan_chunks(long long bins);
-// P2G over the items of `cur`; gidx maps slots of the new order to P.
-// ctas_per_sm: persistent single-warp CTAs per SM (0 = the default 12);
-// cell_cap: particles of a cell its own lane sums before the cell is shared
-// by the whole warp (0 = chosen per work item from its cells' counts).
+// P2G over the items of `cur`; gidx maps slots of the new order to P.  Two
+// launches: the items, then the crowded-cell list they fill (crowd: scratch of
+// crowd_cap entries, at least n / 8 + 64; work[2..3] are its counters, reset
+// by the bin scan).  ctas_per_sm: persistent single-warp CTAs per SM (0 = the
+// default 12); cell_cap: particles of a cell its own lane sums before the rest
+// goes to the list (0 = chosen per work item from its cells' counts).
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
                const int32_t* cstart, const BinSet& cur, const uint8_t* corder, const long long* itemoff,
-               uint32_t* work, float4* accum, uint32_t* status, cudaStream_t st, int ctas_per_sm = 0,
-               int cell_cap = 0);
+               uint32_t* work, float4* accum, int4* crowd, int crowd_cap, uint32_t* status, cudaStream_t st,
+               int ctas_per_sm = 0, int cell_cap = 0);
 // Most P2G CTAs that fit on one SM.
 int p2g_max_ctas_per_sm();
 // p0: the parameters of scene 0, used directly when the table holds one scene.
@@ -145,7 +147,8 @@ int launch_identity(int32_t* dst, int n, cudaStream_t st);
 // Device status bits written by kernels with bounded waits.
 enum : uint32_t {
     kStatusTimeout = 1u << 0,  // a bounded wait gave up
-    kStatusBinning = 1u << 1   // P2G met a particle outside the cell it was filed under
+    kStatusBinning = 1u << 1,  // P2G met a particle outside the cell it was filed under
+    kStatusCrowdList = 1u << 2 // the crowded-cell list of P2G overflowed
 };
 
 // Sets the thread's mpm_global_last_error text (engine.cu).

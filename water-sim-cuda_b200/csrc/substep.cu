@@ -123,15 +123,19 @@ struct SceneLookup {
 // offset is race-free.  A lane sums at most `cap` particles of its cell (a
 // launch parameter; 0 = chosen per work item by item_cap); the rest of a
 // crowded cell (this Tait law resists only expansion, so compressed fluid
-// piles up) is shared by all 32 lanes and reduced across the warp.  The
-// footprint's z-planes that the item reached go to global memory with one
-// vector reduction per touched node.  Unlike the reference, no partial sum
+// piles up) goes to a list in chunks of kCrowdChunk particles, which a
+// second launch spreads over all warps (the count order gathers a bin's
+// crowded cells in one item, and one warp working through all of their
+// particles would hold up the kernel).  The footprint's z-planes that the
+// item reached go to global memory with one vector reduction per touched
+// node.  Unlike the reference, no partial sum
 // is dropped (it drops shared-tile cells whose partial mass is <= 1e-9,
 // kernels.cu:132).
 constexpr int kP2GWarpsPerSM = 12;
 constexpr int kRing = 2;
 constexpr int kGidxStage = 256;   // gather indices of a bin staged in shared memory
-constexpr int kCellCap = 12;      // particles of a cell its own lane sums; the rest: whole warp
+constexpr int kCellCap = 12;      // particles of a cell its own lane sums; the rest: the crowded-cell list
+constexpr int kCrowdChunk = 256;  // particles of a crowded cell per list entry
 constexpr int kTX = kBinX + 2, kTY = kBinY + 2;
 constexpr int kFootPlane = kTX * kTY;              // 60 nodes of one z-plane
 constexpr int kFootNodes = kFootPlane * (kBinZ + 2);  // 360: a bin's stencil footprint
@@ -243,8 +247,9 @@ __device__ __forceinline__ void p2g_stencil(const P2GParticle& r, Emit emit) {
 // The crowded-cell threshold of one work item, from the counts of its 32
 // cells (`full`, one per lane): for each candidate cap the loop costs
 // min(max count, cap) iterations with every lane, plus, per cell above the
-// cap, ceil((count - cap) / 32) iterations and one reduce-scatter (about 1.3
-// iterations); the cheapest candidate wins.  Every cap gives the same sums.
+// cap, ceil((count - cap) / 32) whole-warp iterations and one reduce-scatter
+// (about 1.3 iterations) in the crowded-cell launch; the cheapest candidate
+// wins.  Every cap gives the same sums.
 __device__ __forceinline__ int item_cap(int full) {
     const int maxc = __reduce_max_sync(0xffffffffu, (unsigned)full);
     int best = kCellCap;
@@ -266,8 +271,8 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
                                                                   const uint8_t* __restrict__ corder,
                                                                   const long long* __restrict__ itemoff,
                                                                   uint32_t* __restrict__ work,
-                                                                  float4* __restrict__ accum_all,
-                                                                  uint32_t* __restrict__ status, int cap) {
+                                                                  float4* __restrict__ accum_all, int4* __restrict__ crowd,
+                                                                  int crowd_cap, uint32_t* __restrict__ status, int cap) {
     __shared__ __align__(16) float4 s_ring[kRing][6][32];
     __shared__ float4 s_foot[kFootNodes];
     __shared__ int32_t s_gidx[kGidxStage];
@@ -279,7 +284,7 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
         if (lane == 0) item = (int)atomicAdd(work, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= nitems) return;
-        // Items: kBinZ layers per listed bin, scene after scene.
+        // Items: kBinZ per listed bin, scene after scene.
         const int scene = sc.count == 1 ? 0 : scene_of(itemoff, sc.count, item);
         const SimParams p = sc.prm[scene];
         const int local = item - (int)__ldg(itemoff + scene);
@@ -303,129 +308,87 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
         if (staged)
             for (int q = lane; q < l1 - l0; q += 32) s_gidx[q] = __ldg(gidx + l0 + q);
         __syncwarp();
-        // Pass 0: each lane its own cell's first `cap` particles (slots
-        // cs + s).  Pass k > 0: the k-th crowded cell's further particles,
-        // slot hcs + cap + lane + 32 s, for every lane.  One loop body
-        // serves both; only the flush differs.
+        // Each lane sums its cell's first `icap` particles; the rest of a
+        // crowded cell goes to the crowded-cell list in chunks, which
+        // p2g_crowd_kernel spreads over all warps.
         const int icap = cap > 0 ? cap : item_cap(full);
-        uint32_t crowded = __ballot_sync(0xffffffffu, full > icap);
-        int first = cs, step = 1, cnt = min(full, icap), target = tcell;
-        for (;;) {
-            float am[27], ax[27], ay[27], az[27];
-            int maxc = cnt;
+        for (int off = icap; off < full; off += kCrowdChunk) {
+            const uint32_t e = atomicAdd(work + 2, 1u);
+            if (e < (uint32_t)crowd_cap)
+                crowd[e] = make_int4(scene, bin * kBinCells + tcell, cs + off, min(kCrowdChunk, full - off));
+            else
+                atomicOr(status, kStatusCrowdList);
+        }
+        const int cnt = min(full, icap);
+        const int maxc = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
+        float am[27], ax[27], ay[27], az[27];
+        auto src_of = [&](int s) -> const float4* {
+            const int slot = cs + s;
+            const int g = staged ? s_gidx[slot - l0] : __ldg(gidx + slot);
+            return reinterpret_cast<const float4*>(P + (size_t)g * kAFloats);
+        };
 #pragma unroll
-            for (int o = 16; o; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
-            auto src_of = [&](int s) -> const float4* {
-                const int slot = first + s * step;
-                const int g = staged ? s_gidx[slot - l0] : __ldg(gidx + slot);
-                return reinterpret_cast<const float4*>(P + (size_t)g * kAFloats);
-            };
+        for (int k = 0; k < 27; ++k) am[k] = ax[k] = ay[k] = az[k] = 0.f;
 #pragma unroll
-            for (int k = 0; k < 27; ++k) am[k] = ax[k] = ay[k] = az[k] = 0.f;
+        for (int d = 0; d < kRing - 1; ++d) {
+            if (d < cnt) {
+                const float4* src = src_of(d);
 #pragma unroll
-            for (int d = 0; d < kRing - 1; ++d) {
-                if (d < cnt) {
-                    const float4* src = src_of(d);
-#pragma unroll
-                    for (int v = 0; v < 6; ++v) cp_async16(&s_ring[d][v][lane], src + v);
-                }
-                cp_async_commit();
+                for (int v = 0; v < 6; ++v) cp_async16(&s_ring[d][v][lane], src + v);
             }
-            for (int s = 0; s < maxc; ++s) {
-                const int pf = s + kRing - 1;
-                if (pf < cnt) {
-                    const float4* src = src_of(pf);
+            cp_async_commit();
+        }
+        for (int s = 0; s < maxc; ++s) {
+            const int pf = s + kRing - 1;
+            if (pf < cnt) {
+                const float4* src = src_of(pf);
 #pragma unroll
-                    for (int v = 0; v < 6; ++v) cp_async16(&s_ring[pf % kRing][v][lane], src + v);
-                }
-                cp_async_commit();
-                cp_async_wait<kRing - 1>();
-                __syncwarp();
-                if (s < cnt) {
-                    const int sl = s % kRing;
-                    const P2GParticle r = p2g_particle(p, s_ring[sl][0][lane], s_ring[sl][1][lane], s_ring[sl][2][lane],
-                                                       s_ring[sl][3][lane], s_ring[sl][4][lane], s_ring[sl][5][lane]);
-                    // Filed under a cell of this layer by construction; a
-                    // mismatch is recorded, never scattered to a wrong node.
-                    if (r.bx - ox != target % kBinX || r.by - oy != (target / kBinX) % kBinY ||
-                        r.bz - oz != target / 32) {
-                        atomicOr(status, kStatusBinning);
-                    } else {
-                        p2g_stencil(r, [&](int k, int, int, int, float m, float mx, float my, float mz) {
-                            am[k] += m;
-                            ax[k] += mx;
-                            ay[k] += my;
-                            az[k] += mz;
-                        });
-                    }
-                }
-                __syncwarp();
+                for (int v = 0; v < 6; ++v) cp_async16(&s_ring[pf % kRing][v][lane], src + v);
             }
-            cp_async_wait<0>();
-            if (step == 1) {
-                // One lane per cell: distinct nodes for each stencil offset.
-                const int tx = tcell % kBinX, ty = (tcell / kBinX) % kBinY, tz = (tcell / 32) & (kBinZ - 1);
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-#pragma unroll
-                    for (int b = 0; b < 3; ++b)
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            const int k = (c * 3 + b) * 3 + a;
-                            float4* d = &s_foot[((tz + c) * kTY + ty + b) * kTX + tx + a];
-                            __syncwarp();
-                            if (own) {
-                                float4 v = *d;
-                                v.x += am[k];
-                                v.y += ax[k];
-                                v.z += ay[k];
-                                v.w += az[k];
-                                *d = v;
-                            }
-                        }
-            } else {
-                // A crowded cell's pass: reduce-scatter the 32 lanes' partial
-                // sums (27 nodes x 4, padded to 128 values) by halving them at
-                // each shuffle step, so that lane l ends with node l's totals.
-                float v[128];
-#pragma unroll
-                for (int k = 0; k < 32; ++k) {
-                    v[4 * k + 0] = k < 27 ? am[k < 27 ? k : 0] : 0.f;
-                    v[4 * k + 1] = k < 27 ? ax[k < 27 ? k : 0] : 0.f;
-                    v[4 * k + 2] = k < 27 ? ay[k < 27 ? k : 0] : 0.f;
-                    v[4 * k + 3] = k < 27 ? az[k < 27 ? k : 0] : 0.f;
-                }
-#pragma unroll
-                for (int d = 16, h = 64; d >= 1; d >>= 1, h >>= 1) {
-                    const bool upper = (lane & d) != 0;
-#pragma unroll
-                    for (int i = 0; i < h; ++i) {
-                        const float send = upper ? v[i] : v[i + h];
-                        const float keep = upper ? v[i + h] : v[i];
-                        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
-                    }
-                }
-                if (lane < 27) {
-                    const int a = lane % 3, b = (lane / 3) % 3, c = lane / 9;
-                    const int tx = target % kBinX, ty = (target / kBinX) % kBinY, tz = target / 32;
-                    float4* d = &s_foot[((tz + c) * kTY + ty + b) * kTX + tx + a];
-                    float4 u = *d;
-                    u.x += v[0];
-                    u.y += v[1];
-                    u.z += v[2];
-                    u.w += v[3];
-                    *d = u;
+            cp_async_commit();
+            cp_async_wait<kRing - 1>();
+            __syncwarp();
+            if (s < cnt) {
+                const int sl = s % kRing;
+                const P2GParticle r = p2g_particle(p, s_ring[sl][0][lane], s_ring[sl][1][lane], s_ring[sl][2][lane],
+                                                   s_ring[sl][3][lane], s_ring[sl][4][lane], s_ring[sl][5][lane]);
+                // Filed under this lane's cell by construction; a mismatch is
+                // recorded, never scattered to a wrong node.
+                if (r.bx - ox != tcell % kBinX || r.by - oy != (tcell / kBinX) % kBinY || r.bz - oz != tcell / 32) {
+                    atomicOr(status, kStatusBinning);
+                } else {
+                    p2g_stencil(r, [&](int k, int, int, int, float m, float mx, float my, float mz) {
+                        am[k] += m;
+                        ax[k] += mx;
+                        ay[k] += my;
+                        az[k] += mz;
+                    });
                 }
             }
             __syncwarp();
-            if (!crowded) break;
-            const int src = __ffs(crowded) - 1;
-            crowded &= crowded - 1;
-            const int hcnt = __shfl_sync(0xffffffffu, full, src);
-            first = __shfl_sync(0xffffffffu, cs, src) + icap + lane;
-            step = 32;
-            cnt = max(0, (hcnt - icap - lane + 31) / 32);
-            target = __shfl_sync(0xffffffffu, tcell, src);
+        }
+        cp_async_wait<0>();
+        // One lane per cell: distinct nodes for each stencil offset.
+        {
+            const int tx = tcell % kBinX, ty = (tcell / kBinX) % kBinY, tz = (tcell / 32) & (kBinZ - 1);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const int k = (c * 3 + b) * 3 + a;
+                        float4* d = &s_foot[((tz + c) * kTY + ty + b) * kTX + tx + a];
+                        __syncwarp();
+                        if (own) {
+                            float4 v = *d;
+                            v.x += am[k];
+                            v.y += ax[k];
+                            v.z += ay[k];
+                            v.w += az[k];
+                            *d = v;
+                        }
+                    }
         }
         __syncwarp();
         // The z-planes the group's cells reach: zmin .. zmax + 2.
@@ -437,6 +400,104 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
             s_foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (node_in_grid(p, x, y, z) && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))  // NaN counts
                 red_add_v4(accum + node_index(p, x, y, z), v.x, v.y, v.z, v.w);
+        }
+        __syncwarp();
+    }
+}
+
+// The crowded-cell list: each entry (scene, bin * 128 + cell, first slot,
+// count <= kCrowdChunk) is the next chunk of a crowded cell's particles.  All
+// 32 lanes take its particles (slot first + lane + 32 s), sum their 27 x 4
+// contributions in registers, reduce-scatter them across the warp (five
+// shuffle steps, each halving the 128 padded sums, so lane l ends with node
+// l's totals) and add them to global memory.
+__global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_crowd_kernel(SceneTable sc, const float* __restrict__ P,
+                                                                        const int32_t* __restrict__ gidx,
+                                                                        const int4* __restrict__ crowd, int crowd_cap,
+                                                                        uint32_t* __restrict__ work,
+                                                                        float4* __restrict__ accum_all,
+                                                                        uint32_t* __restrict__ status) {
+    __shared__ __align__(16) float4 s_ring[kRing][6][32];
+    const int lane = threadIdx.x;
+    const int total = (int)min(*reinterpret_cast<volatile const uint32_t*>(work + 2), (uint32_t)crowd_cap);
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = (int)atomicAdd(work + 3, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= total) return;
+        const int4 e = crowd[item];
+        const SimParams p = sc.prm[e.x];
+        const int bin = e.y / kBinCells, cell = e.y % kBinCells;
+        const int bxi = bin % p.nbx, byi = (bin / p.nbx) % p.nby, bzi = bin / (p.nbx * p.nby);
+        const int bx = bxi * kBinX - 2 + cell % kBinX, by = byi * kBinY - 2 + (cell / kBinX) % kBinY;
+        const int bz = bzi * kBinZ - 2 + cell / 32;
+        const int first = e.z + lane, cnt = max(0, (e.w - lane + 31) / 32), maxc = (e.w + 31) / 32;
+        float am[27], ax[27], ay[27], az[27];
+#pragma unroll
+        for (int k = 0; k < 27; ++k) am[k] = ax[k] = ay[k] = az[k] = 0.f;
+        auto src_of = [&](int s) -> const float4* {
+            return reinterpret_cast<const float4*>(P + (size_t)__ldg(gidx + first + 32 * s) * kAFloats);
+        };
+#pragma unroll
+        for (int d = 0; d < kRing - 1; ++d) {
+            if (d < cnt) {
+                const float4* src = src_of(d);
+#pragma unroll
+                for (int v = 0; v < 6; ++v) cp_async16(&s_ring[d][v][lane], src + v);
+            }
+            cp_async_commit();
+        }
+        for (int s = 0; s < maxc; ++s) {
+            const int pf = s + kRing - 1;
+            if (pf < cnt) {
+                const float4* src = src_of(pf);
+#pragma unroll
+                for (int v = 0; v < 6; ++v) cp_async16(&s_ring[pf % kRing][v][lane], src + v);
+            }
+            cp_async_commit();
+            cp_async_wait<kRing - 1>();
+            __syncwarp();
+            if (s < cnt) {
+                const int sl = s % kRing;
+                const P2GParticle r = p2g_particle(p, s_ring[sl][0][lane], s_ring[sl][1][lane], s_ring[sl][2][lane],
+                                                   s_ring[sl][3][lane], s_ring[sl][4][lane], s_ring[sl][5][lane]);
+                if (r.bx != bx || r.by != by || r.bz != bz) {
+                    atomicOr(status, kStatusBinning);
+                } else {
+                    p2g_stencil(r, [&](int k, int, int, int, float m, float mx, float my, float mz) {
+                        am[k] += m;
+                        ax[k] += mx;
+                        ay[k] += my;
+                        az[k] += mz;
+                    });
+                }
+            }
+            __syncwarp();
+        }
+        cp_async_wait<0>();
+        __syncwarp();
+        float v[128];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            v[4 * k + 0] = k < 27 ? am[k < 27 ? k : 0] : 0.f;
+            v[4 * k + 1] = k < 27 ? ax[k < 27 ? k : 0] : 0.f;
+            v[4 * k + 2] = k < 27 ? ay[k < 27 ? k : 0] : 0.f;
+            v[4 * k + 3] = k < 27 ? az[k < 27 ? k : 0] : 0.f;
+        }
+#pragma unroll
+        for (int d = 16, h = 64; d >= 1; d >>= 1, h >>= 1) {
+            const bool upper = (lane & d) != 0;
+#pragma unroll
+            for (int i = 0; i < h; ++i) {
+                const float send = upper ? v[i] : v[i + h];
+                const float keep = upper ? v[i + h] : v[i];
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
+            }
+        }
+        if (lane < 27) {
+            const int x = bx + lane % 3, y = by + (lane / 3) % 3, z = bz + lane / 9;
+            if (node_in_grid(p, x, y, z) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f))
+                red_add_v4(accum_all + p.goff + node_index(p, x, y, z), v[0], v[1], v[2], v[3]);
         }
         __syncwarp();
     }
@@ -532,6 +593,8 @@ __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(SceneTable sc, c
     if (scene == 0 && chunk == 0 && t == 0) {
         work[0] = 0u;  // P2G items
         work[1] = 0u;  // G2P items
+        work[2] = 0u;  // crowded-cell list length
+        work[3] = 0u;  // crowded-cell entries taken
         // Per-scene prefixes: P2G items (kBinZ per listed bin of the current
         // set) and the listed bins of the set to clear.
         long long run = 0, runc = 0;
@@ -1136,13 +1199,16 @@ int p2g_max_ctas_per_sm() {
 
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
                const int32_t* cstart, const BinSet& cur, const uint8_t* corder, const long long* itemoff,
-               uint32_t* work, float4* accum, uint32_t* status, cudaStream_t st, int ctas_per_sm, int cell_cap) {
+               uint32_t* work, float4* accum, int4* crowd, int crowd_cap, uint32_t* status, cudaStream_t st,
+               int ctas_per_sm, int cell_cap) {
     if (n <= 0) return 0;
     const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : kP2GWarpsPerSM;
     const int cap = cell_cap > 0 ? cell_cap : 0;
     const int warps = (int)std::min(bins_total * kBinZ, 148LL * per_sm);
-    p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, corder, itemoff, work, accum, status, cap);
-    return 1;
+    p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, corder, itemoff, work, accum, crowd, crowd_cap, status,
+                                     cap);
+    p2g_crowd_kernel<<<148 * kP2GWarpsPerSM, 32, 0, st>>>(sc, P, gidx, crowd, crowd_cap, work, accum, status);
+    return 2;
 }
 
 int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
