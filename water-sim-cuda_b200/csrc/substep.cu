@@ -249,13 +249,15 @@ __device__ __forceinline__ void p2g_stencil(const P2GParticle& r, Emit emit) {
 // min(max count, cap) iterations with every lane, plus, per cell above the
 // cap, ceil((count - cap) / 32) whole-warp iterations and one reduce-scatter
 // (about 1.3 iterations) in the crowded-cell launch; the cheapest candidate
-// wins.  Every cap gives the same sums.
+// wins.  Every cap gives the same sums.  Caps stop at 32: a larger one makes a
+// few long items that hold up the kernel while other warps idle, whereas the
+// list spreads the rest of a crowded cell over all warps.
 __device__ __forceinline__ int item_cap(int full) {
     const int maxc = __reduce_max_sync(0xffffffffu, (unsigned)full);
     int best = kCellCap;
     float best_cost = 1e30f;
 #pragma unroll
-    for (int cand : {8, 12, 16, 24, 32, 48, 64, 96, 128}) {
+    for (int cand : {8, 12, 16, 24, 32}) {
         const int over = full > cand ? (full - cand + 31) / 32 : 0;
         const int passes = (int)__reduce_add_sync(0xffffffffu, (unsigned)over);
         const int cells = __popc(__ballot_sync(0xffffffffu, full > cand));
