@@ -517,8 +517,8 @@ typedef struct mpm_tuning {
     int32_t grid_block;       /* 128 or 256 (default 256) */
     float p2g_ms, g2p_ms, grid_ms;  /* stage times of the chosen shapes (mpm_autotune) */
     int32_t p2g_cell_cap;     /* 4 .. 64: particles of a cell one lane sums before the
-                               * cell is shared by the warp; 0 (default): chosen per
-                               * work item from its cells' particle counts */
+                               * rest goes, in chunks, to all warps; 0 (default): chosen
+                               * per work item from its cells' particle counts */
 } mpm_tuning;
 mpm_status mpm_autotune(mpm_engine* engine, int32_t repeats, mpm_tuning* out);
 mpm_status mpm_set_tuning(mpm_engine* engine, const mpm_tuning* tuning);

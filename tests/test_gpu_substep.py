@@ -125,3 +125,28 @@ def test_reinit_and_counts(gpu_ok, mpm):
         eng.step(1)
         s = eng.stats()
         assert s["substeps"] == 1 and s["kernel_launches"] > 0
+
+
+@pytest.mark.parametrize("case", ["dense_cap4", "one_cell_pile"])
+def test_crowded_cells_through_the_list(gpu_ok, mpm, oracle64, case):
+    """Particles past a cell's cap go to the crowded-cell list, 256 per entry,
+    and a second launch sums them.  In a dense scene at the smallest cap, every
+    cell above 4 particles takes that path; a pile of 3000 particles in one
+    cell makes several entries of one cell."""
+    from mpm_b200 import scenes
+    cfg, st, tris = scenes.small_scene(30_000 if case == "dense_cap4" else 6000, (16, 16, 16), seed=7,
+                                       obstacle=False)
+    if case == "one_cell_pile":
+        rng = np.random.default_rng(8)
+        st[0:3, :3000] = rng.uniform(8.5, 9.5, (3, 3000)).astype(np.float32)  # stencil base cell (8, 8, 8)
+    with mpm.Engine(cfg) as eng:
+        eng.init(st)
+        eng.init_sdf(tris)
+        if case == "dense_cap4":
+            eng.set_tuning(12, 256, 256, 4)
+        sdf = eng.get_sdf()
+        eng.step(1)
+        got = eng.get_buffer()
+    st0 = oracle64.init_particles(cfg, st)
+    want, _, _, _ = oracle64.substep(cfg, st0, sdf.astype(np.float64))
+    assert_state_close(got, want, st0)

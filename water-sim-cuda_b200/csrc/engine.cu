@@ -236,9 +236,10 @@ mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_by
         CK(e, cudaMalloc(&e->sigma[k], ibytes));
     }
     CK(e, cudaMalloc(&e->gidx, ibytes));
-    // A crowded-cell entry holds at least one particle beyond a cap of 8 or
-    // more, and a cell yields one entry per 256 of them: fewer than n / 8.
-    e->crowd_cap = (int)std::min<long long>(cap / 8 + 64, 0x7fffffffLL);
+    // A crowded-cell entry holds at least one particle beyond a cap of 4 or
+    // more (the smallest mpm_set_tuning accepts), and a cell yields one entry
+    // per 256 of them: fewer than n / 4 entries.
+    e->crowd_cap = (int)std::min<long long>(cap / 4 + 64, 0x7fffffffLL);
     CK(e, cudaMalloc(&e->crowd, (size_t)e->crowd_cap * sizeof(int4)));
     CK(e, cudaMalloc(&e->pcell, ibytes));
     CK(e, cudaMalloc(&e->prank, ibytes));

@@ -82,7 +82,7 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
 int bin_scan_chunks(long long bins);
 // P2G over the items of `cur`; gidx maps slots of the new order to P.  Two
 // launches: the items, then the crowded-cell list they fill (crowd: scratch of
-// crowd_cap entries, at least n / 8 + 64; work[2..3] are its counters, reset
+// crowd_cap entries, at least n / 4 + 64; work[2..3] are its counters, reset
 // by the bin scan).  ctas_per_sm: persistent single-warp CTAs per SM (0 = the
 // default 12); cell_cap: particles of a cell its own lane sums before the rest
 // goes to the list (0 = chosen per work item from its cells' counts).
