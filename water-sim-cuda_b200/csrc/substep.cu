@@ -834,6 +834,15 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
 // R substeps under a constant acceleration move a particle by exactly that.
 enum G2PMode : int { kG2PPlain = 0, kG2PLearned = 1, kG2PCollect = 2, kG2PLarge = 3, kG2PLearnedTc = 4 };
 
+// Particles per thread of a G2P instantiation: two for the batched plain
+// mode (records staged in dynamic shared memory, kPer x 3 x blockDim float4),
+// one otherwise.  Measured per substep on the 64-scene batch, two per thread
+// cut G2P by 5-8 %; on one scene (fewer registers, more warps per SM) two
+// per thread cost 5 % and four 20 %.
+__host__ __device__ constexpr int g2p_per_thread(bool batch, int mode, bool wide) {
+    return (mode == 0 && !wide && batch) ? 2 : 1;
+}
+
 // kWide: 256-thread CTAs free to use up to 255 registers (one CTA per SM,
 // every node load of a particle in flight at once) instead of 64 registers
 // and four CTAs per SM; chosen by the autotuner.
@@ -863,7 +872,28 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
         mlp_tc_begin(ts);  // TMEM columns and the mbarrier; synchronises the CTA
     }
     const SceneLookup<kBatch> look(sc, sc.poff, s_prm, s_first);
-    const long long jj = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    // The plain mode takes kPer particles per thread (block b: particles
+    // b * kPer * blockDim .. + kPer * blockDim, one blockDim-wide slice per
+    // pass) and requests all their positions and F up front, into shared
+    // memory with cp.async, so that a record's load overlaps the passes
+    // before it.  Every lane makes all kPer passes: filing is warp-wide.
+    constexpr int kPer = g2p_per_thread(kBatch, kMode, kWide);
+    float4* s_rec = reinterpret_cast<float4*>(s_dyn);  // [kPer][3][blockDim] when kPer > 1
+    if constexpr (kPer > 1) {
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const long long jk = ((long long)blockIdx.x * kPer + k) * blockDim.x + threadIdx.x;
+            if (jk < n_total) {
+                const float4* qk = reinterpret_cast<const float4*>(Pin + (size_t)__ldg(gidx + jk) * kAFloats);
+#pragma unroll
+                for (int v = 0; v < 3; ++v) cp_async16(s_rec + (k * 3 + v) * blockDim.x + threadIdx.x, qk + v);
+            }
+        }
+        cp_async_commit();
+    }
+#pragma unroll 1
+    for (int k = 0; k < kPer; ++k) {
+    const long long jj = ((long long)blockIdx.x * kPer + k) * blockDim.x + threadIdx.x;
     const bool valid = jj < n_total;
     const long long j = valid ? jj : n_total - 1;  // idle lanes redo the last particle and store nothing
     const int scene = look.scene(j);
@@ -872,7 +902,16 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
     const float* sdf = sdf_all + p.goff;
     const int src = __ldg(gidx + j);
     const float4* q = reinterpret_cast<const float4*>(Pin + (size_t)src * kAFloats);
-    const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+    float4 q0, q1, q2;
+    if constexpr (kPer > 1) {
+        if (k == 0) cp_async_wait<0>();  // every record of this thread has arrived
+        const float4* r = s_rec + (k * 3) * blockDim.x + threadIdx.x;
+        q0 = valid ? r[0] : make_float4(0.f, 0.f, 0.f, 0.f);
+        q1 = valid ? r[blockDim.x] : make_float4(0.f, 0.f, 0.f, 0.f);
+        q2 = valid ? r[2 * blockDim.x] : make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+        q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+    }
     float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);
     if constexpr (kMode != kG2PPlain) qv = __ldg(q + 3);  // old velocity
     const float pos[3] = {q0.x, q0.y, q0.z};
@@ -1044,7 +1083,7 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
         gbin = (int)p.boff + bin;
     }
     const int rank = file_particle(gcell, gbin, bin, scene, p.boff, next);
-    if (!valid) return;
+    if (!valid) continue;  // only the last passes of the last block have idle lanes
     float4* o = reinterpret_cast<float4*>(Pout + (size_t)j * kAFloats);
     o[0] = make_float4(nx, ny, nz, NF[0]);
     o[1] = make_float4(NF[1], NF[2], NF[3], NF[4]);
@@ -1066,6 +1105,7 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
     if (!(nx >= 0.f && nx < (float)p.sx && ny >= 0.f && ny < (float)p.sy && nz >= 0.f && nz < (float)p.sz))
         flags |= 2u;
     if (flags) atomicOr(health, flags);
+    }
 }
 
 // ------------------------------------------------------- state transfer ----
@@ -1260,9 +1300,11 @@ int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const flo
         g2p_kernel<true, kG2PPlain, true><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in,
                                                                             sig_out, vgrid, sdf, pcell, prank, next,
                                                                             health, la);
-    else
-        g2p_kernel<true, kG2PPlain><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out,
-                                                                      vgrid, sdf, pcell, prank, next, health, la);
+    else {
+        constexpr int k = g2p_per_thread(true, kG2PPlain, false);
+        g2p_kernel<true, kG2PPlain><<<blocks_for(n, (long long)pb * k), pb, k * 3 * pb * sizeof(float4), st>>>(
+            sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, prank, next, health, la);
+    }
     return 1;
 }
 
