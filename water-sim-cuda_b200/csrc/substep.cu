@@ -70,9 +70,12 @@ __device__ __forceinline__ int file_particle(int gcell, int gbin, int bin, int s
 
 // Scene lookup for the per-particle and per-node kernels.  With one scene
 // (kBatch false) the parameters are the kernel argument p0, read from the
-// parameter bank; with several, the CTA stages up to kTableScenes scene
-// records and their first indices in shared memory and each thread finds its
-// scene there by binary search (in global memory beyond that).
+// parameter bank.  With several, a CTA whose indices are [i0, i1) needs only
+// the scenes that range touches (usually one or two): the first threads find
+// its first and last scene in one parallel test, and the CTA stages just those
+// records and first indices in shared memory.  Each thread then finds its
+// scene there.  Beyond kTableScenes scenes the lookup searches the global
+// table.
 constexpr int kTableScenes = 64;
 
 template <bool kBatch>
@@ -80,32 +83,50 @@ struct SceneLookup {
     const SimParams* prm;
     const long long* first;
     int count;
+    int lo = 0;  // global index of prm[0] / first[0]
 
     // Must be reached by every thread of the CTA (it may synchronize).
+    // s_range: two ints of shared memory.
     __device__ __forceinline__ SceneLookup(const SceneTable& sc, const long long* first_global, SimParams* s_prm,
-                                           long long* s_first)
+                                           long long* s_first, int* s_range, long long i0, long long i1)
         : prm(sc.prm), first(first_global), count(sc.count) {
         if constexpr (kBatch) {
             if (count <= kTableScenes) {
-                for (int i = threadIdx.x; i < count; i += blockDim.x) s_prm[i] = sc.prm[i];
-                for (int i = threadIdx.x; i <= count; i += blockDim.x) s_first[i] = first_global[i];
+                // Scene s holds index i when it is the last with first[s] <= i
+                // (first[0] = 0, non-decreasing): exactly one thread matches.
+                const int t = threadIdx.x;
+                if (t < count) {
+                    const long long f0 = first_global[t];
+                    const long long f1 = t + 1 < count ? first_global[t + 1] : LLONG_MAX;
+                    if (f0 <= i0 && i0 < f1) s_range[0] = t;
+                    if (f0 <= i1 - 1 && i1 - 1 < f1) s_range[1] = t;
+                }
+                __syncthreads();
+                lo = s_range[0];
+                const int n = s_range[1] - lo + 1;
+                if (t < n) s_prm[t] = sc.prm[lo + t];
+                if (t <= n) s_first[t] = first_global[lo + t];
                 __syncthreads();
                 prm = s_prm;
                 first = s_first;
+                count = n;
             }
         }
     }
 
+    // Global scene index of index i (i in the CTA's range).
     __device__ __forceinline__ int scene(long long i) const {
         if constexpr (!kBatch) return 0;
-        int lo = 0, hi = count - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (first[mid] <= i) lo = mid;
-            else hi = mid - 1;
+        int a = 0, b = count - 1;
+        while (a < b) {
+            const int mid = (a + b + 1) >> 1;
+            if (first[mid] <= i) a = mid;
+            else b = mid - 1;
         }
-        return lo;
+        return lo + a;
     }
+
+    __device__ __forceinline__ const SimParams& params(int scene) const { return prm[scene - lo]; }
 };
 
 // ------------------------------------------------------------------ P2G ----
@@ -783,10 +804,12 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
                                                           const float* __restrict__ sdf_all) {
     __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
     __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
-    const SceneLookup<kBatch> look(sc, sc.goff, s_prm, s_first);
+    __shared__ int s_range[2];
     const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const SceneLookup<kBatch> look(sc, sc.goff, s_prm, s_first, s_range, blockIdx.x * (long long)blockDim.x,
+                                   min((blockIdx.x + 1) * (long long)blockDim.x, g_total));
     if (gi >= g_total) return;
-    const SimParams& p = kBatch ? look.prm[look.scene(gi)] : p0;
+    const SimParams& p = kBatch ? look.params(look.scene(gi)) : p0;
     const int idx = (int)(gi - p.goff);
     const float* sdf = sdf_all + p.goff;
     const float4 a = accum[gi];
@@ -855,6 +878,7 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
                                                   uint32_t* __restrict__ health, LearnArgs la) {
     __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
     __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
+    __shared__ int s_range[2];
     __shared__ __align__(16) unsigned char s_mlp_raw[kMode == kG2PLearned ? sizeof(MlpPacked) : 16];
     __shared__ uint32_t s_stage[kMode == kG2PLearned ? 8 * 32 * kMlpStageStride : 1];
     extern __shared__ __align__(1024) unsigned char s_dyn[];  // MlpTcSmem in the tcgen05 mode
@@ -871,13 +895,15 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
         for (int i = threadIdx.x; i < (int)(sizeof(MlpTc) / 16); i += blockDim.x) dst[i] = __ldg(src + i);
         mlp_tc_begin(ts);  // TMEM columns and the mbarrier; synchronises the CTA
     }
-    const SceneLookup<kBatch> look(sc, sc.poff, s_prm, s_first);
+    constexpr int kPer = g2p_per_thread(kBatch, kMode, kWide);
+    const long long cta0 = (long long)blockIdx.x * kPer * blockDim.x;  // this CTA's particles: [cta0, cta1)
+    const SceneLookup<kBatch> look(sc, sc.poff, s_prm, s_first, s_range, cta0,
+                                   min(cta0 + (long long)kPer * blockDim.x, n_total));
     // The plain mode takes kPer particles per thread (block b: particles
     // b * kPer * blockDim .. + kPer * blockDim, one blockDim-wide slice per
     // pass) and requests all their positions and F up front, into shared
     // memory with cp.async, so that a record's load overlaps the passes
     // before it.  Every lane makes all kPer passes: filing is warp-wide.
-    constexpr int kPer = g2p_per_thread(kBatch, kMode, kWide);
     float4* s_rec = reinterpret_cast<float4*>(s_dyn);  // [kPer][3][blockDim] when kPer > 1
     if constexpr (kPer > 1) {
 #pragma unroll
@@ -897,7 +923,7 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
     const bool valid = jj < n_total;
     const long long j = valid ? jj : n_total - 1;  // idle lanes redo the last particle and store nothing
     const int scene = look.scene(j);
-    const SimParams& p = kBatch ? look.prm[scene] : p0;
+    const SimParams& p = kBatch ? look.params(scene) : p0;
     const float4* vgrid = vgrid_all + p.goff;
     const float* sdf = sdf_all + p.goff;
     const int src = __ldg(gidx + j);
