@@ -866,11 +866,15 @@ __host__ __device__ constexpr int g2p_per_thread(bool batch, int mode, bool wide
     return (mode == 0 && !wide && batch) ? 2 : 1;
 }
 
+// CTAs per SM: the learned tcgen05 mode fits four (64 registers, 128 TMEM
+// columns and about 45 KB of shared memory each), so one CTA's MMA waits
+// overlap the other three's work; mma.sync learned, collect and batched
+// modes need more registers.
 // kWide: 256-thread CTAs free to use up to 255 registers (one CTA per SM,
 // every node load of a particle in flight at once) instead of 64 registers
 // and four CTAs per SM; chosen by the autotuner.
 template <bool kBatch, int kMode, bool kWide = false>
-__global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch || kMode == 2 || kMode == 4) ? 3 : 4))) g2p_kernel(SceneTable sc, SimParams p0, long long n_total, const float* __restrict__ Pin,
+__global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch || kMode == 2) ? 3 : 4))) g2p_kernel(SceneTable sc, SimParams p0, long long n_total, const float* __restrict__ Pin,
                                                   float* __restrict__ Pout, const int32_t* __restrict__ gidx,
                                                   const int32_t* __restrict__ sig_in, int32_t* __restrict__ sig_out,
                                                   const float4* __restrict__ vgrid_all, const float* __restrict__ sdf_all,
