@@ -127,6 +127,28 @@ def test_reinit_and_counts(gpu_ok, mpm):
         assert s["substeps"] == 1 and s["kernel_launches"] > 0
 
 
+def test_reinit_reuses_buffers(gpu_ok, mpm, oracle64):
+    """Re-initialising with no more particles than before keeps the device
+    buffers (6000, then 2500, then 6000 again); the substep after each init
+    still matches the oracle."""
+    from mpm_b200 import scenes
+    cfg, big, tris = scenes.small_scene(6000, (32, 32, 32), seed=10)
+    _, small, _ = scenes.small_scene(2500, (32, 32, 32), seed=11)
+    with mpm.Engine(cfg) as eng:
+        eng.init(big)
+        eng.init_sdf(tris)
+        eng.step(2)
+        for st in (small, big):
+            eng.init(st)
+            assert eng.get_number() == st.shape[1]
+            sdf = eng.get_sdf()
+            eng.step(1)
+            got = eng.get_buffer()
+            st0 = oracle64.init_particles(cfg, st)
+            want = oracle64.substep(cfg, st0, sdf.astype(np.float64))[0]
+            assert_state_close(got, want, st0)
+
+
 @pytest.mark.parametrize("case", ["dense_cap4", "one_cell_pile"])
 def test_crowded_cells_through_the_list(gpu_ok, mpm, oracle64, case):
     """Particles past a cell's cap go to the crowded-cell list, 256 per entry,

@@ -76,6 +76,9 @@ struct mpm_engine {
     bool initialized = false;
     long long n = 0;  // particles of all scenes
     int max_n = 0;    // largest scene
+    long long cap_n = 0;     // particles, largest scene and sort scratch bytes the
+    int cap_max_n = 0;       // particle buffers were allocated for
+    size_t cap_sort = 0;
     float* P[2] = {nullptr, nullptr};        // particle-major state, 24 floats per particle
     int32_t* sigma[2] = {nullptr, nullptr};  // slot -> original slot (global)
     int32_t* gidx = nullptr;                 // new slot -> old slot of the current binning
@@ -226,9 +229,36 @@ mpm_status ensure_staging(mpm_engine* e, size_t bytes) {
 }
 
 mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_bytes) {
+    if (e->P[0] && n <= e->cap_n && max_n <= e->cap_max_n && sort_bytes <= e->cap_sort) {
+        // The buffers of an earlier init are large enough: keep them (freeing
+        // and allocating half a gigabyte takes from a few to hundreds of
+        // milliseconds).  The substep graphs are captured again by the caller;
+        // the learned-step buffers, sized by the earlier n, are allocated
+        // again when next needed.  Work of the earlier state (an asynchronous
+        // positions read-back on the copy stream included) ends first.
+        CK(e, cudaStreamSynchronize(e->stream));
+        CK(e, cudaStreamSynchronize(e->copy_stream));
+        for (int k = 0; k < 2; ++k) {
+            if (e->graph[k]) cudaGraphExecDestroy(e->graph[k]);
+            if (e->graph_src[k]) cudaGraphDestroy(e->graph_src[k]);
+            e->graph[k] = nullptr;
+            e->graph_src[k] = nullptr;
+            e->graph_kernels[k] = 0;
+        }
+        free_dev(e->feat_all);
+        free_dev(e->vlarge);
+        free_dev(e->vplain);
+        e->n = n;
+        e->max_n = max_n;
+        e->initialized = false;
+        return MPM_OK;
+    }
     free_particles(e);
     e->n = n;
     e->max_n = max_n;
+    e->cap_n = std::max(n, 1LL);
+    e->cap_max_n = max_n;
+    e->cap_sort = sort_bytes;
     const size_t cap = (size_t)std::max(n, 1LL);
     const size_t ibytes = cap * sizeof(int32_t);
     for (int k = 0; k < 2; ++k) {
