@@ -1230,13 +1230,13 @@ extern "C" mpm_status mpm_step_learned(mpm_engine* e, int32_t nlarge, mpm_learne
                           tc ? e->mlp_tc : nullptr, e->d_flags + 1};
         // The statistic is read back (a host sync per large step) only when
         // it can trigger the fallback.
-        const bool judge = e->mlp_set && e->max_density_change >= 0.f;
+        const bool checked = e->mlp_set && e->max_density_change >= 0.f;
         if (e->mlp_set) CK(e, cudaMemsetAsync(e->d_stat, 0, sizeof(float), e->stream));
         e->kernel_launches += enqueue_large(e, par, &la);
         CK(e, cudaGetLastError());
         e->sort_src = par;
         bool accept = true;
-        if (judge) {
+        if (checked) {
             float sum = 0.f;
             CK(e, cudaMemcpyAsync(&sum, e->d_stat, sizeof(float), cudaMemcpyDeviceToHost, e->stream));
             CK(e, cudaStreamSynchronize(e->stream));
