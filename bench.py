@@ -424,9 +424,9 @@ def run_engine(args, rank, world, local):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism=f"replicas{world}",
-                           tuning=None if tuning is None else
-                           {k: (round(v, 5) if isinstance(v, float) else v) for k, v in tuning.items()}),
+            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism=f"replicas{world}"),
+            "tuning": None if tuning is None else
+                      {k: (round(v, 5) if isinstance(v, float) else v) for k, v in tuning.items()},
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk.summary(), "stage_ms_per_substep": {k: round(v, 5) for k, v in per_sub.items()},
             "impl": "engine"}
@@ -506,8 +506,8 @@ def run_reference(args, rank, world, local):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism="replicas1",
-                           reference_scenes=len(runs)),
+            "config": dict(workload_config(args.workload, cfg, n, len(tris), args.advance), parallelism="replicas1"),
+            "reference_scenes": len(runs),
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                              "sample": f"{args.steps} frames x {sub} Engine::step() of the reference's own CUDA "

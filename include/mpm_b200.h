@@ -371,7 +371,8 @@ mpm_status mpm_sort_particles_device(const float* d_pos_x, const float* d_pos_y,
  * Runs on the calling thread's current device; `stream` must belong to it.
  * The first call on each device looks up the array's device address
  * (cudaGetSymbolAddress) and caches it, so make that first call before any
- * stream capture begins.
+ * stream capture begins.  The cached address assumes the device is not reset
+ * (cudaDeviceReset) while the process runs; after a reset, do not call it.
  * All calls on a device share the one array and nothing clears it between
  * calls (no part of it needs to start at zero).  Calls that overlap on the
  * GPU, on different streams or from different threads, race on it and give

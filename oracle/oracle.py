@@ -142,7 +142,7 @@ class RefEngine:
             ("ref_config_get_float", ctypes.c_float, [ctypes.c_char_p]),
             ("ref_config_entries", I, [I, P, P, I, I]),
             ("ref_engine_create", I, [L, P]), ("ref_engine_init_sdf", I, [P, L]),
-            ("ref_engine_step", I, [I]), ("ref_engine_time_steps", ctypes.c_float, [I]),
+            ("ref_engine_set_state", I, [P]), ("ref_engine_step", I, [I]), ("ref_engine_time_steps", ctypes.c_float, [I]),
             ("ref_engine_get_state", I, [P]), ("ref_engine_get_grid", I, [P]), ("ref_engine_get_sdf", I, [P]),
             ("ref_engine_get_positions", I, [P]), ("ref_engine_get_perm", I, [P]), ("ref_engine_keys", I, [P]),
             ("ref_engine_sort_only", I, []), ("ref_engine_destroy", None, []),
@@ -171,6 +171,12 @@ class RefEngine:
         rc = self.lib.ref_engine_init_sdf(_p(t) if t.size else None, t.size // 9)
         if rc != 0:
             raise RuntimeError(f"reference initSDF failed (rc={rc})")
+
+    def set_state(self, state26):
+        """The particle buffer replaced by `state26` as it is (no initFMatrices)."""
+        st = np.ascontiguousarray(state26, np.float32).reshape(26, -1)
+        assert st.shape[1] == self.n
+        assert self.lib.ref_engine_set_state(_p(st)) == 0
 
     def step(self, nsub=1):
         assert self.lib.ref_engine_step(nsub) == 0

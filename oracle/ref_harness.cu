@@ -175,6 +175,17 @@ int ref_engine_init_sdf(const float* tris, long t) {
     return 0;
 }
 
+// Overwrites the engine's particle buffer (getBuffer, 26 planes of g_n
+// floats) with a state as it is: Engine::init applies initFMatrices
+// (kernels.cu:349-358), which resets F's diagonal, so a state taken after
+// some substeps is loaded through init and then written over with this.
+int ref_engine_set_state(const float* soa26) {
+    if (!g_engine) return -1;
+    return cudaMemcpy(g_engine->getBuffer(), soa26, sizeof(float) * 26 * g_n, cudaMemcpyHostToDevice) == cudaSuccess
+               ? 0
+               : -2;
+}
+
 int ref_engine_step(int nsub) {
     if (!g_engine) return -1;
     for (int i = 0; i < nsub; ++i) g_engine->step();

@@ -10,6 +10,20 @@ for p in (PKG, ROOT, os.path.dirname(os.path.abspath(__file__))):
         sys.path.insert(0, p)
 
 
+def reference_tree():
+    """The reference's source tree (read as text by a few host tests when it
+    is present): $MPM_REF_TREE, else BASELINE.json's `reference_path`."""
+    import json
+    env = os.environ.get("MPM_REF_TREE")
+    if env:
+        return env
+    try:
+        with open(os.path.join(ROOT, "BASELINE.json")) as f:
+            return json.load(f).get("reference_path")
+    except (OSError, ValueError):
+        return None
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs an sm_100 (B200) GPU; run with -m gpu")
 

@@ -110,3 +110,21 @@ def test_cli_usage_and_checkpoint_errors_without_gpu(tmp_path):
     with pytest.raises(mpm_b200.MpmError) as ei:
         mpm_b200.checkpoint_info(str(tmp_path / "x.ckpt"))
     assert "magic" in str(ei.value)
+
+
+def test_scene_generation_maps_no_library():
+    """The package maps libmpm_b200.so on its first library call, not at
+    import: the reference arm of the benchmark builds its scenes with
+    `mpm_b200.scenes` and must run without the engine's code mapped."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, sys.argv[1])\n"
+            "from mpm_b200 import scenes\n"
+            "cfg, st, tris = scenes.small_scene(512, (16, 16, 16), seed=1)\n"
+            "import mpm_b200\n"
+            "assert not mpm_b200.lib.loaded(), 'library mapped by scene generation'\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libmpm_b200' not in maps, 'libmpm_b200.so is mapped'\n")
+    r = subprocess.run([sys.executable, "-c", code, os.path.join(ROOT, "water-sim-cuda_b200")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -12,7 +12,8 @@ BASE = ("SIZE_X=128\nSIZE_Y=128\nSIZE_Z=128\nPADDING=2\nGRAVITY=9.81\nDT=0.01\nG
 def test_reference_config_file(mpm):
     """The reference's own config.txt, values as std::stoi/std::stof read them
     (read as text from the reference tree when it is present)."""
-    path = "/root/reference/config.txt"
+    from conftest import reference_tree
+    path = os.path.join(reference_tree() or "", "config.txt")
     text = open(path).read() if os.path.exists(path) else (
         BASE + "\n\nWATER=models/sphere.obj;15.0;0.0;20.0;25.0\nWATER=models/sphere.obj;15.0;10.0;20.0;25.0\n\n"
         "OBJECT=models/u.obj;110.0;0.0;-10.0;0.0")

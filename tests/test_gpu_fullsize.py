@@ -1,0 +1,136 @@
+"""Per-particle parity at the benchmark scenes' full sizes.
+
+One substep of the sphere drop (113k particles, 64^3) and of the 2M dam break
+(1,989,120 particles, 128^3, torus obstacle) runs in the engine and in the
+reference's own engine (engine.cu/kernels.cu compiled from its sources into
+oracle/_ref) from the same state, and the FP64 oracle restates the same
+substep: keys and sort permutation bit-exact between the two engines; state
+and grid of each engine within the parity tolerances of tests/parity.py
+against FP64 (which also pins the oracle against the reference at full
+size).  The dam break is checked again from a late, crowded state, where most
+of P2G's work runs through the crowded-cell list (cells above 32 particles),
+loaded into the reference engine as it is (no initFMatrices).
+
+Reference: Engine::step (engine.cu:54-70), p2GTransferScatter
+(kernels.cu:6-142), gridUpdate (kernels.cu:144-196), g2PTransfer
+(kernels.cu:199-280), setKeys + thrust::sort_by_key (kernels.cu:361-371,
+engine.cu:92-102).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from parity import assert_normwise, assert_state_close
+
+pytestmark = pytest.mark.gpu
+
+REF_LIB = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "libref_engine.so")
+needs_ref = pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference engine not built")
+
+# The crowded-cell threshold of P2G: a lane sums at most 32 particles of its
+# cell, the rest of the cell goes to the crowded-cell list.
+CELL_CAP = 32
+
+
+@pytest.fixture(scope="module")
+def ref():
+    from oracle.oracle import RefEngine
+    r = RefEngine()
+    yield r
+    r.destroy()
+
+
+def _scene(workload):
+    from mpm_b200 import scenes
+    if workload == "sphere_drop":
+        return scenes.sphere_drop(1234)
+    return scenes.dam_break(1235)
+
+
+def _cell_counts(cfg, state):
+    """Particles per stencil base cell, (int)(pos - 0.5) as P2G takes it."""
+    base = np.trunc(state[0:3].astype(np.float32) - np.float32(0.5)).astype(np.int64)
+    ok = np.all((base >= 0) & (base < np.array([[cfg.size_x], [cfg.size_y], [cfg.size_z]])), axis=0)
+    idx = (base[2] * cfg.size_y + base[1]) * cfg.size_x + base[0]
+    return np.bincount(idx[ok], minlength=cfg.grid_number)
+
+
+def _check(cfg, start, got, grid, r_state, r_grid, want, wgrid):
+    # Both FP32 engines against the FP64 oracle, then against each other.
+    assert_state_close(r_state, want, start)
+    assert_state_close(got, want, start)
+    assert_state_close(got, r_state, start, rtol=2e-5)
+    assert_normwise("grid mass vs FP64", grid[0], wgrid[0])
+    assert_normwise("grid velocity vs FP64", grid[1:4], wgrid[1:4])
+    assert_normwise("grid mass vs reference", grid[0], r_grid[0], rtol=2e-5)
+    assert_normwise("grid velocity vs reference", grid[1:4], r_grid[1:4], rtol=2e-5)
+    total = float(np.sum(start[25], dtype=np.float64))
+    assert float(np.sum(grid[0], dtype=np.float64)) == pytest.approx(total, rel=1e-5)
+
+
+@needs_ref
+@pytest.mark.parametrize("workload", ["sphere_drop", "dam_break_2M"])
+def test_full_scene_substep_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_path, workload):
+    cfg, st, tris = _scene(workload)
+    ref.create(cfg, st, tris, str(tmp_path / "config.txt"))
+    r_start, r_keys, r_sdf = ref.state(), ref.keys(), ref.sdf()
+    ref.step(1)
+    r_state, r_grid, r_perm = ref.state(), ref.grid(), ref.perm()
+    with mpm.Engine(cfg) as eng:
+        eng.init(st)
+        eng.init_sdf(tris)
+        start, sdf = eng.get_buffer(), eng.get_sdf()
+        eng.step(1)
+        keys, perm = eng.get_sort()
+        state, grid = eng.get_buffer(), eng.get_grid()
+    assert np.array_equal(start, r_start), "initial state (initFMatrices) differs from the reference"
+    assert np.array_equal(keys, r_keys), "Morton keys differ from the reference's setKeys"
+    assert np.array_equal(perm, r_perm), "sort permutation differs from the reference's thrust sort"
+    assert np.abs(sdf.astype(np.float64) - r_sdf).max() <= 1e-4, "SDF differs from the reference's makeSDF"
+    want, wgrid, okeys, operm = oracle64.substep(cfg, r_start.astype(np.float64), r_sdf.astype(np.float64))
+    assert np.array_equal(okeys, r_keys) and np.array_equal(operm, r_perm)
+    _check(cfg, r_start, state, grid, r_state, r_grid, want, wgrid)
+
+
+@needs_ref
+def test_dam_break_crowded_state_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_path):
+    """The 2M dam break advanced 2400 substeps in chunks of 200 (this GAMMA = 7
+    Tait law resists only expansion, so the fluid piles up against the top
+    wall); from the chunk end with the most particles in cells above 32, one
+    substep in both engines."""
+    cfg, st, tris = _scene("dam_break_2M")
+    best, best_frac, best_at, fullest = None, -1.0, 0, 0
+    with mpm.Engine(cfg) as eng:
+        eng.init(st)
+        eng.init_sdf(tris)
+        for done in range(200, 2401, 200):
+            eng.step(200)
+            s = eng.get_buffer()
+            counts = _cell_counts(cfg, s)
+            frac = float(counts[counts > CELL_CAP].sum()) / s.shape[1]
+            if frac > best_frac:
+                best, best_frac, best_at, fullest = s, frac, done, int(counts.max())
+    print(f"crowded state: substep {best_at}, {best_frac:.3f} of particles in cells above {CELL_CAP}, "
+          f"fullest cell {fullest}")
+    assert best_frac >= 0.05, f"no crowded state: at most {best_frac:.3f} of the particles in cells above 32"
+    late = best
+    with mpm.Engine(cfg) as eng:
+        eng.init(late)  # applies initFMatrices; set_state then loads the state as it is
+        eng.init_sdf(tris)
+        eng.set_state(late)
+        assert np.array_equal(eng.get_buffer(), late)
+        eng.step(1)
+        keys, perm = eng.get_sort()
+        state, grid = eng.get_buffer(), eng.get_grid()
+    ref.create(cfg, late, tris, str(tmp_path / "config.txt"))
+    ref.set_state(late)
+    assert np.array_equal(ref.state(), late)
+    r_keys, r_sdf = ref.keys(), ref.sdf()
+    ref.step(1)
+    r_state, r_grid, r_perm = ref.state(), ref.grid(), ref.perm()
+    assert np.array_equal(keys, r_keys), "Morton keys differ from the reference's setKeys"
+    assert np.array_equal(perm, r_perm), "sort permutation differs from the reference's thrust sort"
+    want, wgrid, _, _ = oracle64.substep(cfg, late.astype(np.float64), r_sdf.astype(np.float64))
+    _check(cfg, late, state, grid, r_state, r_grid, want, wgrid)

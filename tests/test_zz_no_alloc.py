@@ -49,6 +49,26 @@ def test_static_sort_matches_allocating_sort_twice(gpu_ok, mpm):
         assert np.array_equal(np.sort(p_st), np.arange(n, dtype=np.int32))
 
 
+def test_static_sort_allocates_nothing(gpu_ok, mpm):
+    """After a first call (which may load the module), a static sort leaves
+    the device's free memory unchanged."""
+    import torch
+    rng = np.random.default_rng(7)
+    n = 300_000
+    d = torch.from_numpy(np.ascontiguousarray(_positions(n, rng))).cuda()
+    keys = torch.empty(n, dtype=torch.int32, device="cuda")
+    perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    args = (d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), n, keys.data_ptr(), perm.data_ptr(), stream)
+    mpm.sort_particles_device_static(*args)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        mpm.sort_particles_device_static(*args)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_static_sort_rejects_oversize(gpu_ok, mpm):
     n = mpm.SORT_STATIC_MAX_PARTICLES + 1
     with pytest.raises(mpm.MpmError) as ei:

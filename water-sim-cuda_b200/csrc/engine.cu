@@ -194,6 +194,14 @@ void free_dev(T*& p) {
     p = nullptr;
 }
 
+// Buffers of the learned large step, sized by the particle count; allocated
+// when first needed after an init.
+void free_learned_buffers(mpm_engine* e) {
+    free_dev(e->feat_all);
+    free_dev(e->vlarge);
+    free_dev(e->vplain);
+}
+
 void free_particles(mpm_engine* e) {
     for (int k = 0; k < 2; ++k) {
         free_dev(e->P[k]);
@@ -213,9 +221,11 @@ void free_particles(mpm_engine* e) {
     free_dev(e->sort_mem);
     free_dev(e->pos_buf[0]);
     free_dev(e->pos_buf[1]);
-    free_dev(e->feat_all);
-    free_dev(e->vlarge);
-    free_dev(e->vplain);
+    free_learned_buffers(e);
+    // No buffer is left: the reuse test in alloc_particles must fail.
+    e->cap_n = 0;
+    e->cap_max_n = 0;
+    e->cap_sort = 0;
     e->initialized = false;
 }
 
@@ -229,7 +239,7 @@ mpm_status ensure_staging(mpm_engine* e, size_t bytes) {
 }
 
 mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_bytes) {
-    if (e->P[0] && n <= e->cap_n && max_n <= e->cap_max_n && sort_bytes <= e->cap_sort) {
+    if (e->cap_n > 0 && n <= e->cap_n && max_n <= e->cap_max_n && sort_bytes <= e->cap_sort) {
         // The buffers of an earlier init are large enough: keep them (freeing
         // and allocating half a gigabyte takes from a few to hundreds of
         // milliseconds).  The substep graphs are captured again by the caller;
@@ -245,20 +255,15 @@ mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_by
             e->graph_src[k] = nullptr;
             e->graph_kernels[k] = 0;
         }
-        free_dev(e->feat_all);
-        free_dev(e->vlarge);
-        free_dev(e->vplain);
+        free_learned_buffers(e);
         e->n = n;
         e->max_n = max_n;
         e->initialized = false;
         return MPM_OK;
     }
-    free_particles(e);
+    free_particles(e);  // also zeroes the recorded capacities
     e->n = n;
     e->max_n = max_n;
-    e->cap_n = std::max(n, 1LL);
-    e->cap_max_n = max_n;
-    e->cap_sort = sort_bytes;
     const size_t cap = (size_t)std::max(n, 1LL);
     const size_t ibytes = cap * sizeof(int32_t);
     for (int k = 0; k < 2; ++k) {
@@ -279,6 +284,11 @@ mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_by
     CK(e, cudaMalloc(&e->sort_mem, sort_bytes));
     CK(e, cudaMalloc(&e->pos_buf[0], cap * 3 * sizeof(float)));
     CK(e, cudaMalloc(&e->pos_buf[1], cap * 3 * sizeof(float)));
+    // Recorded only now: after a failed allocation above the capacities stay
+    // zero, so the next init allocates again instead of reusing null buffers.
+    e->cap_n = std::max(n, 1LL);
+    e->cap_max_n = max_n;
+    e->cap_sort = sort_bytes;
     return MPM_OK;
 }
 

@@ -14,7 +14,10 @@
 // resident until the process exits.  Host code cannot pass the array's name
 // to a kernel (on the host it names a stand-in object, not device memory),
 // so the first call on each device looks up its device address with
-// cudaGetSymbolAddress, with that device current, and caches it.
+// cudaGetSymbolAddress, with that device current, and caches it.  The cache
+// assumes the device's primary context lives as long as the process: after a
+// cudaDeviceReset the module is loaded again at another address, and a
+// process that resets a device must not call this entry point afterwards.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -4,8 +4,10 @@ The class `Engine` mirrors the reference's C++ `Engine` (engine.h:14-43):
 `init(n, buffer)`, `step()`, `init_sdf(triangles)`, `get_buffer()`,
 `get_positions()`, `get_grid()`, `get_number()`, and `sort_particles()`;
 `parse_config_file` mirrors GameConfigData (game_configdata.cpp:22-90).
-Every call goes through libmpm_b200.so.  There is no CPU fallback: importing
-this module without the built library raises.
+Every call goes through libmpm_b200.so.  There is no CPU fallback: the first
+call into the library raises when it has not been built.  The library is
+mapped on that first call, not at import, so that code which only needs the
+pure-numpy parts (`Config`, `scenes`) maps no GPU code.
 """
 from __future__ import annotations
 
@@ -235,7 +237,23 @@ def _load() -> ctypes.CDLL:
     return lib
 
 
-lib = _load()
+class _LazyLib:
+    """libmpm_b200.so, loaded (and its signatures set) on the first attribute
+    access; raises RuntimeError there if the library is missing."""
+
+    _cdll = None
+
+    def __getattr__(self, name):
+        if _LazyLib._cdll is None:
+            _LazyLib._cdll = _load()
+        return getattr(_LazyLib._cdll, name)
+
+    @staticmethod
+    def loaded() -> bool:
+        return _LazyLib._cdll is not None
+
+
+lib = _LazyLib()
 
 
 def _ptr(a: np.ndarray) -> ctypes.c_void_p:
