@@ -51,6 +51,8 @@ METRIC = "particle-substeps/s at 2M pcl, 128^3; learned 4xDT vs plain at <=2% de
 UNIT = "particle-substeps/s"
 FALLBACK_HBM_GBS = 6650.0
 SEEDS = {"dam_break_2M": 1235, "dam_break_5M": 1235, "sphere_drop": 1234, "scale_256": 1236, "batched_64": 1237}
+# Frames (steps of SUBSTEPS substeps) of each workload's whole run.
+WHOLE_RUN = {"dam_break_2M": 1000, "dam_break_5M": 1000, "sphere_drop": 500, "scale_256": 200, "batched_64": 300}
 # Algorithmic bytes per unit (FP32 reference state): per particle and per grid
 # node of each stage, from the hot-path scope table of this project.
 ALGO_BYTES = {"sort": (16, 0), "p2g": (108, 16), "grid": (0, 48), "g2p": (148, 12)}
@@ -70,6 +72,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--advance", type=int, default=0,
                     help="substeps simulated before the warm-up, to measure a later state of the scene")
+    ap.add_argument("--no-whole-run", action="store_true",
+                    help="skip the leg that times the workload's whole run from its initial state")
     return ap.parse_args(argv)
 
 
@@ -218,6 +222,55 @@ def load_traffic(kernel: str, workload: str):
         return None
 
 
+def kernel_rooflines(per_sub, n, g_active, peak, peak_kind):
+    """Achieved HBM bandwidth of each stage from its average time per substep
+    and its algorithmic bytes (ALGO_BYTES), as a fraction of the peak."""
+    out = {}
+    for k, (bpp, bpn) in ALGO_BYTES.items():
+        if per_sub.get(k, 0) <= 0:
+            continue
+        algo = bpp * n + bpn * g_active
+        ach = algo / (per_sub[k] / 1e3) / 1e9
+        out[k] = {"ms": round(per_sub[k], 5), "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4),
+                  "algorithmic_bytes": algo}
+    out["peak_gbs"] = peak
+    out["peak_source"] = f"hbm_gbs of {peak_kind}"
+    return out
+
+
+def whole_run_leg(eng, st0, frames, sub, n, cfg, stream):
+    """The workload's whole run (`frames` frames) from its initial state st0:
+    device time on the engine's stream, then the same frames again with
+    stage events for the per-stage times."""
+    import numpy as np
+    import torch
+    eng.set_state(st0)
+    eng.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(frames):
+        eng.step_async(sub)
+    e1.record(stream)
+    eng.synchronize()
+    ms = e0.elapsed_time(e1)
+    g_end = int(np.count_nonzero(eng.get_grid()[0] > 0))
+    eng.set_state(st0)
+    eng.set_stage_timing(frames * sub)
+    for _ in range(frames):
+        eng.step_async(sub)
+    stage_ms, cnt = eng.stage_times()
+    eng.set_stage_timing(0)
+    per_sub = {k: v / max(cnt, 1) for k, v in stage_ms.items()}
+    peak, peak_kind = load_peaks()
+    return {"frames": frames, "substeps": frames * sub, "value": n * sub * frames / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / frames,
+            "stage_ms_per_substep": {k: round(v, 5) for k, v in per_sub.items()},
+            "roofline_by_kernel": kernel_rooflines(per_sub, n, g_end, peak, peak_kind),
+            "active_nodes_at_end": g_end,
+            "note": "from the initial state over the workload's whole run; node terms use the active nodes at "
+                    "the end of the run"}
+
+
 # -------------------------------------------------------------- CPU leg ----
 CPU_SNIPPET = r"""
 import json, os, sys, time
@@ -234,9 +287,18 @@ while True:
     st = o.substep(cfg, st, sdf)[0]
     done += 1
     el = time.perf_counter() - t0
-    if el >= budget or done >= 16:
+    if el >= budget:
         break
-print(json.dumps({"substeps": done, "seconds": el, "n": int(st.shape[1]), "threads": o.threads()}))
+model = ""
+try:
+    for line in open("/proc/cpuinfo"):
+        if line.startswith("model name"):
+            model = line.split(":", 1)[1].strip()
+            break
+except OSError:
+    pass
+print(json.dumps({"substeps": done, "seconds": el, "n": int(st.shape[1]), "threads": o.threads(),
+                  "cpu_model": model, "logical_cpus": os.cpu_count()}))
 """
 
 
@@ -258,8 +320,10 @@ def cpu_baseline(workload: str, seconds: float, sdf):
         return {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": "failed: " + r.stderr[-300:]}
     d = json.loads(r.stdout.strip().splitlines()[-1])
     return {"value": d["n"] * d["substeps"] / d["seconds"], "unit": UNIT, "cores": d["threads"], "kind": "port",
-            "sample": f"{d['substeps']} substeps of the full {d['n']}-particle scene (SDF build excluded), "
-                      f"FP32 OpenMP restatement of Engine::step, {d['seconds']:.1f} s"}
+            "cpu_model": d["cpu_model"], "logical_cpus": d["logical_cpus"],
+            "sample": f"{d['substeps']} substeps of the full {d['n']}-particle scene from its initial state (SDF "
+                      f"build excluded), FP32 OpenMP restatement of Engine::step on {d['threads']} threads, "
+                      f"{d['seconds']:.1f} s"}
 
 
 # ----------------------------------------------------------- engine arm ----
@@ -294,6 +358,7 @@ def run_engine(args, rank, world, local):
         eng = mpm_b200.Engine(cfg, device=local)
         eng.init(st)
         eng.init_sdf(tris)
+    st0 = None if batched else eng.get_buffer()  # the initial state (initFMatrices applied)
     if args.advance > 0:
         eng.step(args.advance)
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
@@ -355,6 +420,10 @@ def run_engine(args, rank, world, local):
             "traffic": load_traffic(dom, args.workload),
             "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(per_sub[dom], 5),
             "units": f"{bpp} B x {n} particles + {bpn} B x {g_active} active nodes (dense grid {g_dense})"}
+    by_kernel = kernel_rooflines(per_sub, n, g_active, peak, peak_kind)
+    whole = None
+    if not batched and not args.no_whole_run and world == 1:
+        whole = whole_run_leg(eng, st0, WHOLE_RUN[args.workload], sub, n, cfg, stream)
 
     # End to end through the C ABI with host buffers (pinned).
     e2e = None
@@ -429,6 +498,7 @@ def run_engine(args, rank, world, local):
                       {k: (round(v, 5) if isinstance(v, float) else v) for k, v in tuning.items()},
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk.summary(), "stage_ms_per_substep": {k: round(v, 5) for k, v in per_sub.items()},
+            "roofline_by_kernel": by_kernel, "whole_run": whole,
             "impl": "engine"}
     if learned is not None:
         line["learned"] = learned

@@ -220,6 +220,28 @@ mpm_status mpm_substep_partial(mpm_engine* engine, int32_t upto);
  * like the reference, the step never fails on state contents. */
 mpm_status mpm_set_checks(mpm_engine* engine, uint32_t flags);
 
+/* Test hooks of the bounded device-side waits (failure detection without a
+ * GPU fault).  Every mbarrier wait of the SDF build's triangle copies and of
+ * the learned step's tcgen05 MMAs has a time limit; when it runs out the
+ * kernel drains what it has in flight, records a status bit, frees its TMEM
+ * and returns, and the call fails with MPM_ERR_TIMEOUT while the context stays
+ * usable.  These flags make the first such wait of the next mpm_init_sdf /
+ * mpm_scene_init_sdf (SDF_*) or mpm_step_learned on tcgen05 (MMA_*) give up,
+ * always after the real completion has been observed, so that nothing is in
+ * flight when it does:
+ *   *_GIVE_UP  reports the give-up at once;
+ *   *_EXPIRE   then waits for the barrier's next phase, which nothing
+ *              completes, until a 20 ms limit really runs out.
+ * The outputs of a call that failed this way are unspecified (an SDF left
+ * unbuilt, a large step without its correction); the engine is usable for
+ * the next call.  0 (the default) clears the hooks.  No counterpart in the
+ * reference, which has no bounded waits. */
+#define MPM_WAIT_TEST_SDF_GIVE_UP 0x1u
+#define MPM_WAIT_TEST_SDF_EXPIRE 0x2u
+#define MPM_WAIT_TEST_MMA_GIVE_UP 0x4u
+#define MPM_WAIT_TEST_MMA_EXPIRE 0x8u
+mpm_status mpm_set_wait_test(mpm_engine* engine, uint32_t flags);
+
 /* ------------------------------------------------------------------ */
 /* Readback                                                             */
 /* ------------------------------------------------------------------ */
@@ -537,10 +559,9 @@ mpm_status mpm_get_tuning(mpm_engine* engine, mpm_tuning* tuning);
  * (3), interpolated grid mass over the seeding density, minus 1 (1), and the
  * obstacle SDF folded into one vector n * phi * max(0, 1 - |phi| / 4) (3), all
  * gathered from the large step's grid at the particle's start position.
- * The plain substep is the fallback and the yardstick: a large step whose mean
- * predicted relative density change, mean over particles of
- * |1 / det(I + RATIO DT C) - 1|, exceeds max_density_change is undone and
- * replaced by RATIO plain substeps.  Engines of one scene only. */
+ * The plain substep is the fallback and the yardstick: a large step whose
+ * fallback statistic (mpm_set_fallback_rule) exceeds max_density_change is
+ * undone and replaced by RATIO plain substeps.  Engines of one scene only. */
 #define MPM_CORRECTOR_PARAMS 5478   /* fp32 parameter vector, layout below */
 #define MPM_CORRECTOR_FEATURES 16
 #define MPM_CORRECTOR_OUTPUTS 3
@@ -570,6 +591,26 @@ mpm_status mpm_set_corrector(mpm_engine* engine, const float* params_host, int32
 mpm_status mpm_set_corrector_kernel(mpm_engine* engine, int32_t kind);
 /* nlarge large steps (each RATIO x DT of simulated time); stats optional. */
 mpm_status mpm_step_learned(mpm_engine* engine, int32_t nlarge, mpm_learned_stats* stats);
+/* The fallback statistic, a mean over particles computed by the large step's
+ * G2P from the step's own grid (J = det(I + RATIO DT C) the predicted volume
+ * change, rho / rho0 the interpolated grid mass over the seeding density):
+ *   MPM_FALLBACK_DENSITY_CHANGE       |1 / J - 1|: the density change the
+ *                                     step predicts (default);
+ *   MPM_FALLBACK_REST_DENSITY         |rho / rho0 / J - 1|: how far the
+ *                                     predicted density lies from rest
+ *                                     density (free-surface particles, with
+ *                                     part of their stencil empty, count too);
+ *   MPM_FALLBACK_REST_DENSITY_EXCESS  the mean above minus the mean of
+ *                                     |rho / rho0 - 1| before the step: how
+ *                                     much the step moves the density away
+ *                                     from rest. */
+#define MPM_FALLBACK_DENSITY_CHANGE 0
+#define MPM_FALLBACK_REST_DENSITY 1
+#define MPM_FALLBACK_REST_DENSITY_EXCESS 2
+mpm_status mpm_set_fallback_rule(mpm_engine* engine, int32_t rule);
+/* The three means above (in that order: |1/J - 1|, |rho/rho0/J - 1|,
+ * |rho/rho0 - 1|) of the last large step that was checked. */
+mpm_status mpm_learned_statistics(mpm_engine* engine, double* out3);
 
 /* Training data and training.  A corrector holds a dataset of (features,
  * target) pairs on the device and the parameters with their Adam state. */

@@ -136,3 +136,67 @@ def test_two_engines_one_process(gpu_ok, mpm):
         b.step(2)
         assert a.get_number() == b.get_number() == 2000
         assert not np.array_equal(a.get_buffer(), b.get_buffer())
+
+
+# Bounded device waits.  The test hooks make the first wait of the SDF build
+# (triangle tile copies) or of the learned step's tcgen05 MMAs give up, only
+# after the real completion has been observed: *_GIVE_UP reports it at once,
+# *_EXPIRE waits for a barrier phase that nothing completes until the 20 ms
+# limit really runs out.  Nothing is in flight when the CTAs give up, free
+# their TMEM and return, so the GPU context stays usable.
+@pytest.mark.parametrize("hook", ["WAIT_TEST_SDF_GIVE_UP", "WAIT_TEST_SDF_EXPIRE"])
+def test_sdf_wait_gives_up_and_engine_recovers(gpu_ok, mpm, oracle64, hook):
+    from mpm_b200 import scenes
+    cfg, st, _ = scenes.small_scene(2000, (32, 32, 32), seed=3)
+    # Two tiles of triangles (the kernel streams 256 per tile).
+    tris = np.concatenate([scenes.torus(8.0, 3.0, (16.2, 15.7, 16.1), 24, 12),
+                           scenes.uv_sphere(4.0, (8.3, 9.1, 22.4), 16, 8)])
+    assert len(tris) > 256
+    with mpm.Engine(cfg) as eng:
+        eng.init(st)
+        eng.set_wait_test(getattr(mpm, hook))
+        with pytest.raises(mpm.MpmError) as ei:
+            eng.init_sdf(tris)
+        assert ei.value.name == "MPM_ERR_TIMEOUT"
+        eng.set_wait_test(0)
+        eng.init_sdf(tris)  # the next call succeeds
+        sdf = eng.get_sdf()
+        want, _ = oracle64.make_sdf(cfg, tris)
+        assert np.abs(sdf.astype(np.float64) - want).max() <= 1e-4
+        eng.step(2)
+
+
+@pytest.mark.parametrize("hook", ["WAIT_TEST_MMA_GIVE_UP", "WAIT_TEST_MMA_EXPIRE"])
+def test_tcgen05_wait_gives_up_and_engine_recovers(gpu_ok, mpm, hook):
+    from mpm_b200 import learned
+    from mpm_b200 import scenes
+    cfg, st, tris = scenes.small_scene(4096, (32, 32, 32), seed=11)
+    params, _ = learned.load_params(learned.PHYSICAL_PARAMS)
+    with mpm.Engine(cfg) as ref_eng:
+        ref_eng.init(st)
+        ref_eng.init_sdf(tris)
+        ref_eng.set_corrector(params, ratio=4, max_density_change=-1.0)
+        ref_eng.step_learned(1)
+        want = ref_eng.get_buffer()
+    with mpm.Engine(cfg) as eng:
+        eng.init(st)
+        eng.init_sdf(tris)
+        eng.set_corrector(params, ratio=4, max_density_change=-1.0)
+        eng.set_wait_test(getattr(mpm, hook))
+        with pytest.raises(mpm.MpmError) as ei:
+            eng.step_learned(1)
+        assert ei.value.name == "MPM_ERR_TIMEOUT"
+        eng.set_wait_test(0)
+        eng.init(st)  # the failed step's state is unspecified: start again
+        eng.step_learned(1)
+        got = eng.get_buffer()
+    assert np.abs(got.astype(np.float64) - want).max() <= 1e-4 * max(1.0, np.abs(want).max())
+
+
+def test_wait_test_rejects_unknown_flags(gpu_ok, mpm):
+    cfg, st, tris = _small()
+    with mpm.Engine(cfg) as eng:
+        eng.init(st)
+        with pytest.raises(mpm.MpmError) as ei:
+            eng.set_wait_test(0x100)
+        assert ei.value.name == "MPM_ERR_INVALID_ARGUMENT"

@@ -45,6 +45,7 @@ struct MlpTcSmem {
     unsigned long long mbar;
     uint32_t tmem;
     uint32_t failed;
+    uint32_t wait_test;  // test hooks for the first layer's wait (kWaitTest*)
 };
 constexpr int kTcThreads = 256;
 constexpr int kTcTmemCols = 128;  // two tiles x 64 fp32 columns
@@ -95,11 +96,30 @@ __device__ __forceinline__ void mbar_init(void* mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
 }
 
-// Waits for phase `parity` of the mbarrier with an iteration limit; false if
+__device__ __forceinline__ unsigned long long tc_globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Limits of the bounded MMA waits: a commit normally lands within
+// microseconds; the test hook's expiring wait (below) gives up after 20 ms.
+constexpr unsigned long long kMmaWaitNs = 1000000000ull;
+constexpr unsigned long long kTestWaitNs = 20000000ull;
+
+// Test hooks of the bounded waits (mpm_set_wait_test), acted on only after
+// the real completion has been observed, so that no MMA or copy is in flight
+// when the caller gives up: kWaitTestGiveUp reports a give-up at once;
+// kWaitTestExpire waits for the barrier's next phase, which nothing
+// completes, until the short limit really runs out.
+enum : uint32_t { kWaitTestGiveUp = 1u, kWaitTestExpire = 2u };
+
+// Waits for phase `parity` of the mbarrier for at most limit_ns; false if
 // it gave up.
-__device__ __forceinline__ bool mbar_wait(void* mbar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(void* mbar, uint32_t parity, unsigned long long limit_ns = kMmaWaitNs) {
     const uint32_t addr = smem_u32(mbar);
-    for (int i = 0; i < (1 << 20); ++i) {
+    unsigned long long t0 = 0;
+    for (int i = 0;; ++i) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -107,8 +127,22 @@ __device__ __forceinline__ bool mbar_wait(void* mbar, uint32_t parity) {
             : "r"(addr), "r"(parity)
             : "memory");
         if (done) return true;
+        if (i == 0) t0 = tc_globaltimer_ns();
+        else if (tc_globaltimer_ns() - t0 > limit_ns) return false;
     }
-    return false;
+}
+
+// Waits for the commit of phase `parity`.  If the wait gives up, waits once
+// more (bounded) so that the committed MMAs have finished before the caller
+// frees its TMEM columns, and returns false.  wait_test: the test hooks above.
+__device__ __forceinline__ bool mma_wait_checked(void* mbar, uint32_t parity, uint32_t wait_test) {
+    if (!mbar_wait(mbar, parity)) {
+        mbar_wait(mbar, parity);  // drain
+        return false;
+    }
+    if (wait_test & kWaitTestGiveUp) return false;
+    if (wait_test & kWaitTestExpire) return mbar_wait(mbar, parity ^ 1u, kTestWaitNs);
+    return true;
 }
 
 // 16 consecutive fp32 columns of this thread's TMEM lane.
@@ -126,8 +160,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 // Allocates kTcTmemCols TMEM columns (warp 0) and initialises the mbarrier;
-// every thread of the CTA calls it.
-__device__ __forceinline__ void mlp_tc_begin(MlpTcSmem& s) {
+// every thread of the CTA calls it.  wait_test: test hooks (kWaitTest*) for
+// the first layer's wait.
+__device__ __forceinline__ void mlp_tc_begin(MlpTcSmem& s, uint32_t wait_test = 0u) {
     if (threadIdx.x < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem)),
                      "r"(kTcTmemCols)
@@ -137,6 +172,7 @@ __device__ __forceinline__ void mlp_tc_begin(MlpTcSmem& s) {
     if (threadIdx.x == 0) {
         mbar_init(&s.mbar, 1);
         s.failed = 0u;
+        s.wait_test = wait_test;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -157,8 +193,10 @@ __device__ __forceinline__ void mlp_tc_end(MlpTcSmem& s) {
 
 // One layer: thread 0 issues D[tile] = A[tile] * B^T for both tiles (K / 16
 // MMAs each) and commits; everyone waits for `parity`.  Returns false if the
-// wait gave up (the caller stops using TMEM).
-__device__ __forceinline__ bool mlp_tc_layer(MlpTcSmem& s, const __nv_bfloat16* b, int n, int k, uint32_t parity) {
+// wait gave up (the caller stops using TMEM; the MMAs have been drained).
+// `first`: the layer to which the test hooks apply.
+__device__ __forceinline__ bool mlp_tc_layer(MlpTcSmem& s, const __nv_bfloat16* b, int n, int k, uint32_t parity,
+                                             bool first = false) {
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -180,7 +218,7 @@ __device__ __forceinline__ bool mlp_tc_layer(MlpTcSmem& s, const __nv_bfloat16* 
     }
     // A wait that gives up is recorded and turned into a CTA-wide decision,
     // so every thread takes the same path through the barriers that follow.
-    if (!mbar_wait(&s.mbar, parity)) atomicOr(&s.failed, 1u);
+    if (!mma_wait_checked(&s.mbar, parity, first ? s.wait_test : 0u)) atomicOr(&s.failed, 1u);
     __syncthreads();
     tc_fence_after();
     return s.failed == 0u;
@@ -225,7 +263,7 @@ __device__ __forceinline__ void mlp_forward_tc(MlpTcSmem& s, const float (&x)[kM
             *reinterpret_cast<__nv_bfloat162*>(a + canon_index(r, i, 16)) = __floats2bfloat162_rn(u0, u1);
         }
     }
-    if (!mlp_tc_layer(s, s.w.w1, 64, 16, 0)) return;
+    if (!mlp_tc_layer(s, s.w.w1, 64, 16, 0, true)) return;
     mlp_tc_hidden(s, s.w.b1);
     if (!mlp_tc_layer(s, s.w.w2, 64, 64, 1)) return;
     mlp_tc_hidden(s, s.w.b2);

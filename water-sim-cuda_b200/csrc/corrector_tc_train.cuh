@@ -88,10 +88,11 @@ __device__ __forceinline__ void mlp_tr_publish() {
     tc_fence_after();
 }
 
-// Waits for the commit of phase `phase` (bounded).  A wait that gives up is
-// recorded and turned into a CTA-wide outcome.
+// Waits for the commit of phase `phase` (bounded; a wait that gives up
+// drains the committed MMAs first).  A give-up is recorded and turned into a
+// CTA-wide outcome.
 __device__ __forceinline__ bool mlp_tr_wait(MlpTrainSmem& s, uint32_t& phase) {
-    if (!mbar_wait(&s.mbar, phase)) atomicOr(&s.failed, 1u);
+    if (!mma_wait_checked(&s.mbar, phase, 0u)) atomicOr(&s.failed, 1u);
     phase ^= 1u;
     __syncthreads();
     tc_fence_after();

@@ -115,6 +115,7 @@ struct mpm_engine {
     int scan_chunks = 1;
     uint32_t* ctl = nullptr;
     uint32_t* d_flags = nullptr;  // [0] health bits, [1] kernel status bits
+    uint32_t wait_test = 0;       // MPM_WAIT_TEST_* (test hooks of the bounded device waits)
 
     float* staging = nullptr;  // device staging for imports/exports
     size_t staging_bytes = 0;
@@ -162,6 +163,8 @@ struct mpm_engine {
     int64_t large_steps = 0;
     int64_t fallbacks = 0;
     double last_density_change = 0.0;
+    int fallback_rule = MPM_FALLBACK_DENSITY_CHANGE;
+    double last_stats[3] = {0.0, 0.0, 0.0};  // the three means of the last checked large step
 
     // Launch shapes of the substep (mpm_autotune / mpm_set_tuning).
     mpm_tuning tune{12, 256, 256, 0.f, 0.f, 0.f, 0};
@@ -702,7 +705,7 @@ SimParams large_params(const mpm_engine* e, int s) {
 mpm_status prepare_large(mpm_engine* e) {
     if (!e->d_prm_large) {
         CK(e, cudaMalloc(&e->d_prm_large, e->scenes * sizeof(SimParams)));
-        CK(e, cudaMalloc(&e->d_stat, sizeof(float)));
+        CK(e, cudaMalloc(&e->d_stat, 3 * sizeof(float)));
     }
     std::vector<SimParams> big(e->scenes);
     for (int s = 0; s < e->scenes; ++s) big[s] = large_params(e, s);
@@ -901,12 +904,23 @@ extern "C" mpm_status mpm_scene_init_sdf(mpm_engine* e, int32_t scene, const flo
     cudaError_t err = cudaMemsetAsync(d_tris, 0, align_up(bytes, 16) + 16, e->stream);
     if (err == cudaSuccess) err = cudaMemcpyAsync(d_tris, tris, bytes, cudaMemcpyHostToDevice, e->stream);
     if (err == cudaSuccess) {
-        e->kernel_launches += mpm::launch_sdf_build(p, d_tris, (int)t, sdf, e->d_flags + 1, e->stream);
+        e->kernel_launches += mpm::launch_sdf_build(p, d_tris, (int)t, sdf, e->d_flags + 1, e->stream,
+                                                    e->wait_test & (MPM_WAIT_TEST_SDF_GIVE_UP | MPM_WAIT_TEST_SDF_EXPIRE));
         err = cudaGetLastError();
     }
     const mpm_status s2 = err != cudaSuccess ? cuda_fail(e, err, "sdf build") : sync_and_collect(e);
     cudaFree(d_tris);
     return s2;
+}
+
+extern "C" mpm_status mpm_set_wait_test(mpm_engine* e, uint32_t flags) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (flags & ~(uint32_t)(MPM_WAIT_TEST_SDF_GIVE_UP | MPM_WAIT_TEST_SDF_EXPIRE | MPM_WAIT_TEST_MMA_GIVE_UP |
+                            MPM_WAIT_TEST_MMA_EXPIRE))
+        return record(e, MPM_ERR_INVALID_ARGUMENT, "unknown wait-test flag");
+    e->wait_test = flags;
+    return MPM_OK;
 }
 
 extern "C" mpm_status mpm_init_sdf(mpm_engine* e, const float* tris, int64_t t) {
@@ -1237,21 +1251,27 @@ extern "C" mpm_status mpm_step_learned(mpm_engine* e, int32_t nlarge, mpm_learne
         const int par = e->parity;
         const bool tc = e->mlp_set && e->corrector_kernel == MPM_CORRECTOR_TCGEN05;
         mpm::LearnArgs la{e->mlp_set ? e->mlp : nullptr, nullptr, nullptr, e->d_stat, large_blend(e),
-                          tc ? e->mlp_tc : nullptr, e->d_flags + 1};
+                          tc ? e->mlp_tc : nullptr, e->d_flags + 1,
+                          (e->wait_test & (MPM_WAIT_TEST_MMA_GIVE_UP | MPM_WAIT_TEST_MMA_EXPIRE)) >> 2};
         // The statistic is read back (a host sync per large step) only when
         // it can trigger the fallback.
         const bool checked = e->mlp_set && e->max_density_change >= 0.f;
-        if (e->mlp_set) CK(e, cudaMemsetAsync(e->d_stat, 0, sizeof(float), e->stream));
+        if (e->mlp_set) CK(e, cudaMemsetAsync(e->d_stat, 0, 3 * sizeof(float), e->stream));
         e->kernel_launches += enqueue_large(e, par, &la);
         CK(e, cudaGetLastError());
         e->sort_src = par;
         bool accept = true;
         if (checked) {
-            float sum = 0.f;
-            CK(e, cudaMemcpyAsync(&sum, e->d_stat, sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+            float sum[3] = {0.f, 0.f, 0.f};
+            CK(e, cudaMemcpyAsync(sum, e->d_stat, sizeof(sum), cudaMemcpyDeviceToHost, e->stream));
             CK(e, cudaStreamSynchronize(e->stream));
-            e->last_density_change = e->n > 0 ? (double)sum / (double)e->n : 0.0;
-            accept = e->last_density_change <= e->max_density_change;
+            for (int q = 0; q < 3; ++q) e->last_stats[q] = e->n > 0 ? (double)sum[q] / (double)e->n : 0.0;
+            // The statistic the rule compares with max_density_change.
+            double stat = e->last_stats[0];
+            if (e->fallback_rule == MPM_FALLBACK_REST_DENSITY) stat = e->last_stats[1];
+            if (e->fallback_rule == MPM_FALLBACK_REST_DENSITY_EXCESS) stat = e->last_stats[1] - e->last_stats[2];
+            e->last_density_change = stat;
+            accept = stat <= e->max_density_change;
         }
         if (accept) {
             e->parity = 1 - par;
@@ -1288,7 +1308,7 @@ extern "C" mpm_status mpm_corrector_collect(mpm_corrector* c, mpm_engine* e, int
     // The uncorrected large step, recording features and final velocities;
     // then back to its start state for RATIO plain substeps.
     const int par = e->parity;
-    mpm::LearnArgs la{nullptr, e->feat_all, e->vlarge, nullptr, large_blend(e), nullptr, nullptr};
+    mpm::LearnArgs la{nullptr, e->feat_all, e->vlarge, nullptr, large_blend(e), nullptr, nullptr, 0u};
     e->kernel_launches += enqueue_large(e, par, &la);
     CK(e, cudaGetLastError());
     if ((s = rebin(e, par)) != MPM_OK) return s;
@@ -1628,6 +1648,24 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
     if (s != MPM_OK) return s;
     if ((s = capture_graphs(e)) != MPM_OK) return s;
     if (out) *out = best;
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_set_fallback_rule(mpm_engine* e, int32_t rule) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (rule != MPM_FALLBACK_DENSITY_CHANGE && rule != MPM_FALLBACK_REST_DENSITY &&
+        rule != MPM_FALLBACK_REST_DENSITY_EXCESS)
+        return record(e, MPM_ERR_INVALID_ARGUMENT, "unknown fallback rule");
+    e->fallback_rule = rule;
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_learned_statistics(mpm_engine* e, double* out3) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    if (!out3) return record(e, MPM_ERR_INVALID_ARGUMENT, "out is NULL");
+    for (int q = 0; q < 3; ++q) out3[q] = e->last_stats[q];
     return MPM_OK;
 }
 

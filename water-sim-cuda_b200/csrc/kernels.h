@@ -109,6 +109,7 @@ struct LearnArgs {
     float blend;
     const MlpTc* mlp_tc;  // set: the MLP runs on tcgen05 (mlp unused)
     uint32_t* status;     // kStatusTimeout when a tcgen05 wait gives up
+    uint32_t wait_test;   // test hooks of the first tcgen05 wait (kWaitTest*, corrector_tc.cuh)
 };
 
 // G2P: slot j of Pout = particle gidx[j] of Pin advanced one substep;
@@ -139,7 +140,10 @@ int launch_grid_export(const SimParams& p, const float4* grid, float* planes4, c
 
 // ----------------------------------------------------------------- sdf ----
 // tris: 9*t floats on the device, allocation padded by >= 16 bytes.
-int launch_sdf_build(const SimParams& p, const float* tris, int t, float* sdf, uint32_t* status, cudaStream_t st);
+// wait_test: test hooks of the first triangle tile's wait (kWaitTestGiveUp /
+// kWaitTestExpire, corrector_tc.cuh), acted on after the real completion.
+int launch_sdf_build(const SimParams& p, const float* tris, int t, float* sdf, uint32_t* status, cudaStream_t st,
+                     uint32_t wait_test = 0u);
 int launch_fill(float* dst, long long count, float value, cudaStream_t st);
 // dst[i] = i for i < n.
 int launch_identity(int32_t* dst, int n, cudaStream_t st);

@@ -24,6 +24,10 @@ constexpr int kSdfThreads = 256;
 constexpr int kTriTile = 256;                 // triangles per stage
 constexpr int kTriFloats = 9;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per wait
+constexpr unsigned long long kSdfTestWaitNs = 20000000ull;  // the test hook's expiring wait: 20 ms
+// Test hooks (the engine's wait test, the values of kWaitTest* in
+// corrector_tc.cuh), acted on at the first tile after its copy has landed.
+constexpr uint32_t kSdfTestGiveUp = 1u, kSdfTestExpire = 2u;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -66,12 +70,12 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     return t;
 }
 
-// Waits for phase `parity` of `bar`; false after kWaitNs.
-__device__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Waits for phase `parity` of `bar`; false after limit_ns.
+__device__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned long long limit_ns = kWaitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     while (!mbar_try_wait(bar, parity)) {
-        if (globaltimer_ns() - t0 > kWaitNs) return false;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
     }
     return true;
 }
@@ -134,7 +138,7 @@ __device__ __forceinline__ float tri_dist2(float px, float py, float pz, const f
 
 __global__ void __launch_bounds__(kSdfThreads) sdf_build_kernel(SimParams p, const float* __restrict__ tris,
                                                                 int t_count, float* __restrict__ sdf,
-                                                                uint32_t* __restrict__ status) {
+                                                                uint32_t* __restrict__ status, uint32_t wait_test) {
     __shared__ __align__(128) float s_tri[2][kTriTile * kTriFloats];
     __shared__ __align__(8) uint64_t s_bar[2];
 
@@ -166,7 +170,15 @@ __global__ void __launch_bounds__(kSdfThreads) sdf_build_kernel(SimParams p, con
     for (; tile < ntiles; ++tile) {
         const int b = tile & 1;
         if (threadIdx.x == 0 && tile + 1 < ntiles) issue(tile + 1);
-        const bool ok = mbar_wait_bounded(&s_bar[b], (uint32_t)((tile >> 1) & 1));
+        bool ok = mbar_wait_bounded(&s_bar[b], (uint32_t)((tile >> 1) & 1));
+        if (ok && tile == 0 && wait_test) {
+            // Test hooks, with tile 0's copy landed: report a give-up, or
+            // wait for the barrier's next phase, which no copy completes yet
+            // (tile 2 is issued only at the next iteration), until the short
+            // limit runs out.
+            if (wait_test & kSdfTestGiveUp) ok = false;
+            else if (wait_test & kSdfTestExpire) ok = mbar_wait_bounded(&s_bar[b], 1u, kSdfTestWaitNs);
+        }
         if (__syncthreads_or(!ok)) {
             aborted = true;
             break;
@@ -200,9 +212,11 @@ __global__ void __launch_bounds__(kSdfThreads) sdf_build_kernel(SimParams p, con
 
 }  // namespace
 
-int launch_sdf_build(const SimParams& p, const float* tris, int t, float* sdf, uint32_t* status, cudaStream_t st) {
+int launch_sdf_build(const SimParams& p, const float* tris, int t, float* sdf, uint32_t* status, cudaStream_t st,
+                     uint32_t wait_test) {
     if (p.g <= 0) return 0;
-    sdf_build_kernel<<<(p.g + kSdfThreads - 1) / kSdfThreads, kSdfThreads, 0, st>>>(p, tris, t, sdf, status);
+    sdf_build_kernel<<<(p.g + kSdfThreads - 1) / kSdfThreads, kSdfThreads, 0, st>>>(p, tris, t, sdf, status,
+                                                                                     wait_test);
     return 1;
 }
 

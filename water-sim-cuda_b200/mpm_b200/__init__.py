@@ -25,6 +25,8 @@ GRID_PLANES = 4
 POS_X, VEL_X, C00, F00, VOL, MASS = 0, 3, 6, 15, 24, 25
 STAGE_SORT, STAGE_P2G, STAGE_GRID, STAGE_G2P = 1, 2, 3, 4
 HEALTH_NONFINITE, HEALTH_OUT_OF_GRID = 1, 2
+FALLBACK_RULES = {"density_change": 0, "rest_density": 1, "rest_density_excess": 2}
+WAIT_TEST_SDF_GIVE_UP, WAIT_TEST_SDF_EXPIRE, WAIT_TEST_MMA_GIVE_UP, WAIT_TEST_MMA_EXPIRE = 1, 2, 4, 8
 SORT_STATIC_MAX_PARTICLES = 1 << 20  # MPM_SORT_STATIC_MAX_PARTICLES
 CORRECTOR_PARAMS, CORRECTOR_FEATURES, CORRECTOR_OUTPUTS = 5478, 16, 3
 
@@ -145,6 +147,7 @@ def _load() -> ctypes.CDLL:
         "mpm_synchronize": (I32, [P]),
         "mpm_substep_partial": (I32, [P, I32]),
         "mpm_set_checks": (I32, [P, U32]),
+        "mpm_set_wait_test": (I32, [P, U32]),
         "mpm_num_particles": (I64, [P]),
         "mpm_get_state": (I32, [P, P]),
         "mpm_set_state": (I32, [P, I64, P]),
@@ -213,6 +216,8 @@ def _load() -> ctypes.CDLL:
         "mpm_set_corrector": (I32, [P, P, I32, ctypes.c_float]),
         "mpm_step_learned": (I32, [P, I32, P]),
         "mpm_set_corrector_kernel": (I32, [P, I32]),
+        "mpm_set_fallback_rule": (I32, [P, I32]),
+        "mpm_learned_statistics": (I32, [P, P]),
         "mpm_corrector_create": (I32, [I32, I64, P]),
         "mpm_corrector_destroy": (None, [P]),
         "mpm_corrector_last_error": (ctypes.c_char_p, [P]),
@@ -356,6 +361,10 @@ class Engine:
     def set_checks(self, flags: int):
         self._check(lib.mpm_set_checks(self._h, int(flags)))
 
+    def set_wait_test(self, flags: int):
+        """Test hooks of the bounded device waits (WAIT_TEST_* bits; 0 clears)."""
+        self._check(lib.mpm_set_wait_test(self._h, int(flags)))
+
     # -- readback -----------------------------------------------------------------
     def get_number(self) -> int:
         return int(lib.mpm_num_particles(self._h))
@@ -457,6 +466,17 @@ class Engine:
     def set_corrector_kernel(self, tcgen05: bool = True):
         """The MLP inside the learned G2P: tcgen05 + TMEM (default) or mma.sync."""
         self._check(lib.mpm_set_corrector_kernel(self._h, 0 if tcgen05 else 1))
+
+    def set_fallback_rule(self, rule: str = "density_change"):
+        """The fallback statistic: "density_change" (default), "rest_density" or
+        "rest_density_excess" (mpm_set_fallback_rule)."""
+        self._check(lib.mpm_set_fallback_rule(self._h, FALLBACK_RULES[rule]))
+
+    def learned_statistics(self) -> dict:
+        """The three fallback means of the last checked large step."""
+        out = np.zeros(3, np.float64)
+        self._check(lib.mpm_learned_statistics(self._h, _ptr(out)))
+        return {"density_change": float(out[0]), "rest_density": float(out[1]), "rest_density_before": float(out[2])}
 
     def step_learned(self, nlarge: int = 1) -> dict:
         """nlarge large steps of RATIO x DT; returns the running learned-step counters."""

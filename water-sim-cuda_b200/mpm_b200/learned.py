@@ -152,14 +152,16 @@ def _timed(fn):
 
 
 def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_density_change: float = 0.02,
-             checkpoints=(10, 25, 50, 100), perturb: float = 1e-4) -> dict:
+             checkpoints=(10, 25, 50, 100), perturb: float = 1e-4, rule: str = "density_change") -> dict:
     """Plain (ratio * nlarge substeps) vs learned (nlarge large steps) vs the
     uncorrected large step, from the same state; metrics at each checkpoint
     (in large steps) and at the end.  "perturbed" is the plain run from
     positions moved by N(0, perturb) cells: its distance from the plain run
-    is the chaos floor of the scene, what no large step can undercut."""
+    is the chaos floor of the scene, what no large step can undercut.
+    rule: the fallback statistic (Engine.set_fallback_rule); the learned run
+    also reports the mean of each statistic over its checked large steps."""
     marks = sorted(set([c for c in checkpoints if c <= nlarge] + [nlarge]))
-    res = {"ratio": ratio, "large_steps": nlarge, "max_density_change": max_density_change}
+    res = {"ratio": ratio, "large_steps": nlarge, "max_density_change": max_density_change, "rule": rule}
     runs = {}
     st_p = st.copy()
     st_p[0:3] += np.random.default_rng(99).normal(0, perturb, st_p[0:3].shape).astype(np.float32)
@@ -169,13 +171,24 @@ def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_densi
             e.init_sdf(tris)
             if tag == "learned":
                 e.set_corrector(params, ratio=ratio, max_density_change=max_density_change)
+                e.set_fallback_rule(rule)
             elif tag == "uncorrected":
                 e.set_corrector(None, ratio=ratio)
             pos, total, prev, stats = {}, 0.0, 0, {}
+            seen = {"density_change": [], "rest_density": [], "rest_density_before": []}
             for m in marks:
                 k = m - prev
                 if tag in ("plain", "perturbed"):
                     _, dt = _timed(lambda: e.step(k * ratio))
+                elif tag == "learned" and max_density_change >= 0:
+                    # One call per large step, to record each step's statistics
+                    # (the step is synchronous when checked either way).
+                    dt = 0.0
+                    for _ in range(k):
+                        stats, d = _timed(lambda: e.step_learned(1))
+                        dt += d
+                        for key, v in e.learned_statistics().items():
+                            seen[key].append(v)
                 else:
                     stats, dt = _timed(lambda: e.step_learned(k))
                 total += dt
@@ -187,6 +200,8 @@ def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_densi
                         "particle_substeps_per_s": e.get_number() * nlarge * ratio / total}
             if tag == "learned":
                 res[tag].update(stats)
+                if seen["density_change"]:
+                    res[tag]["mean_statistics"] = {key: float(np.mean(v)) for key, v in seen.items()}
     for tag in ("perturbed", "learned", "uncorrected"):
         for m in marks:
             res[tag][f"at_{m}"] = compare(cfg, runs[tag][m], runs["plain"][m])
@@ -230,7 +245,47 @@ def main(argv=None):
     ev.add_argument("--physical", action="store_true")
     ev.add_argument("--seed", type=int, default=1235)
     ev.add_argument("--alpha", type=float, default=1.0, help="scale of the applied correction")
+    pr = sub.add_parser("probe", help="a few learned large steps on a thinned dam break (a small case to profile)")
+    pr.add_argument("--params", default=PHYSICAL_PARAMS)
+    pr.add_argument("--thin", type=int, default=5, help="keep every THIN-th particle")
+    pr.add_argument("--large-steps", type=int, default=4)
+    pr.add_argument("--kernel", choices=["tcgen05", "mma_sync"], default="tcgen05")
+    tt = sub.add_parser("train-timing", help="wall-clock time per Adam step of each training kernel")
+    tt.add_argument("--samples", type=int, default=1_000_000)
+    tt.add_argument("--batch", type=int, default=65536)
+    tt.add_argument("--warmup", type=int, default=20)
+    tt.add_argument("--steps", type=int, default=200)
     a = ap.parse_args(argv)
+    if a.cmd == "probe":
+        params, meta = load_params(a.params)
+        cfg, st, tris = scenes.dam_break(seed=1235)
+        if meta.get("physical"):
+            cfg = physical_config(cfg)
+        st = np.ascontiguousarray(st[:, ::a.thin])
+        with Engine(cfg) as e:
+            e.init(st)
+            e.init_sdf(tris)
+            e.set_corrector(params, ratio=int(meta.get("ratio", 4)), max_density_change=-1.0)
+            e.set_corrector_kernel(a.kernel == "tcgen05")
+            _, dt = _timed(lambda: e.step_learned(a.large_steps))
+        print(json.dumps({"particles": int(st.shape[1]), "large_steps": a.large_steps, "kernel": a.kernel,
+                          "seconds": dt}))
+        return
+    if a.cmd == "train-timing":
+        rng = np.random.default_rng(17)
+        feats = rng.normal(0, 1, (a.samples, 16)).astype(np.float32)
+        targs = (np.tanh(feats[:, 9:12]) + 0.1 * rng.normal(0, 1, (a.samples, 3))).astype(np.float32)
+        out = {}
+        with Corrector(a.samples) as c:
+            c.add_data(feats, targs)
+            for kind in ("tcgen05", "fp32", "tcgen05"):
+                c.init(seed=1)
+                c.set_train_kernel(kind)
+                c.train(a.warmup, batch=a.batch, lr=1e-3, seed=3)
+                loss, dt = _timed(lambda: c.train(a.steps, batch=a.batch, lr=1e-3, seed=5))
+                out[kind] = {"ms_per_step": 1e3 * dt / a.steps, "loss": float(loss)}
+        print(json.dumps({"samples": a.samples, "batch": a.batch, "steps": a.steps} | out))
+        return
     if a.cmd == "train":
         seeds = list(range(a.first_seed, a.first_seed + a.variants))
         probes = a.substeps // a.probe_every
