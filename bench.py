@@ -74,6 +74,9 @@ def parse_args(argv=None):
                     help="substeps simulated before the warm-up, to measure a later state of the scene")
     ap.add_argument("--no-whole-run", action="store_true",
                     help="skip the leg that times the workload's whole run from its initial state")
+    ap.add_argument("--compare-stages", action="store_true",
+                    help="instead of the bench line: per-stage device times of the reference engine and of this "
+                         "engine on the workload (K frames after the warm-up), the SDF build and the sort")
     return ap.parse_args(argv)
 
 
@@ -588,12 +591,73 @@ def run_reference(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def compare_stages(args, local):
+    """Per-stage device times (CUDA events) of the reference's engine and of
+    this engine on the same scene and frames, plus the one-time SDF build and
+    the bit-exact sort on their own.  One JSON line."""
+    import numpy as np
+    import torch
+    from oracle.oracle import REF_LIB, RefEngine
+    import mpm_b200
+    torch.cuda.set_device(local)
+    cfg, st, tris = make_scene(args.workload, 0)
+    n, sub, K = st.shape[1], cfg.substeps, args.steps
+    out = {"workload": args.workload, "particles": n, "frames": K, "substeps": K * sub, "advanced": args.advance}
+    if os.path.exists(REF_LIB) and cfg.grid_number % 256 == 0:
+        ref = RefEngine()
+        ref.create(cfg, st, tris, f"/tmp/ref_stages_config_{os.getpid()}.txt")
+        ref.step(args.advance + max(args.warmup, 3) * sub)
+        r = ref.time_stages(K * sub)
+        out["reference_ms_per_substep"] = {k: round(v / (K * sub), 5) for k, v in r.items()}
+        out["reference_make_sdf_ms"] = round(ref.time_make_sdf(tris), 3)
+        out["reference_sort_ms"] = round(ref.time_sort(10), 4)
+        ref.destroy()
+    with mpm_b200.Engine(cfg, device=local) as eng:
+        eng.init(st)
+        stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        eng.init_sdf(tris)  # warm
+        ev[0].record(stream)
+        eng.init_sdf(tris)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        out["sdf_build_ms"] = round(ev[0].elapsed_time(ev[1]), 3)
+        eng.step(args.advance + max(args.warmup, 3) * sub)
+        eng.autotune(3)
+        eng.set_stage_timing(K * sub)
+        for _ in range(K):
+            eng.step_async(sub)
+        ms, cnt = eng.stage_times()
+        eng.set_stage_timing(0)
+        out["engine_ms_per_substep"] = {k: round(v / max(cnt, 1), 5) for k, v in ms.items()}
+        out["engine_tuning"] = eng.tuning()
+        # The bit-exact Morton sort on the same positions (caller-owned buffers).
+        cur = eng.get_buffer()
+        d = torch.from_numpy(np.ascontiguousarray(cur[0:3])).cuda()
+        keys = torch.empty(n, dtype=torch.int32, device="cuda")
+        perm = torch.empty(n, dtype=torch.int32, device="cuda")
+        cs = torch.cuda.current_stream()
+        args_ = (d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), n, keys.data_ptr(), perm.data_ptr(),
+                 cs.cuda_stream)
+        mpm_b200.sort_particles_device(*args_)
+        ev[0].record(cs)
+        for _ in range(10):
+            mpm_b200.sort_particles_device(*args_)
+        ev[1].record(cs)
+        torch.cuda.synchronize()
+        out["engine_sort_ms"] = round(ev[0].elapsed_time(ev[1]) / 10, 4)
+    print(json.dumps(out), flush=True)
+
+
 def main(argv=None):
     args = parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
+    if args.compare_stages:
+        if rank == 0:
+            compare_stages(args, local)
+    elif args.impl == "reference":
         run_reference(args, rank, world, local)
     else:
         run_engine(args, rank, world, local)

@@ -146,6 +146,8 @@ class RefEngine:
             ("ref_engine_get_state", I, [P]), ("ref_engine_get_grid", I, [P]), ("ref_engine_get_sdf", I, [P]),
             ("ref_engine_get_positions", I, [P]), ("ref_engine_get_perm", I, [P]), ("ref_engine_keys", I, [P]),
             ("ref_engine_sort_only", I, []), ("ref_engine_destroy", None, []),
+            ("ref_engine_time_stages", I, [I, P]), ("ref_time_make_sdf", ctypes.c_float, [P, L]),
+            ("ref_time_sort", ctypes.c_float, [I]),
         ]:
             f = getattr(self.lib, name)
             f.restype = res
@@ -216,6 +218,19 @@ class RefEngine:
 
     def sort_only(self):
         assert self.lib.ref_engine_sort_only() == 0
+
+    def time_stages(self, nsub):
+        """Per-stage device ms summed over nsub substeps: sort, clear, p2g, grid, g2p, export."""
+        ms = np.zeros(6, np.float32)
+        assert self.lib.ref_engine_time_stages(nsub, _p(ms)) == 0
+        return dict(zip(("sort", "clear", "p2g", "grid", "g2p", "export"), ms.astype(float)))
+
+    def time_make_sdf(self, tris) -> float:
+        t = np.ascontiguousarray(tris, np.float32).reshape(-1)
+        return float(self.lib.ref_time_make_sdf(_p(t) if t.size else None, t.size // 9))
+
+    def time_sort(self, reps=10) -> float:
+        return float(self.lib.ref_time_sort(reps))
 
     def destroy(self):
         self.lib.ref_engine_destroy()

@@ -36,6 +36,11 @@
 
 __global__ void setKeys(Particles p, int* keys, int number);                                   // kernels.cu:361
 __global__ void makeSDF(float* sdfGrid, const Triangle* __restrict__ triangles, int triangleNumber);  // kernels.cu:282
+__global__ void p2GTransferScatter(Particles p, Grid g, int number, int* sortedIndices);  // kernels.cu:6
+__global__ void gridUpdate(Grid g);                                                      // kernels.cu:144
+__global__ void g2PTransfer(Particles p, Grid g, int number, int* sortedIndices);        // kernels.cu:199
+__global__ void emptyGrid(Grid g);                                                       // kernels.cu:311
+__global__ void changeFormat(Particles p, float3* buf, int number);                      // kernels.cu:341
 
 namespace {
 
@@ -53,6 +58,11 @@ struct SdfTag {
     friend type get(SdfTag);
 };
 template struct Expose<SdfTag, &Engine::d_sdf_buffer>;
+struct PositionsTag {
+    typedef float3* Engine::*type;
+    friend type get(PositionsTag);
+};
+template struct Expose<PositionsTag, &Engine::positionsToOpenGL>;
 struct MapTag {
     typedef std::unordered_map<std::string, std::string>* type;
     friend type get(MapTag);
@@ -237,6 +247,109 @@ int ref_engine_get_perm(int* out) {
     if (!g_engine) return -1;
     int* v = g_engine->*get(ValuesTag());
     return cudaMemcpy(out, v, sizeof(int) * g_n, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : -2;
+}
+
+// Engine::step (engine.cu:54-70) with CUDA events between its stages: the
+// same calls in the same order and with the same launch shapes
+// (sortParticles, emptyGrid, p2GTransferScatter, gridUpdate, g2PTransfer,
+// changeFormat), without the host synchronisation after each launch.  Sums
+// each stage's device time over nsub substeps into ms6[0..5] in that order;
+// the sort includes the reference's per-call cudaMalloc/cudaFree of its key
+// buffer, as Engine::sortParticles does it.
+int ref_engine_time_stages(int nsub, float* ms6) {
+    if (!g_engine) return -1;
+    cudaEvent_t ev[7];
+    for (auto& x : ev) cudaEventCreate(&x);
+    for (int k = 0; k < 6; ++k) ms6[k] = 0.0f;
+    const int n = (int)g_n;
+    const int blocks = (n + THREADS_PER_BLOCK - 1) / THREADS_PER_BLOCK;
+    const int gblocks = GameConfigData::getInt("GRID_BLOCKS");
+    int* values = g_engine->*get(ValuesTag());
+    float3* positions = g_engine->*get(PositionsTag());
+    cudaDeviceSynchronize();
+    for (int i = 0; i < nsub; ++i) {
+        cudaEventRecord(ev[0]);
+        g_engine->sortParticles();
+        cudaEventRecord(ev[1]);
+        emptyGrid<<<gblocks, THREADS_PER_BLOCK>>>(g_engine->getGrid());
+        cudaEventRecord(ev[2]);
+        p2GTransferScatter<<<blocks, THREADS_PER_BLOCK>>>(g_engine->getParticles(), g_engine->getGrid(), n, values);
+        cudaEventRecord(ev[3]);
+        gridUpdate<<<gblocks, THREADS_PER_BLOCK>>>(g_engine->getGrid());
+        cudaEventRecord(ev[4]);
+        g2PTransfer<<<blocks, THREADS_PER_BLOCK>>>(g_engine->getParticles(), g_engine->getGrid(), n, values);
+        cudaEventRecord(ev[5]);
+        changeFormat<<<blocks, THREADS_PER_BLOCK>>>(g_engine->getParticles(), positions, n);
+        cudaEventRecord(ev[6]);
+        cudaEventSynchronize(ev[6]);
+        for (int k = 0; k < 6; ++k) {
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+            ms6[k] += t;
+        }
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// Device time of one makeSDF launch (kernels.cu:282-300) over the loaded
+// config's grid with Engine::initSDF's launch shape (engine.cu:105-114), the
+// triangles already on the device.
+float ref_time_make_sdf(const float* tris, long t) {
+    const long g = (long)GameConfigData::getInt("GRID_NUMBER");
+    float* sdf = nullptr;
+    Triangle* d_tris = nullptr;
+    if (cudaMalloc((void**)&sdf, sizeof(float) * g) != cudaSuccess) return -1.0f;
+    if (t > 0 && cudaMalloc((void**)&d_tris, sizeof(Triangle) * t) != cudaSuccess) {
+        cudaFree(sdf);
+        return -1.0f;
+    }
+    if (t > 0) cudaMemcpy(d_tris, tris, sizeof(Triangle) * t, cudaMemcpyHostToDevice);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a);
+    makeSDF<<<GameConfigData::getInt("GRID_BLOCKS"), THREADS_PER_BLOCK>>>(sdf, d_tris, (int)t);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sdf);
+    if (d_tris) cudaFree(d_tris);
+    return cudaGetLastError() == cudaSuccess ? ms : -2.0f;
+}
+
+// Device time of `reps` reference sorts of n keys (setKeys on the engine's
+// particles, then thrust::sequence + thrust::sort_by_key as
+// Engine::sortParticles runs them, engine.cu:92-102), the key buffer
+// allocated once outside the timed region.
+float ref_time_sort(int reps) {
+    if (!g_engine) return -1.0f;
+    const int n = (int)g_n;
+    int* keys = nullptr;
+    if (cudaMalloc((void**)&keys, sizeof(int) * n) != cudaSuccess) return -1.0f;
+    int* values = g_engine->*get(ValuesTag());
+    const int blocks = (n + THREADS_PER_BLOCK - 1) / THREADS_PER_BLOCK;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaDeviceSynchronize();
+    cudaEventRecord(a);
+    for (int r = 0; r < reps; ++r) {
+        setKeys<<<blocks, THREADS_PER_BLOCK>>>(g_engine->getParticles(), keys, n);
+        thrust::sequence(thrust::device, values, values + n);
+        thrust::sort_by_key(thrust::device, keys, keys + n, values);
+    }
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(keys);
+    return cudaGetLastError() == cudaSuccess ? ms / (float)reps : -2.0f;
 }
 
 // setKeys on the current particle state (the keys the next substep sorts).
