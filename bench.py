@@ -458,7 +458,7 @@ def run_engine(args, rank, world, local):
         init2()  # warm the allocation path once
         if tuning:
             eng2.set_tuning(tuning["p2g_ctas_per_sm"], tuning["g2p_block"], tuning["grid_block"],
-                            tuning["p2g_cell_cap"], tuning["p2g_lanes_per_cell"])
+                            tuning["p2g_cell_cap"])
         eng2.step(sub)
         dist.barrier()
         marks = [time.perf_counter()]

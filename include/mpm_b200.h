@@ -542,9 +542,6 @@ typedef struct mpm_tuning {
     int32_t p2g_cell_cap;     /* 4 .. 64: particles of a cell one lane sums before the
                                * rest goes, in chunks, to all warps; 0 (default): chosen
                                * per work item from its cells' particle counts */
-    int32_t p2g_lanes_per_cell; /* 1: a lane sums all 27 x 4 node values of its cell;
-                                 * 2: two lanes share a cell, 27 x 2 values each, so that
-                                 * more warps fit per SM (the same sums bit for bit) */
 } mpm_tuning;
 mpm_status mpm_autotune(mpm_engine* engine, int32_t repeats, mpm_tuning* out);
 mpm_status mpm_set_tuning(mpm_engine* engine, const mpm_tuning* tuning);

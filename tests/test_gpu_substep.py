@@ -25,25 +25,20 @@ def _scene(name):
     return scenes.small_scene(n, size, **kw)
 
 
-def _run(mpm, cfg, st, tris, nsub, lanes=1):
+def _run(mpm, cfg, st, tris, nsub):
     with mpm.Engine(cfg) as eng:
         eng.init(st)
         eng.init_sdf(tris)
-        if lanes != 1:
-            eng.set_tuning(20, 256, 256, 0, lanes)
         start = eng.get_buffer()
         sdf = eng.get_sdf()
         eng.step(nsub)
         return start, sdf, eng.get_buffer(), eng.get_grid(), eng.get_positions()
 
 
-@pytest.mark.parametrize("lanes", [1, 2])
 @pytest.mark.parametrize("name", sorted(SCENES))
-def test_one_substep(gpu_ok, mpm, oracle64, name, lanes):
-    """lanes: P2G lanes per cell (one lane sums a cell's 27 x 4 node values, or
-    two lanes share them)."""
+def test_one_substep(gpu_ok, mpm, oracle64, name):
     cfg, st, tris = _scene(name)
-    start, sdf, got, grid, pos = _run(mpm, cfg, st, tris, 1, lanes)
+    start, sdf, got, grid, pos = _run(mpm, cfg, st, tris, 1)
     st0 = oracle64.init_particles(cfg, st)
     assert np.array_equal(start, st0.astype(np.float32)), "init rules (initFMatrices) differ"
     want, wgrid, _, _ = oracle64.substep(cfg, st0, sdf.astype(np.float64))
@@ -154,9 +149,8 @@ def test_reinit_reuses_buffers(gpu_ok, mpm, oracle64):
             assert_state_close(got, want, st0)
 
 
-@pytest.mark.parametrize("lanes", [1, 2])
 @pytest.mark.parametrize("case", ["dense_cap4", "one_cell_pile"])
-def test_crowded_cells_through_the_list(gpu_ok, mpm, oracle64, case, lanes):
+def test_crowded_cells_through_the_list(gpu_ok, mpm, oracle64, case):
     """Particles past a cell's cap go to the crowded-cell list, 256 per entry,
     and a second launch sums them.  In a dense scene at the smallest cap, every
     cell above 4 particles takes that path; a pile of 3000 particles in one
@@ -171,9 +165,7 @@ def test_crowded_cells_through_the_list(gpu_ok, mpm, oracle64, case, lanes):
         eng.init(st)
         eng.init_sdf(tris)
         if case == "dense_cap4":
-            eng.set_tuning(12, 256, 256, 4, lanes)
-        elif lanes != 1:
-            eng.set_tuning(20, 256, 256, 0, lanes)
+            eng.set_tuning(12, 256, 256, 4)
         sdf = eng.get_sdf()
         eng.step(1)
         got = eng.get_buffer()

@@ -167,7 +167,7 @@ struct mpm_engine {
     double last_stats[3] = {0.0, 0.0, 0.0};  // the three means of the last checked large step
 
     // Launch shapes of the substep (mpm_autotune / mpm_set_tuning).
-    mpm_tuning tune{12, 256, 256, 0.f, 0.f, 0.f, 0, 1};
+    mpm_tuning tune{12, 256, 256, 0.f, 0.f, 0.f, 0};
 };
 
 namespace {
@@ -351,7 +351,7 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
         launches += mpm::launch_p2g(sc, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par], e->corder, e->d_itemoff,
                                     work, e->accum, e->crowd, e->crowd_cap, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
-                                    e->tune.p2g_cell_cap, e->tune.p2g_lanes_per_cell);
+                                    e->tune.p2g_cell_cap);
     mark(2);
     if (from <= MPM_STAGE_GRID && upto >= MPM_STAGE_GRID)
         launches += mpm::launch_grid_update(sc, e->prm[0], e->g_total, e->accum, e->vgrid, e->sdf, st,
@@ -739,7 +739,7 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
                                           e->scan_chunks, st);
     launches += mpm::launch_p2g(e->table_large, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par],
                                 e->corder, e->d_itemoff, work, e->accum, e->crowd, e->crowd_cap, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
-                                e->tune.p2g_cell_cap, e->tune.p2g_lanes_per_cell);
+                                e->tune.p2g_cell_cap);
     launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, st,
                                         e->tune.grid_block);
     launches += mpm::launch_g2p(e->table_large, big, e->n, e->P[par], e->P[1 - par], e->gidx, e->sigma[par],
@@ -1542,8 +1542,7 @@ extern "C" mpm_status mpm_checkpoint_load(const char* path, int32_t device, mpm_
 // ------------------------------------------------------------ autotune ----
 namespace {
 bool valid_tuning(const mpm_tuning& t) {
-    return (t.p2g_lanes_per_cell == 1 || t.p2g_lanes_per_cell == 2) && t.p2g_ctas_per_sm >= 1 &&
-           t.p2g_ctas_per_sm <= mpm::p2g_max_ctas_per_sm(t.p2g_lanes_per_cell) &&
+    return t.p2g_ctas_per_sm >= 1 && t.p2g_ctas_per_sm <= mpm::p2g_max_ctas_per_sm() &&
            (t.g2p_block == 128 || t.g2p_block == 256 || t.g2p_block == 512) &&
            (t.grid_block == 128 || t.grid_block == 256) &&
            (t.p2g_cell_cap == 0 || (t.p2g_cell_cap >= 4 && t.p2g_cell_cap <= 64));
@@ -1576,7 +1575,6 @@ extern "C" mpm_status mpm_set_tuning(mpm_engine* e, const mpm_tuning* t) {
     e->tune.g2p_block = t->g2p_block;
     e->tune.grid_block = t->grid_block;
     e->tune.p2g_cell_cap = t->p2g_cell_cap;
-    e->tune.p2g_lanes_per_cell = t->p2g_lanes_per_cell;
     return e->initialized ? capture_graphs(e) : MPM_OK;
 }
 
@@ -1616,22 +1614,16 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
         *ms = t[repeats / 2];
         return MPM_OK;
     };
-    // Each stage is its own kernel: tune them one at a time.  P2G: both
-    // layouts (one or two lanes per cell), each over its warps per SM.
+    // Each stage is its own kernel: tune them one at a time.
+    const int max_p2g = mpm::p2g_max_ctas_per_sm();
     float tbest = 1e30f, ms = 0.f;
-    for (int lanes : {1, 2}) {
-        const int max_p2g = mpm::p2g_max_ctas_per_sm(lanes);
-        for (int k : {4, 6, 8, 10, 12, 14, 16, 20, 24, 28, 32}) {
-            if (k > max_p2g || s != MPM_OK) break;
-            e->tune.p2g_lanes_per_cell = lanes;
-            e->tune.p2g_ctas_per_sm = k;
-            if ((s = median_time(MPM_STAGE_P2G, &ms)) != MPM_OK) break;
-            if (ms < tbest)
-                tbest = ms, best.p2g_ctas_per_sm = k, best.p2g_lanes_per_cell = lanes, best.p2g_ms = ms;
-        }
+    for (int k : {4, 6, 8, 10, 12, 14, 16, 20, 24}) {
+        if (k > max_p2g) break;
+        e->tune.p2g_ctas_per_sm = k;
+        if ((s = median_time(MPM_STAGE_P2G, &ms)) != MPM_OK) break;
+        if (ms < tbest) tbest = ms, best.p2g_ctas_per_sm = k, best.p2g_ms = ms;
     }
     e->tune.p2g_ctas_per_sm = best.p2g_ctas_per_sm;
-    e->tune.p2g_lanes_per_cell = best.p2g_lanes_per_cell;
     // The crowded-cell threshold is not tuned here: P2G chooses it per work
     // item from the counts it sees, which follows the state as it evolves,
     // while a fixed value timed on one state can cost far more later.

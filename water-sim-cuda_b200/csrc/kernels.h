@@ -84,17 +84,14 @@ int bin_scan_chunks(long long bins);
 // launches: the items, then the crowded-cell list they fill (crowd: scratch of
 // crowd_cap entries, at least n / 4 + 64; work[2..3] are its counters, reset
 // by the bin scan).  ctas_per_sm: persistent single-warp CTAs per SM (0 = the
-// default of the layout); cell_cap: particles of a cell its own lanes sum
-// before the rest goes to the list (0 = chosen per work item from its cells'
-// counts); lanes_per_cell: 1 (a lane sums a cell's 27 x 4 values) or 2 (two
-// lanes share a cell, 27 x 2 values each, more warps per SM).
+// default 12); cell_cap: particles of a cell its own lane sums before the rest
+// goes to the list (0 = chosen per work item from its cells' counts).
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
                const int32_t* cstart, const BinSet& cur, const uint8_t* corder, const long long* itemoff,
                uint32_t* work, float4* accum, int4* crowd, int crowd_cap, uint32_t* status, cudaStream_t st,
-               int ctas_per_sm = 0, int cell_cap = 0, int lanes_per_cell = 1);
-// Most P2G CTAs that fit on one SM, and the default, for a layout.
-int p2g_max_ctas_per_sm(int lanes_per_cell);
-int p2g_default_ctas_per_sm(int lanes_per_cell);
+               int ctas_per_sm = 0, int cell_cap = 0);
+// Most P2G CTAs that fit on one SM.
+int p2g_max_ctas_per_sm();
 // p0: the parameters of scene 0, used directly when the table holds one scene.
 int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
                        const float* sdf, cudaStream_t st, int block = 256);

@@ -153,7 +153,6 @@ struct SceneLookup {
 // is dropped (it drops shared-tile cells whose partial mass is <= 1e-9,
 // kernels.cu:132).
 constexpr int kP2GWarpsPerSM = 12;
-constexpr int kP2GPairWarpsPerSM = 20;  // two lanes per cell: 27 x 2 sums per lane
 constexpr int kRing = 2;
 constexpr int kGidxStage = 256;   // gather indices of a bin staged in shared memory
 constexpr int kCellCap = 12;      // particles of a cell its own lane sums; the rest: the crowded-cell list
@@ -266,95 +265,53 @@ __device__ __forceinline__ void p2g_stencil(const P2GParticle& r, Emit emit) {
     }
 }
 
-// The crowded-cell threshold of one work item, from the counts of its cells
-// (`full`, one per lane; `counted`: the lane that speaks for its cell, since
-// with two lanes per cell both hold its count): for each candidate cap the
-// loop costs min(max count, cap) iterations with every lane, plus, per cell
-// above the cap, ceil((count - cap) / 32) whole-warp iterations and one
-// reduce-scatter (about 1.3 iterations) in the crowded-cell launch; the
-// cheapest candidate wins.  Every cap gives the same sums.  Caps stop at 32:
-// a larger one makes a few long items that hold up the kernel while other
-// warps idle, whereas the list spreads the rest of a crowded cell over all
-// warps.
-__device__ __forceinline__ int item_cap(int full, bool counted) {
+// The crowded-cell threshold of one work item, from the counts of its 32
+// cells (`full`, one per lane): for each candidate cap the loop costs
+// min(max count, cap) iterations with every lane, plus, per cell above the
+// cap, ceil((count - cap) / 32) whole-warp iterations and one reduce-scatter
+// (about 1.3 iterations) in the crowded-cell launch; the cheapest candidate
+// wins.  Every cap gives the same sums.  Caps stop at 32: a larger one makes a
+// few long items that hold up the kernel while other warps idle, whereas the
+// list spreads the rest of a crowded cell over all warps.
+__device__ __forceinline__ int item_cap(int full) {
     const int maxc = __reduce_max_sync(0xffffffffu, (unsigned)full);
     int best = kCellCap;
     float best_cost = 1e30f;
 #pragma unroll
     for (int cand : {8, 12, 16, 24, 32}) {
-        const int over = counted && full > cand ? (full - cand + 31) / 32 : 0;
+        const int over = full > cand ? (full - cand + 31) / 32 : 0;
         const int passes = (int)__reduce_add_sync(0xffffffffu, (unsigned)over);
-        const int cells = __popc(__ballot_sync(0xffffffffu, counted && full > cand));
+        const int cells = __popc(__ballot_sync(0xffffffffu, full > cand));
         const float cost = (float)min(maxc, cand) + (float)passes + 1.3f * (float)cells;
         if (cost < best_cost) best_cost = cost, best = cand;
     }
     return best;
 }
 
-// The 27 sums of one half of a cell's contributions when two lanes share a
-// cell: half 0 sums (mass, momentum x), half 1 (momentum y, momentum z).
-// With (u_A, C_A) = (1, 0) or (u1, row 1 of C') and (u_B, C_B) = (u0, row 0)
-// or (u2, row 2), node o gets w_o (u_A + C_A o) and w_o (u_B + C_B o): the
-// same operations, in the same order, as the single-lane sums of p2g_stencil
-// (for half 0, u_A + C_A o is exactly 1), so both layouts give the same bits.
-__device__ __forceinline__ void p2g_stencil_half(const P2GParticle& r, int h, float (&A)[27], float (&B)[27]) {
-    const float cA0 = h ? r.C[3] : 0.f, cA1 = h ? r.C[4] : 0.f, cA2 = h ? r.C[5] : 0.f;
-    const float cB0 = h ? r.C[6] : r.C[0], cB1 = h ? r.C[7] : r.C[1], cB2 = h ? r.C[8] : r.C[2];
-    float zA = h ? r.u1 : 1.0f, zB = h ? r.u2 : r.u0;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        float yA = zA, yB = zB;
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-            const float wyz = r.wy[b] * r.wz[c];
-            float tA = yA, tB = yB;
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                const int k = (c * 3 + b) * 3 + a;
-                const float w = r.wx[a] * wyz;
-                A[k] += w * tA;
-                B[k] += w * tB;
-                tA += cA0;
-                tB += cB0;
-            }
-            yA += cA1;
-            yB += cB1;
-        }
-        zA += cA2;
-        zB += cB2;
-    }
-}
-
-// kPair lanes per cell: 1 (a lane sums all 27 x 4 values of its cell, 32
-// cells per item) or 2 (p2g_stencil_half: 27 x 2 values per lane, about half
-// the registers and so more warps per SM, 16 cells per item).  Items: a
-// listed bin has kBinCells / (32 / kPair) of them; itemoff counts kBinZ per
-// listed bin, so the item index space is kPair times that.
-template <int kPair>
-__global__ void __launch_bounds__(32, kPair == 1 ? kP2GWarpsPerSM : kP2GPairWarpsPerSM)
-    p2g_kernel(SceneTable sc, const float* __restrict__ P, const int32_t* __restrict__ gidx,
-               const int32_t* __restrict__ cstart, BinSet set, const uint8_t* __restrict__ corder,
-               const long long* __restrict__ itemoff, uint32_t* __restrict__ work, float4* __restrict__ accum_all,
-               int4* __restrict__ crowd, int crowd_cap, uint32_t* __restrict__ status, int cap) {
-    constexpr int kCells = 32 / kPair;                 // cells per item
-    constexpr int kItemsPerBin = kBinCells / kCells;   // 4 or 8
-    __shared__ __align__(16) float4 s_ring[kRing][6][kCells];
+__global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, const float* __restrict__ P,
+                                                                  const int32_t* __restrict__ gidx,
+                                                                  const int32_t* __restrict__ cstart, BinSet set,
+                                                                  const uint8_t* __restrict__ corder,
+                                                                  const long long* __restrict__ itemoff,
+                                                                  uint32_t* __restrict__ work,
+                                                                  float4* __restrict__ accum_all, int4* __restrict__ crowd,
+                                                                  int crowd_cap, uint32_t* __restrict__ status, int cap) {
+    __shared__ __align__(16) float4 s_ring[kRing][6][32];
     __shared__ float4 s_foot[kFootNodes];
     __shared__ int32_t s_gidx[kGidxStage];
     const int lane = threadIdx.x;
-    const int slot = lane / kPair, half = lane % kPair;  // this lane's cell of the item, and its half
-    const long long nitems = *reinterpret_cast<volatile const long long*>(itemoff + sc.count) * kPair;
+    const long long nitems = *reinterpret_cast<volatile const long long*>(itemoff + sc.count);
     for (int q = lane; q < kFootNodes; q += 32) s_foot[q] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (;;) {
         int item = 0;
         if (lane == 0) item = (int)atomicAdd(work, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= nitems) return;
-        // Items: kItemsPerBin per listed bin, scene after scene.
-        const int scene = sc.count == 1 ? 0 : scene_of(itemoff, sc.count, item / kPair);
+        // Items: kBinZ per listed bin, scene after scene.
+        const int scene = sc.count == 1 ? 0 : scene_of(itemoff, sc.count, item);
         const SimParams p = sc.prm[scene];
-        const int local = item - (int)__ldg(itemoff + scene) * kPair;
-        const int bin = __ldg(set.blist + p.boff + local / kItemsPerBin), group = local % kItemsPerBin;
+        const int local = item - (int)__ldg(itemoff + scene);
+        const int bin = __ldg(set.blist + p.boff + local / kBinZ), group = local % kBinZ;
         if (bin >= p.nb) continue;  // the overflow bin reaches no node
         float4* accum = accum_all + p.goff;
         const int bxi = bin % p.nbx, byi = (bin / p.nbx) % p.nby, bzi = bin / (p.nbx * p.nby);
@@ -362,7 +319,7 @@ __global__ void __launch_bounds__(32, kPair == 1 ? kP2GWarpsPerSM : kP2GPairWarp
         const int ox = bxi * kBinX - 2, oy = byi * kBinY - 2, oz = bzi * kBinZ - 2;
         const size_t cb = (size_t)p.coff + (size_t)bin * kBinCells;
         // This lane's cell (z * 32 + y * 8 + x in the bin), 0xFF for none.
-        const int tcell = __ldg(corder + cb + group * kCells + slot);
+        const int tcell = __ldg(corder + cb + group * 32 + lane);
         if (__ballot_sync(0xffffffffu, tcell != 0xFF) == 0u) continue;
         const bool own = tcell != 0xFF;
         const int cs = own ? __ldg(cstart + cb + tcell) : 0;
@@ -374,77 +331,67 @@ __global__ void __launch_bounds__(32, kPair == 1 ? kP2GWarpsPerSM : kP2GPairWarp
         if (staged)
             for (int q = lane; q < l1 - l0; q += 32) s_gidx[q] = __ldg(gidx + l0 + q);
         __syncwarp();
-        // Each cell's first `icap` particles are summed here; the rest of a
+        // Each lane sums its cell's first `icap` particles; the rest of a
         // crowded cell goes to the crowded-cell list in chunks, which
         // p2g_crowd_kernel spreads over all warps.
-        const int icap = cap > 0 ? cap : item_cap(full, half == 0);
-        if (half == 0) {
-            for (int off = icap; off < full; off += kCrowdChunk) {
-                const uint32_t e = atomicAdd(work + 2, 1u);
-                if (e < (uint32_t)crowd_cap)
-                    crowd[e] = make_int4(scene, bin * kBinCells + tcell, cs + off, min(kCrowdChunk, full - off));
-                else
-                    atomicOr(status, kStatusCrowdList);
-            }
+        const int icap = cap > 0 ? cap : item_cap(full);
+        for (int off = icap; off < full; off += kCrowdChunk) {
+            const uint32_t e = atomicAdd(work + 2, 1u);
+            if (e < (uint32_t)crowd_cap)
+                crowd[e] = make_int4(scene, bin * kBinCells + tcell, cs + off, min(kCrowdChunk, full - off));
+            else
+                atomicOr(status, kStatusCrowdList);
         }
         const int cnt = min(full, icap);
         const int maxc = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
-        constexpr int kSums = kPair == 1 ? 4 : 2;  // values summed per node by this lane
-        float acc[kSums][27];
+        float am[27], ax[27], ay[27], az[27];
         auto src_of = [&](int s) -> const float4* {
-            const int sl = cs + s;
-            const int g = staged ? s_gidx[sl - l0] : __ldg(gidx + sl);
+            const int slot = cs + s;
+            const int g = staged ? s_gidx[slot - l0] : __ldg(gidx + slot);
             return reinterpret_cast<const float4*>(P + (size_t)g * kAFloats);
         };
-        // A particle's six 16-byte vectors into ring slot d: one lane copies
-        // all six, or each of a cell's two lanes three.
-        auto fetch = [&](int s, int d) {
-            const float4* src = src_of(s);
 #pragma unroll
-            for (int v = 0; v < 6 / kPair; ++v) {
-                const int vv = half * (6 / kPair) + v;
-                cp_async16(&s_ring[d][vv][slot], src + vv);
-            }
-        };
-#pragma unroll
-        for (int q = 0; q < kSums; ++q)
-#pragma unroll
-            for (int k = 0; k < 27; ++k) acc[q][k] = 0.f;
+        for (int k = 0; k < 27; ++k) am[k] = ax[k] = ay[k] = az[k] = 0.f;
 #pragma unroll
         for (int d = 0; d < kRing - 1; ++d) {
-            if (d < cnt) fetch(d, d);
+            if (d < cnt) {
+                const float4* src = src_of(d);
+#pragma unroll
+                for (int v = 0; v < 6; ++v) cp_async16(&s_ring[d][v][lane], src + v);
+            }
             cp_async_commit();
         }
         for (int s = 0; s < maxc; ++s) {
             const int pf = s + kRing - 1;
-            if (pf < cnt) fetch(pf, pf % kRing);
+            if (pf < cnt) {
+                const float4* src = src_of(pf);
+#pragma unroll
+                for (int v = 0; v < 6; ++v) cp_async16(&s_ring[pf % kRing][v][lane], src + v);
+            }
             cp_async_commit();
             cp_async_wait<kRing - 1>();
             __syncwarp();
             if (s < cnt) {
                 const int sl = s % kRing;
-                const P2GParticle r = p2g_particle(p, s_ring[sl][0][slot], s_ring[sl][1][slot], s_ring[sl][2][slot],
-                                                   s_ring[sl][3][slot], s_ring[sl][4][slot], s_ring[sl][5][slot]);
+                const P2GParticle r = p2g_particle(p, s_ring[sl][0][lane], s_ring[sl][1][lane], s_ring[sl][2][lane],
+                                                   s_ring[sl][3][lane], s_ring[sl][4][lane], s_ring[sl][5][lane]);
                 // Filed under this lane's cell by construction; a mismatch is
                 // recorded, never scattered to a wrong node.
                 if (r.bx - ox != tcell % kBinX || r.by - oy != (tcell / kBinX) % kBinY || r.bz - oz != tcell / 32) {
                     atomicOr(status, kStatusBinning);
-                } else if constexpr (kPair == 1) {
-                    p2g_stencil(r, [&](int k, int, int, int, float m, float mx, float my, float mz) {
-                        acc[0][k] += m;
-                        acc[1][k] += mx;
-                        acc[2][k] += my;
-                        acc[3][k] += mz;
-                    });
                 } else {
-                    p2g_stencil_half(r, half, acc[0], acc[1]);
+                    p2g_stencil(r, [&](int k, int, int, int, float m, float mx, float my, float mz) {
+                        am[k] += m;
+                        ax[k] += mx;
+                        ay[k] += my;
+                        az[k] += mz;
+                    });
                 }
             }
             __syncwarp();
         }
         cp_async_wait<0>();
-        // One cell per lane (or per lane pair, each half its own components):
-        // distinct nodes for each stencil offset.
+        // One lane per cell: distinct nodes for each stencil offset.
         {
             const int tx = tcell % kBinX, ty = (tcell / kBinX) % kBinY, tz = (tcell / 32) & (kBinZ - 1);
 #pragma unroll
@@ -457,20 +404,12 @@ __global__ void __launch_bounds__(32, kPair == 1 ? kP2GWarpsPerSM : kP2GPairWarp
                         float4* d = &s_foot[((tz + c) * kTY + ty + b) * kTX + tx + a];
                         __syncwarp();
                         if (own) {
-                            if constexpr (kPair == 1) {
-                                float4 v = *d;
-                                v.x += acc[0][k];
-                                v.y += acc[1][k];
-                                v.z += acc[2][k];
-                                v.w += acc[3][k];
-                                *d = v;
-                            } else {
-                                float2* d2 = reinterpret_cast<float2*>(d) + half;
-                                float2 v = *d2;
-                                v.x += acc[0][k];
-                                v.y += acc[1][k];
-                                *d2 = v;
-                            }
+                            float4 v = *d;
+                            v.x += am[k];
+                            v.y += ax[k];
+                            v.z += ay[k];
+                            v.w += az[k];
+                            *d = v;
                         }
                     }
         }
@@ -1335,37 +1274,25 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
     return 4;
 }
 
-int p2g_max_ctas_per_sm(int lanes_per_cell) {
+int p2g_max_ctas_per_sm() {
     int k = 0;
-    const cudaError_t err = lanes_per_cell == 2
-                                ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, p2g_kernel<2>, 32, 0)
-                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, p2g_kernel<1>, 32, 0);
-    if (err != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, p2g_kernel, 32, 0) != cudaSuccess) {
         cudaGetLastError();
-        return lanes_per_cell == 2 ? kP2GPairWarpsPerSM : kP2GWarpsPerSM;
+        return kP2GWarpsPerSM;
     }
     return k;
-}
-
-int p2g_default_ctas_per_sm(int lanes_per_cell) {
-    return lanes_per_cell == 2 ? kP2GPairWarpsPerSM : kP2GWarpsPerSM;
 }
 
 int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const float* P, const int32_t* gidx,
                const int32_t* cstart, const BinSet& cur, const uint8_t* corder, const long long* itemoff,
                uint32_t* work, float4* accum, int4* crowd, int crowd_cap, uint32_t* status, cudaStream_t st,
-               int ctas_per_sm, int cell_cap, int lanes_per_cell) {
+               int ctas_per_sm, int cell_cap) {
     if (n <= 0) return 0;
-    const int pair = lanes_per_cell == 2 ? 2 : 1;
-    const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : p2g_default_ctas_per_sm(pair);
+    const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : kP2GWarpsPerSM;
     const int cap = cell_cap > 0 ? cell_cap : 0;
-    const int warps = (int)std::min(bins_total * kBinZ * pair, 148LL * per_sm);
-    if (pair == 2)
-        p2g_kernel<2><<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, corder, itemoff, work, accum, crowd, crowd_cap,
-                                            status, cap);
-    else
-        p2g_kernel<1><<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, corder, itemoff, work, accum, crowd, crowd_cap,
-                                            status, cap);
+    const int warps = (int)std::min(bins_total * kBinZ, 148LL * per_sm);
+    p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, corder, itemoff, work, accum, crowd, crowd_cap, status,
+                                     cap);
     p2g_crowd_kernel<<<148 * kP2GWarpsPerSM, 32, 0, st>>>(sc, P, gidx, crowd, crowd_cap, work, accum, status);
     return 2;
 }

@@ -69,7 +69,7 @@ class _LearnedStats(ctypes.Structure):
 class _Tuning(ctypes.Structure):
     _fields_ = [("p2g_ctas_per_sm", ctypes.c_int32), ("g2p_block", ctypes.c_int32), ("grid_block", ctypes.c_int32),
                 ("p2g_ms", ctypes.c_float), ("g2p_ms", ctypes.c_float), ("grid_ms", ctypes.c_float),
-                ("p2g_cell_cap", ctypes.c_int32), ("p2g_lanes_per_cell", ctypes.c_int32)]
+                ("p2g_cell_cap", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -432,9 +432,8 @@ class Engine:
         return {k: getattr(t, k) for k, _ in _Tuning._fields_}
 
     def set_tuning(self, p2g_ctas_per_sm: int = 12, g2p_block: int = 256, grid_block: int = 256,
-                   p2g_cell_cap: int = 0, p2g_lanes_per_cell: int = 1):
-        t = _Tuning(int(p2g_ctas_per_sm), int(g2p_block), int(grid_block), 0.0, 0.0, 0.0, int(p2g_cell_cap),
-                    int(p2g_lanes_per_cell))
+                   p2g_cell_cap: int = 0):
+        t = _Tuning(int(p2g_ctas_per_sm), int(g2p_block), int(grid_block), 0.0, 0.0, 0.0, int(p2g_cell_cap))
         self._check(lib.mpm_set_tuning(self._h, ctypes.byref(t)))
 
     # -- checkpoints ----------------------------------------------------------
