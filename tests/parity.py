@@ -2,8 +2,12 @@
 
 Tolerances (FP32 engine vs FP64 oracle, one substep, same inputs):
   * Morton keys and sort permutation: bit-exact.
-  * velocity, C, F: max |got - want| <= RTOL * max |want| over the field
+  * velocity, F: max |got - want| <= RTOL * max |want| over the field
     (normwise relative error, RTOL = 1e-5).
+  * C: the same, relative to max(max |C|, max |velocity|).  C = 4 sum w v
+    (x_node - x_p)^T is a velocity over one cell; in uniform flow (a scene at
+    rest under gravity) its terms cancel to near zero and what is left is the
+    rounding of the velocity terms, so a velocity is its natural scale.
   * positions: the error of the DISPLACEMENT, max |got - want| <=
     RTOL * max |want - start| + 2 ulp(|position|) (a position near 100 cannot
     be stored closer than its float spacing).
@@ -42,7 +46,8 @@ def assert_state_close(got, want, start, rtol=RTOL):
     err = float(np.max(np.abs(got[0:3] - want[0:3])))
     assert err <= rtol * disp + 2 * ulp, f"position: max error {err:.3e} > {rtol:g} x {disp:.3e} + 2 ulp"
     assert_normwise("velocity", got[3:6], want[3:6], rtol)
-    assert_normwise("C", got[6:15], want[6:15], rtol)
+    vmax = float(np.max(np.abs(want[3:6]))) if want.size else 0.0
+    assert_normwise("C", got[6:15], want[6:15], rtol, floor=max(vmax, 1e-12))
     assert_normwise("F", got[15:24], want[15:24], rtol)
     assert np.array_equal(np.asarray(got[24:26], np.float32), np.asarray(want[24:26], np.float32)), "VOL/MASS changed"
 

@@ -170,7 +170,11 @@ def test_sdf_wait_gives_up_and_engine_recovers(gpu_ok, mpm, oracle64, hook):
 def test_tcgen05_wait_gives_up_and_engine_recovers(gpu_ok, mpm, hook):
     from mpm_b200 import learned
     from mpm_b200 import scenes
-    cfg, st, tris = scenes.small_scene(4096, (32, 32, 32), seed=11)
+    # Water at rest in the physical orientation (the corrector's training
+    # regime): a large step of random C and F could invert F, which the
+    # reference's J < 0.3 rescue turns into NaN.
+    cfg, st, tris = scenes.small_scene(4096, (32, 32, 32), seed=11, randomize=False)
+    cfg = learned.physical_config(cfg)
     params, _ = learned.load_params(learned.PHYSICAL_PARAMS)
     with mpm.Engine(cfg) as ref_eng:
         ref_eng.init(st)
@@ -190,6 +194,7 @@ def test_tcgen05_wait_gives_up_and_engine_recovers(gpu_ok, mpm, hook):
         eng.init(st)  # the failed step's state is unspecified: start again
         eng.step_learned(1)
         got = eng.get_buffer()
+    assert np.isfinite(want).all()
     assert np.abs(got.astype(np.float64) - want).max() <= 1e-4 * max(1.0, np.abs(want).max())
 
 

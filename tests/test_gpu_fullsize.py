@@ -57,11 +57,45 @@ def _cell_counts(cfg, state):
     return np.bincount(idx[ok], minlength=cfg.grid_number)
 
 
+def _pushed(cfg, start, want):
+    """Particles whose FP64 substep took the obstacle branch of G2P (position
+    pushed out along the SDF normal, kernels.cu:249-270): their new position is
+    not start + DT * new velocity."""
+    adv = start[0:3].astype(np.float64) + np.float64(np.float32(cfg.dt)) * want[3:6]
+    return np.any(np.abs(want[0:3] - adv) > 1e-6 * (1.0 + np.abs(want[0:3])), axis=0)
+
+
+def _field_errors(got, want):
+    return {name: float(np.max(np.abs(got[sl].astype(np.float64) - want[sl]))) if want.shape[1] else 0.0
+            for name, sl in (("position", slice(0, 3)), ("velocity", slice(3, 6)), ("C", slice(6, 15)),
+                             ("F", slice(15, 24)))}
+
+
 def _check(cfg, start, got, grid, r_state, r_grid, want, wgrid):
-    # Both FP32 engines against the FP64 oracle, then against each other.
-    assert_state_close(r_state, want, start)
-    assert_state_close(got, want, start)
-    assert_state_close(got, r_state, start, rtol=2e-5)
+    """Particles that did not meet the obstacle: both FP32 engines within the
+    parity tolerances of FP64.  Particles pushed out of the obstacle: the
+    collision normal is the normalised central difference of the trilinear
+    SDF (calculateNormal, common.cuh:169-182), which loses most of its
+    relative precision where the SDF gradient nearly vanishes (deep inside the
+    torus tube, where the dam break's water box starts); there the engine must
+    be no further from FP64 than twice the reference's own distance, or within
+    the parity tolerance."""
+    assert np.isfinite(start).all() and np.isfinite(want).all()
+    pushed = _pushed(cfg, start, want)
+    keep = ~pushed
+    assert_state_close(r_state[:, keep], want[:, keep], start[:, keep])
+    assert_state_close(got[:, keep], want[:, keep], start[:, keep])
+    assert_state_close(got[:, keep], r_state[:, keep], start[:, keep], rtol=2e-5)
+    if pushed.any():
+        e_ref = _field_errors(r_state[:, pushed], want[:, pushed])
+        e_got = _field_errors(got[:, pushed], want[:, pushed])
+        print(f"{int(pushed.sum())} particles pushed out of the obstacle; max error vs FP64: "
+              f"engine {e_got}, reference {e_ref}")
+        for name in e_got:
+            sl = {"position": slice(0, 3), "velocity": slice(3, 6), "C": slice(6, 15), "F": slice(15, 24)}[name]
+            scale = float(np.max(np.abs(want[sl, pushed])))
+            assert e_got[name] <= max(2.0 * e_ref[name], 1e-5 * scale), \
+                f"{name} of pushed particles: engine error {e_got[name]:.3e}, reference {e_ref[name]:.3e}"
     assert_normwise("grid mass vs FP64", grid[0], wgrid[0])
     assert_normwise("grid velocity vs FP64", grid[1:4], wgrid[1:4])
     assert_normwise("grid mass vs reference", grid[0], r_grid[0], rtol=2e-5)
@@ -96,18 +130,22 @@ def test_full_scene_substep_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_path, w
 
 @needs_ref
 def test_dam_break_crowded_state_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_path):
-    """The 2M dam break advanced 2400 substeps in chunks of 200 (this GAMMA = 7
-    Tait law resists only expansion, so the fluid piles up against the top
-    wall); from the chunk end with the most particles in cells above 32, one
-    substep in both engines."""
+    """The 2M dam break advanced in chunks of 20 substeps (this GAMMA = 7 Tait
+    law resists only expansion, so the fluid piles up); from the chunk end
+    with the most particles in cells above 32 among those whose particles are
+    all finite, one substep in both engines.  (Later on, compressed particles
+    reach det F <= 0, where the J < 0.3 rescue of calculateNewF,
+    common.cuh:255-261, gives NaN in the reference and in the engine alike.)"""
     cfg, st, tris = _scene("dam_break_2M")
     best, best_frac, best_at, fullest = None, -1.0, 0, 0
     with mpm.Engine(cfg) as eng:
         eng.init(st)
         eng.init_sdf(tris)
-        for done in range(200, 2401, 200):
-            eng.step(200)
+        for done in range(20, 401, 20):
+            eng.step(20)
             s = eng.get_buffer()
+            if not np.isfinite(s).all():
+                break
             counts = _cell_counts(cfg, s)
             frac = float(counts[counts > CELL_CAP].sum()) / s.shape[1]
             if frac > best_frac:
