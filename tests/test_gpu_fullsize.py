@@ -79,8 +79,21 @@ def _check(cfg, start, got, grid, r_state, r_grid, want, wgrid):
     relative precision where the SDF gradient nearly vanishes (deep inside the
     torus tube, where the dam break's water box starts); there the engine must
     be no further from FP64 than twice the reference's own distance, or within
-    the parity tolerance."""
-    assert np.isfinite(start).all() and np.isfinite(want).all()
+    the parity tolerance.
+
+    Non-finite particles (det F <= 0 makes the J < 0.3 rescue of
+    calculateNewF, common.cuh:255-261, NaN, in the reference as here) must be
+    the same in both engines and FP64, up to a few whose det F lies at the
+    sign boundary; they take no further part.  Grid nodes that such particles
+    reach hold a NaN mass (and velocity 0: NaN > 1e-9 is false) in all three;
+    the comparison covers the finite nodes."""
+    bad_want = ~np.isfinite(want).all(0)
+    bad_got, bad_ref = ~np.isfinite(got).all(0), ~np.isfinite(r_state).all(0)
+    tol = max(10, int(bad_want.sum()) // 100)
+    assert int((bad_got ^ bad_want).sum()) <= tol, "non-finite particles differ from FP64"
+    assert int((bad_ref ^ bad_want).sum()) <= tol, "the reference's non-finite particles differ from FP64"
+    ok = np.isfinite(start).all(0) & ~bad_want & ~bad_got & ~bad_ref
+    start, got, r_state, want = start[:, ok], got[:, ok], r_state[:, ok], want[:, ok]
     pushed = _pushed(cfg, start, want)
     keep = ~pushed
     assert_state_close(r_state[:, keep], want[:, keep], start[:, keep])
@@ -96,12 +109,16 @@ def _check(cfg, start, got, grid, r_state, r_grid, want, wgrid):
             scale = float(np.max(np.abs(want[sl, pushed])))
             assert e_got[name] <= max(2.0 * e_ref[name], 1e-5 * scale), \
                 f"{name} of pushed particles: engine error {e_got[name]:.3e}, reference {e_ref[name]:.3e}"
-    assert_normwise("grid mass vs FP64", grid[0], wgrid[0])
-    assert_normwise("grid velocity vs FP64", grid[1:4], wgrid[1:4])
-    assert_normwise("grid mass vs reference", grid[0], r_grid[0], rtol=2e-5)
-    assert_normwise("grid velocity vs reference", grid[1:4], r_grid[1:4], rtol=2e-5)
-    total = float(np.sum(start[25], dtype=np.float64))
-    assert float(np.sum(grid[0], dtype=np.float64)) == pytest.approx(total, rel=1e-5)
+    nodes = np.isfinite(wgrid).all(0)
+    assert np.array_equal(nodes, np.isfinite(grid).all(0)), "non-finite grid nodes differ from FP64"
+    assert np.array_equal(nodes, np.isfinite(r_grid).all(0)), "the reference's non-finite grid nodes differ"
+    assert_normwise("grid mass vs FP64", grid[0, nodes], wgrid[0, nodes])
+    assert_normwise("grid velocity vs FP64", grid[1:4, nodes], wgrid[1:4, nodes])
+    assert_normwise("grid mass vs reference", grid[0, nodes], r_grid[0, nodes], rtol=2e-5)
+    assert_normwise("grid velocity vs reference", grid[1:4, nodes], r_grid[1:4, nodes], rtol=2e-5)
+    if nodes.all() and ok.all():
+        total = float(np.sum(start[25], dtype=np.float64))
+        assert float(np.sum(grid[0], dtype=np.float64)) == pytest.approx(total, rel=1e-5)
 
 
 @needs_ref
@@ -132,19 +149,20 @@ def test_full_scene_substep_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_path, w
 def test_dam_break_crowded_state_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_path):
     """The 2M dam break advanced in chunks of 20 substeps (this GAMMA = 7 Tait
     law resists only expansion, so the fluid piles up); from the chunk end
-    with the most particles in cells above 32 among those whose particles are
-    all finite, one substep in both engines.  (Later on, compressed particles
+    with the most particles in cells above 32 among those with at most 1 % of
+    non-finite particles, one substep in both engines.  (Compressed particles
     reach det F <= 0, where the J < 0.3 rescue of calculateNewF,
-    common.cuh:255-261, gives NaN in the reference and in the engine alike.)"""
+    common.cuh:255-261, gives NaN in the reference and in the engine alike;
+    from about substep 100 on their number grows quickly.)"""
     cfg, st, tris = _scene("dam_break_2M")
     best, best_frac, best_at, fullest = None, -1.0, 0, 0
     with mpm.Engine(cfg) as eng:
         eng.init(st)
         eng.init_sdf(tris)
-        for done in range(20, 401, 20):
+        for done in range(20, 201, 20):
             eng.step(20)
             s = eng.get_buffer()
-            if not np.isfinite(s).all():
+            if (~np.isfinite(s).all(0)).mean() > 0.01:
                 break
             counts = _cell_counts(cfg, s)
             frac = float(counts[counts > CELL_CAP].sum()) / s.shape[1]
@@ -158,13 +176,13 @@ def test_dam_break_crowded_state_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_pa
         eng.init(late)  # applies initFMatrices; set_state then loads the state as it is
         eng.init_sdf(tris)
         eng.set_state(late)
-        assert np.array_equal(eng.get_buffer(), late)
+        assert np.array_equal(eng.get_buffer(), late, equal_nan=True)
         eng.step(1)
         keys, perm = eng.get_sort()
         state, grid = eng.get_buffer(), eng.get_grid()
     ref.create(cfg, late, tris, str(tmp_path / "config.txt"))
     ref.set_state(late)
-    assert np.array_equal(ref.state(), late)
+    assert np.array_equal(ref.state(), late, equal_nan=True)
     r_keys, r_sdf = ref.keys(), ref.sdf()
     ref.step(1)
     r_state, r_grid, r_perm = ref.state(), ref.grid(), ref.perm()
