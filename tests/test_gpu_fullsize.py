@@ -7,9 +7,11 @@ oracle/_ref) from the same state, and the FP64 oracle restates the same
 substep: keys and sort permutation bit-exact between the two engines; state
 and grid of each engine within the parity tolerances of tests/parity.py
 against FP64 (which also pins the oracle against the reference at full
-size).  The dam break is checked again from a late, crowded state, where most
+size).  The dam break is checked again from a late, crowded state, where much
 of P2G's work runs through the crowded-cell list (cells above 32 particles),
-loaded into the reference engine as it is (no initFMatrices).
+loaded into the reference engine as it is (no initFMatrices); there the FP32
+results are ill-conditioned and the engine is held to the reference's own
+distance from FP64.
 
 Reference: Engine::step (engine.cu:54-70), p2GTransferScatter
 (kernels.cu:6-142), gridUpdate (kernels.cu:144-196), g2PTransfer
@@ -121,6 +123,38 @@ def _check(cfg, start, got, grid, r_state, r_grid, want, wgrid):
         assert float(np.sum(grid[0], dtype=np.float64)) == pytest.approx(total, rel=1e-5)
 
 
+def _check_reference_bounded(cfg, start, got, grid, r_state, r_grid, want, wgrid):
+    """For states in which the FP32 results themselves are ill-conditioned:
+    each of the engine's distances from FP64 (normwise per field, over the
+    particles finite in all three; the set of non-finite particles; the grid
+    over its finite nodes) must be within the parity tolerance or at most
+    twice the reference engine's own distance from FP64."""
+    bad_want = ~np.isfinite(want).all(0)
+    bad_got, bad_ref = ~np.isfinite(got).all(0), ~np.isfinite(r_state).all(0)
+    d_got, d_ref = int((bad_got ^ bad_want).sum()), int((bad_ref ^ bad_want).sum())
+    ok = np.isfinite(start).all(0) & ~bad_want & ~bad_got & ~bad_ref
+    e_got = _field_errors(got[:, ok], want[:, ok])
+    e_ref = _field_errors(r_state[:, ok], want[:, ok])
+    nodes = np.isfinite(wgrid).all(0) & np.isfinite(grid).all(0) & np.isfinite(r_grid).all(0)
+    g_got = {"mass": float(np.max(np.abs(grid[0, nodes] - wgrid[0, nodes]))),
+             "velocity": float(np.max(np.abs(grid[1:4, nodes] - wgrid[1:4, nodes])))}
+    g_ref = {"mass": float(np.max(np.abs(r_grid[0, nodes] - wgrid[0, nodes]))),
+             "velocity": float(np.max(np.abs(r_grid[1:4, nodes] - wgrid[1:4, nodes])))}
+    print(f"non-finite particles differing from FP64: engine {d_got}, reference {d_ref} "
+          f"(of {int(bad_want.sum())} in FP64); particle errors vs FP64: engine {e_got}, reference {e_ref}; "
+          f"grid errors: engine {g_got}, reference {g_ref}")
+    assert d_got <= max(10, 2 * d_ref), f"non-finite particles: engine {d_got} differ from FP64, reference {d_ref}"
+    scales = {"position": float(np.max(np.abs(want[0:3, ok]))), "velocity": float(np.max(np.abs(want[3:6, ok]))),
+              "C": float(np.max(np.abs(want[6:15, ok]))), "F": float(np.max(np.abs(want[15:24, ok])))}
+    for name in e_got:
+        assert e_got[name] <= max(2.0 * e_ref[name], 1e-5 * scales[name]), \
+            f"{name}: engine error {e_got[name]:.3e}, reference {e_ref[name]:.3e}"
+    for name, sl in (("mass", 0), ("velocity", slice(1, 4))):
+        scale = float(np.max(np.abs(wgrid[sl, nodes])))
+        assert g_got[name] <= max(2.0 * g_ref[name], 1e-5 * scale), \
+            f"grid {name}: engine error {g_got[name]:.3e}, reference {g_ref[name]:.3e}"
+
+
 @needs_ref
 @pytest.mark.parametrize("workload", ["sphere_drop", "dam_break_2M"])
 def test_full_scene_substep_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_path, workload):
@@ -189,4 +223,8 @@ def test_dam_break_crowded_state_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_pa
     assert np.array_equal(keys, r_keys), "Morton keys differ from the reference's setKeys"
     assert np.array_equal(perm, r_perm), "sort permutation differs from the reference's thrust sort"
     want, wgrid, _, _ = oracle64.substep(cfg, late.astype(np.float64), r_sdf.astype(np.float64))
-    _check(cfg, late, state, grid, r_state, r_grid, want, wgrid)
+    # In this state repeated J < 0.3 rescues have scaled up many deformation
+    # gradients, so det F and with it the clamped pressure and the sign test
+    # of the rescue are ill-conditioned in FP32: the reference's own result
+    # sets the bar.
+    _check_reference_bounded(cfg, late, state, grid, r_state, r_grid, want, wgrid)
