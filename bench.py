@@ -514,13 +514,18 @@ def run_engine(args, rank, world, local):
 def learned_leg(cfg, st, tris, device):
     """The learned 4xDT path beside the plain engine on the same scene: both
     from the same state, plain for 4 x 100 substeps, learned for 100 large
-    steps (density-change fallback at 2 %), simulated time per second of each
-    (host wall clock around synchronous calls: the learned step reads its
-    fallback statistic every large step), and the learned state's distance
-    from the plain one; "perturbed" is the plain run from positions moved by
-    1e-4 cells, the scene's chaos floor."""
+    steps, simulated time per second of each (host wall clock around
+    synchronous calls: a checked large step reads its fallback statistic), and
+    the learned state's distance from the plain one; "perturbed" is the plain
+    run from positions moved by 1e-4 cells, the scene's chaos floor.  Fallback
+    rules (Engine.set_fallback_rule) at 2 %: "rest_density" (the predicted
+    density's deviation from rest density), "density_change" (the density
+    change the step predicts), and none."""
     from mpm_b200 import learned as L
     out = {}
+    legs = {"literal": (("density_change_2pct", "density_change", 0.02), ("no_fallback", "density_change", -1.0)),
+            "physical": (("rest_density_2pct", "rest_density", 0.02),
+                         ("density_change_2pct", "density_change", 0.02), ("no_fallback", "density_change", -1.0))}
     for name, path, phys in (("literal", L.DEFAULT_PARAMS, False), ("physical", L.PHYSICAL_PARAMS, True)):
         if not os.path.exists(path):
             out[name] = {"unavailable": f"no trained corrector parameters ({os.path.basename(path)})"}
@@ -529,13 +534,14 @@ def learned_leg(cfg, st, tris, device):
         c = L.physical_config(cfg) if phys else cfg
         v = {"config": "GRAVITY and GAMMA as configured" if not phys else
              "physical orientation: GRAVITY and GAMMA negated (gravity pulls -y, pressure resists compression)"}
-        for thr in (0.02, -1.0):
+        for key, rule, thr in legs[name]:
             res = L.evaluate(c, st, tris, params, nlarge=100, ratio=int(meta.get("ratio", 4)),
-                             max_density_change=thr, checkpoints=(10, 25, 100))
-            key = "fallback_2pct" if thr >= 0 else "no_fallback"
-            r = {"speedup_sim_time": round(res["speedup_sim_time"], 3),
+                             max_density_change=thr, checkpoints=(10, 25, 100), rule=rule)
+            r = {"rule": rule if thr >= 0 else None, "threshold": thr if thr >= 0 else None,
+                 "speedup_sim_time": round(res["speedup_sim_time"], 3),
                  "sim_time_per_s": {k: round(res[k]["sim_time_per_s"], 2) for k in ("plain", "learned", "uncorrected")},
-                 "fallbacks": res["learned"].get("fallbacks")}
+                 "fallbacks": res["learned"].get("fallbacks"),
+                 "mean_statistics": {k: round(x, 5) for k, x in res["learned"].get("mean_statistics", {}).items()}}
             for tag in ("learned", "uncorrected", "perturbed"):
                 r[tag] = {m: {k: round(val, 4) for k, val in res[tag][f"at_{m}"].items()} for m in (10, 25, 100)}
             v[key] = r

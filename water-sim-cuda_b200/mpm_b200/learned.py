@@ -245,6 +245,8 @@ def main(argv=None):
     ev.add_argument("--physical", action="store_true")
     ev.add_argument("--seed", type=int, default=1235)
     ev.add_argument("--alpha", type=float, default=1.0, help="scale of the applied correction")
+    ev.add_argument("--rule", choices=["density_change", "rest_density", "rest_density_excess"],
+                    default="density_change", help="the fallback statistic")
     pr = sub.add_parser("probe", help="a few learned large steps on a thinned dam break (a small case to profile)")
     pr.add_argument("--params", default=PHYSICAL_PARAMS)
     pr.add_argument("--thin", type=int, default=5, help="keep every THIN-th particle")
@@ -316,7 +318,7 @@ def main(argv=None):
         if a.physical:
             cfg = physical_config(cfg)
         res = evaluate(cfg, st, tris, params, nlarge=a.large_steps, ratio=int(meta.get("ratio", 4)),
-                       max_density_change=a.threshold)
+                       max_density_change=a.threshold, rule=a.rule)
         res["alpha"] = a.alpha
         print(json.dumps(res))
 
