@@ -433,6 +433,18 @@ const char* mpm_renderer_last_error(const mpm_renderer* renderer);
 /* Background image (width x height RGB8, row 0 at the bottom) in place of
  * the clear colour: what the framebuffer held before the fluid pass. */
 mpm_status mpm_renderer_set_background(mpm_renderer* renderer, const uint8_t* rgb8_host);
+/* The obstacle pass (shaders/dot.vert + dot.frag, renderer.cpp:247-303, the
+ * default opaque mode): t triangles (9 floats each, grid coordinates, the
+ * same list as mpm_init_sdf) drawn once over the background with a depth
+ * test, flat Lambert shading 0.3 C + max(n . L, 0) C (rgb NULL: C = 0.5 grey)
+ * and stored as 8 bits; the fluid's composite is depth-tested against them.
+ * t = 0 removes them.  The glass and wireframe toggles are not restated; a
+ * triangle with a vertex behind the near plane is dropped (GL would clip it). */
+mpm_status mpm_renderer_set_obstacles(mpm_renderer* renderer, const float* tris_host, int64_t t,
+                                      const float* rgb_host);
+/* The background texture (RGB8, after the obstacle pass) and / or the
+ * obstacles' window depth in [0, 1] (1 where none); either may be NULL. */
+mpm_status mpm_renderer_get_background(mpm_renderer* renderer, uint8_t* rgb8_host, float* depth_host);
 /* All passes for n positions (float3, device memory), enqueued on `stream`. */
 mpm_status mpm_render_points(mpm_renderer* renderer, const float* xyz_device, int64_t n, void* stream);
 /* All passes for the engine's current positions, on the engine's stream. */

@@ -9,7 +9,13 @@ fluid passes, the checker of the library's mpm_render_* kernels.
   blur       shaders/ssf_blur.frag, horizontal then vertical, wrapping
              texture coordinates (GL_REPEAT)
   composite  shaders/screen.frag: normal from depth differences, refracted
-             background (bilinear, wrapping), Fresnel, specular
+             background (bilinear, wrapping), Fresnel, specular; depth-tested
+             against the obstacles (gl_FragDepth)
+  obstacles  shaders/dot.vert + dot.frag, the default opaque mode
+             (renderer.cpp:247-303): triangles rasterised at pixel centres
+             (top-left rule), depth test GL_LESS from 1, flat Lambert colour
+             0.3 C + max(n . L, 0) C with n the plane normal towards the eye,
+             8-bit framebuffer
 
 Arrays are (height, width[, 3]) with row 0 at the bottom (GL window
 coordinates), float32 throughout like the shaders.
@@ -61,6 +67,103 @@ def camera(width, height, grid, zoom=None, rotation=0.0, rotation_vertical=0.0, 
     L = np.array(light) / np.linalg.norm(light)
     lv = (view[:3, :3] @ L).astype(F)
     return mv, F(fy / (width / height)), F(fy), lv, F(near), F(far)
+
+
+def _model(grid, rotation=0.0, rotation_vertical=0.0):
+    cx, cy, cz = grid[0] / 2.0, grid[1] / 2.0, grid[2] / 2.0
+
+    def rot(a, axis):
+        c, sn = math.cos(a), math.sin(a)
+        x, y, z = axis
+        return np.array([[c + (1 - c) * x * x, (1 - c) * x * y - sn * z, (1 - c) * x * z + sn * y, 0],
+                         [(1 - c) * y * x + sn * z, c + (1 - c) * y * y, (1 - c) * y * z - sn * x, 0],
+                         [(1 - c) * z * x - sn * y, (1 - c) * z * y + sn * x, c + (1 - c) * z * z, 0],
+                         [0, 0, 0, 1.0]])
+
+    def tr(x, y, z):
+        m = np.eye(4)
+        m[:3, 3] = (x, y, z)
+        return m
+
+    return tr(cx, cy, cz) @ rot(rotation_vertical, (1, 0, 0)) @ rot(rotation, (0, 1, 0)) @ tr(-cx, -cy, -cz)
+
+
+def _unorm8(v):
+    return np.floor(np.clip(np.asarray(v, F), 0, 1) * F(255) + F(0.5)).astype(np.uint8)
+
+
+def obstacles(tris, width, height, grid, zoom=None, rotation=0.0, rotation_vertical=0.0, fov=45.0, near=0.1,
+              far=5000.0, light=(0.2, 10.0, 0.5), color=(0.5, 0.5, 0.5), clear=(0.85, 0.9, 0.95), background=None):
+    """The framebuffer after the obstacle pass: (RGB8 (h, w, 3), window depth (h, w), 1 where empty)."""
+    mv, p00, p11, _, near32, far32 = camera(width, height, grid, zoom, rotation, rotation_vertical, fov, near, far,
+                                            light)
+    p22 = F(-(far + near) / (far - near))
+    p32 = F(-(2.0 * far * near) / (far - near))
+    model = _model(grid, rotation, rotation_vertical)
+    zoom = grid[2] * 2.0 if zoom is None else zoom
+    eye = np.array([grid[0] / 2.0, grid[1] / 2.0, zoom])
+    L = np.array(light) / np.linalg.norm(light)
+    col = np.array(color, np.float64)
+    if background is None:
+        bg = np.broadcast_to(_unorm8(clear), (height, width, 3)).copy()
+    else:
+        bg = np.asarray(background, np.uint8).reshape(height, width, 3).copy()
+    depth = np.ones((height, width), F)
+    t = np.asarray(tris, F).reshape(-1, 9)
+    for i in range(len(t)):
+        V = t[i].reshape(3, 3)
+        X, Y, Z = np.zeros(3, F), np.zeros(3, F), np.zeros(3, F)
+        ok = True
+        for k in range(3):
+            x, y, z = V[k]
+            vx = ((mv[0, 0] * x + mv[0, 1] * y) + mv[0, 2] * z) + mv[0, 3]
+            vy = ((mv[1, 0] * x + mv[1, 1] * y) + mv[1, 2] * z) + mv[1, 3]
+            vz = ((mv[2, 0] * x + mv[2, 1] * y) + mv[2, 2] * z) + mv[2, 3]
+            wc = -vz
+            if not wc > near32:
+                ok = False
+                break
+            X[k] = (p00 * vx / wc * F(0.5) + F(0.5)) * F(width)
+            Y[k] = (p11 * vy / wc * F(0.5) + F(0.5)) * F(height)
+            Z[k] = (p22 * vz + p32) / wc * F(0.5) + F(0.5)
+        if not ok:
+            continue
+        area = (X[1] - X[0]) * (Y[2] - Y[0]) - (X[2] - X[0]) * (Y[1] - Y[0])
+        if area == 0 or not np.isfinite(area):
+            continue
+        sgn = F(1) if area > 0 else F(-1)
+        area = area * sgn
+        x0 = max(0, int(math.ceil(float(X.min()) - 0.5)))
+        x1 = min(width - 1, int(math.floor(float(X.max()) - 0.5)))
+        y0 = max(0, int(math.ceil(float(Y.min()) - 0.5)))
+        y1 = min(height - 1, int(math.floor(float(Y.max()) - 0.5)))
+        if x0 > x1 or y0 > y1:
+            continue
+        sx = (np.arange(x0, x1 + 1).astype(F) + F(0.5))[None, :]
+        sy = (np.arange(y0, y1 + 1).astype(F) + F(0.5))[:, None]
+        inside = np.ones((y1 - y0 + 1, x1 - x0 + 1), bool)
+        e = []
+        for k in range(3):
+            a, b = (k + 1) % 3, (k + 2) % 3
+            ek = ((X[b] - X[a]) * (sy - Y[a]) - (Y[b] - Y[a]) * (sx - X[a])) * sgn
+            ex, ey = (X[b] - X[a]) * sgn, (Y[b] - Y[a]) * sgn
+            tl = (ey == 0 and ex < 0) or ey < 0
+            inside &= (ek > 0) | ((ek == 0) & tl)
+            e.append(ek)
+        zw = ((e[0] * Z[0] + e[1] * Z[1]) + e[2] * Z[2]) / area
+        sub = depth[y0:y1 + 1, x0:x1 + 1]
+        win = inside & (zw >= 0) & (zw <= 1) & (zw < sub)
+        # flat colour: the plane normal in the model-rotated frame, towards the eye
+        W = (model[:3, :3] @ V.astype(np.float64).T).T + model[:3, 3]
+        n = np.cross(W[1] - W[0], W[2] - W[0])
+        if np.linalg.norm(n) > 0:
+            n = n / np.linalg.norm(n)
+        if n @ (eye - W[0]) < 0:
+            n = -n
+        c8 = _unorm8(0.3 * col + max(float(n @ L), 0.0) * col)
+        sub[win] = zw[win]
+        bg[y0:y1 + 1, x0:x1 + 1][win] = c8
+    return bg, depth
 
 
 def splat(xyz, width, height, cam, radius=2.0):
@@ -118,8 +221,8 @@ def blur(depth, axis, filter_size=10.0, falloff=0.01):
     return np.where(d > 5000, d, out)
 
 
-def composite(depth, cam, background=None, clear=(0.85, 0.9, 0.95)):
-    _, p00, p11, L, _, _ = cam
+def composite(depth, cam, background=None, clear=(0.85, 0.9, 0.95), obstacle_depth=None):
+    _, p00, p11, L, near, far = cam
     h, w = depth.shape
     if background is None:
         q = np.floor(np.clip(np.array(clear, F), 0, 1) * F(255) + F(0.5)).astype(np.uint8)
@@ -154,7 +257,14 @@ def composite(depth, cam, background=None, clear=(0.85, 0.9, 0.95)):
     a = (F(0.3) + fres * F(0.5))[..., None]
     water = np.array([0.1, 0.5, 0.8], F)
     col = b * (1 - a) + water * a + spec[..., None]
-    return np.where((depth > 5000)[..., None], bg, col).astype(F)
+    keep = depth > 5000
+    if obstacle_depth is not None:
+        p22 = F(-(float(far) + float(near)) / (float(far) - float(near)))
+        p32 = F(-(2.0 * float(far) * float(near)) / (float(far) - float(near)))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            fz = ((p22 * depth + p32) / -depth) * F(0.5) + F(0.5)
+        keep |= ~(fz < obstacle_depth)
+    return np.where(keep[..., None], bg, col).astype(F)
 
 
 def render(xyz, width, height, grid, **kw):

@@ -92,3 +92,41 @@ def test_render_engine_frame(gpu_ok, mpm):
         img, _ = r.image()
         d = r.depth(2)
     assert np.isfinite(img).all() and (d < 5000).any()
+
+
+def test_obstacle_pass_matches_oracle(gpu_ok, mpm, ro):
+    """The obstacle pass (dot.vert/dot.frag) against the numpy restatement:
+    coverage equal on at least 99.5 % of the pixels (pixel centres on a
+    triangle edge within float rounding may differ), window depth to 1e-5
+    and the 8-bit colour to 1 where both draw, then the fluid composite
+    depth-tested against the obstacles."""
+    from mpm_b200 import scenes
+    grid, w, h = (48, 48, 48), 200, 160
+    kw = dict(rotation=0.4, rotation_vertical=0.2)
+    tris = scenes.torus(12.0, 4.0, (25.0, 22.0, 24.0), 48, 24)
+    xyz = _points(2000, grid, 9)
+    with mpm.Renderer(grid, w, h, **kw) as r:
+        r.set_obstacles(tris)
+        bg, dep = r.background()
+        r.render_device(torch.from_numpy(xyz).cuda().data_ptr(), len(xyz))
+        torch.cuda.synchronize()
+        fin = r.depth(2)
+        img, _ = r.image()
+        r.set_obstacles(np.zeros((0, 9), np.float32))  # removed: the clear colour again
+        bg0, dep0 = r.background()
+    wbg, wdep = ro.obstacles(tris, w, h, grid, **kw)
+    cov, wcov = dep < 1.0, wdep < 1.0
+    assert wcov.mean() > 0.05
+    assert (cov == wcov).mean() > 0.995
+    both = cov & wcov
+    assert np.abs(dep[both] - wdep[both]).max() <= 1e-5
+    diff = np.abs(bg.astype(int) - wbg.astype(int)).max(-1)
+    assert (diff[both] <= 1).mean() > 0.995
+    assert (bg0 == [217, 230, 242]).all() and (dep0 == 1.0).all()
+    # The composite: the library's own blurred depth and background, so
+    # that only the composite's depth test and shading are compared.
+    cam = ro.camera(w, h, grid, **kw)
+    want = ro.composite(fin, cam, background=bg, obstacle_depth=dep)
+    hidden = (fin < 5000) & ~(np.abs(want - img).max(-1) < 2e-3)
+    assert hidden.mean() < 0.002
+    assert ((fin < 5000) & cov).any()  # some fluid lies in front of or behind the torus

@@ -21,13 +21,31 @@
 // Camera (renderer.cpp:95-96, 186-195): eye (SX/2, SY/2, zoom), looking at
 // the grid centre, up +y; model = rotation about the centre by the vertical
 // angle (x axis) then the horizontal angle (y axis); perspective 45 degrees,
-// near 0.1, far 5000.  Differences from the GL pipeline, where the
-// rasteriser's choices are not observable in the shaders: a sprite whose
-// centre lies outside the clip volume is dropped whole; depths are compared
-// as floats (GL's 24-bit depth buffer can keep the earlier of two fragments
-// closer than its resolution); the obstacle pass (dot.frag) is not part of
-// the image: the background is the clear colour as stored in the 8-bit
-// framebuffer, or an image the caller supplies.
+// near 0.1, far 5000.
+//
+//  0. Obstacles (dot.vert + dot.frag, renderer.cpp:247-303, the default
+//     opaque mode), drawn once per renderer into the background: each
+//     triangle in grid coordinates goes through the model, view and
+//     projection matrices, covers the pixels whose centres lie inside it
+//     (top-left rule on shared edges), and the depth test (GL_LESS, depth
+//     cleared to 1) keeps the nearest fragment, the earlier triangle on a
+//     tie.  Its colour is flat: dot.frag's normal, the cross product of the
+//     screen-space derivatives of the world position, is the triangle's plane
+//     normal turned towards the eye; colour = 0.3 C + max(n . L, 0) C with
+//     C = (0.5, 0.5, 0.5) and L the normalised world light, stored as 8 bits
+//     like the framebuffer that glCopyTexSubImage2D turns into the
+//     background texture.  The fluid's composite then passes the depth test
+//     against the obstacles' window depth (screen.frag's gl_FragDepth).
+//
+// Differences from the GL pipeline, where the rasteriser's choices are not
+// observable in the shaders: a sprite whose centre lies outside the clip
+// volume is dropped whole; an obstacle triangle with a vertex behind the
+// near plane is dropped whole (GL clips it); depths are compared as floats
+// (GL's 24-bit depth buffer can keep the earlier of two fragments closer
+// than its resolution); the glass and wireframe modes, keyboard toggles of
+// the interactive viewer, are not restated.  Without obstacles the
+// background is the clear colour as stored in the 8-bit framebuffer, or an
+// image the caller supplies.
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -151,13 +169,93 @@ __device__ float3 sample_rgb8(const unsigned char* __restrict__ img, int w, int 
     return r;
 }
 
+// One thread per obstacle triangle: the pixels whose centres it covers, as
+// 64-bit keys (window depth bits, triangle index) kept by atomicMin, so the
+// nearest fragment wins and, at equal depth, the earlier triangle.
+__global__ void obstacle_raster_kernel(const float* __restrict__ tris, int t, Cam c,
+                                       unsigned long long* __restrict__ key) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= t) return;
+    float X[3], Y[3], Z[3];
+    for (int k = 0; k < 3; ++k) {
+        const float x = tris[i * 9 + 3 * k], y = tris[i * 9 + 3 * k + 1], z = tris[i * 9 + 3 * k + 2];
+        const float vx = c.m[0] * x + c.m[4] * y + c.m[8] * z + c.m[12];
+        const float vy = c.m[1] * x + c.m[5] * y + c.m[9] * z + c.m[13];
+        const float vz = c.m[2] * x + c.m[6] * y + c.m[10] * z + c.m[14];
+        const float wc = -vz;
+        if (!(wc > c.near_clip)) return;  // GL would clip at the near plane
+        X[k] = (c.p00 * vx / wc * 0.5f + 0.5f) * (float)c.w;
+        Y[k] = (c.p11 * vy / wc * 0.5f + 0.5f) * (float)c.h;
+        Z[k] = (c.p22 * vz + c.p32) / wc * 0.5f + 0.5f;
+    }
+    float area = (X[1] - X[0]) * (Y[2] - Y[0]) - (X[2] - X[0]) * (Y[1] - Y[0]);
+    if (area == 0.0f || !isfinite(area)) return;
+    const float sgn = area > 0.0f ? 1.0f : -1.0f;
+    area *= sgn;
+    // Edge k runs from vertex k + 1 to k + 2; with the counter-clockwise
+    // orientation (sgn applied) a top edge is horizontal and points left, a
+    // left edge points down.
+    bool tl[3];
+    for (int k = 0; k < 3; ++k) {
+        const int a = (k + 1) % 3, b = (k + 2) % 3;
+        const float ex = (X[b] - X[a]) * sgn, ey = (Y[b] - Y[a]) * sgn;
+        tl[k] = (ey == 0.0f && ex < 0.0f) || ey < 0.0f;
+    }
+    const int x0 = max(0, (int)ceilf(fminf(X[0], fminf(X[1], X[2])) - 0.5f));
+    const int x1 = min(c.w - 1, (int)floorf(fmaxf(X[0], fmaxf(X[1], X[2])) - 0.5f));
+    const int y0 = max(0, (int)ceilf(fminf(Y[0], fminf(Y[1], Y[2])) - 0.5f));
+    const int y1 = min(c.h - 1, (int)floorf(fmaxf(Y[0], fmaxf(Y[1], Y[2])) - 0.5f));
+    for (int py = y0; py <= y1; ++py) {
+        const float sy = (float)py + 0.5f;
+        for (int px = x0; px <= x1; ++px) {
+            const float sx = (float)px + 0.5f;
+            float e[3];
+            bool in = true;
+            for (int k = 0; k < 3; ++k) {
+                const int a = (k + 1) % 3, b = (k + 2) % 3;
+                e[k] = ((X[b] - X[a]) * (sy - Y[a]) - (Y[b] - Y[a]) * (sx - X[a])) * sgn;
+                in = in && (e[k] > 0.0f || (e[k] == 0.0f && tl[k]));
+            }
+            if (!in) continue;
+            const float zw = (e[0] * Z[0] + e[1] * Z[1] + e[2] * Z[2]) / area;
+            if (!(zw >= 0.0f && zw <= 1.0f)) continue;
+            atomicMin(key + (size_t)py * c.w + px,
+                      ((unsigned long long)__float_as_uint(zw) << 32) | (unsigned long long)(unsigned)i);
+        }
+    }
+}
+
+// The framebuffer after the obstacle pass: the winning triangle's flat
+// colour over the base image, and its window depth (1 where none).
+__global__ void obstacle_resolve_kernel(const unsigned long long* __restrict__ key,
+                                        const unsigned char* __restrict__ tri_rgb8,
+                                        const unsigned char* __restrict__ base, long long npix,
+                                        unsigned char* __restrict__ bg, float* __restrict__ odepth) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    const unsigned long long k = key[i];
+    if (k == ~0ull) {
+        for (int c = 0; c < 3; ++c) bg[i * 3 + c] = base[i * 3 + c];
+        odepth[i] = 1.0f;
+        return;
+    }
+    const unsigned tri = (unsigned)(k & 0xffffffffull);
+    for (int c = 0; c < 3; ++c) bg[i * 3 + c] = tri_rgb8[(size_t)tri * 3 + c];
+    odepth[i] = __uint_as_float((unsigned)(k >> 32));
+}
+
 __global__ void composite_kernel(const float* __restrict__ depth, const unsigned char* __restrict__ bg, int w, int h,
-                                 float p00, float p11, float lx, float ly, float lz, float* __restrict__ rgb) {
+                                 float p00, float p11, float p22, float p32, float lx, float ly, float lz,
+                                 const float* __restrict__ odepth, float* __restrict__ rgb) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= w || y >= h) return;
     const size_t o = ((size_t)y * w + x) * 3;
     const float d = depth[(size_t)y * w + x];
-    if (d > 5000.0f) {  // discard: the framebuffer keeps the background
+    // discard, or the fluid surface behind an obstacle (gl_FragDepth of
+    // screen.frag against the obstacles' depth, GL_LESS): the framebuffer
+    // keeps the background
+    const bool hidden = odepth && !(((p22 * d + p32) / -d) * 0.5f + 0.5f < odepth[(size_t)y * w + x]);
+    if (d > 5000.0f || hidden) {
         for (int c = 0; c < 3; ++c) rgb[o + c] = bg[o + c] / 255.0f;
         return;
     }
@@ -229,7 +327,13 @@ struct mpm_renderer {
     float* tmp = nullptr;    // after the horizontal blur
     float* fin = nullptr;    // after the vertical blur
     float* rgb = nullptr;
-    unsigned char* bg = nullptr;
+    unsigned char* bg = nullptr;       // the background texture: base + obstacles
+    unsigned char* base = nullptr;     // clear colour or the caller's image
+    float* odepth = nullptr;           // obstacles' window depth; null without obstacles
+    unsigned long long* okey = nullptr;
+    float* otris = nullptr;            // obstacle triangles (grid coordinates)
+    unsigned char* ocolor = nullptr;   // their flat colours, 8 bits
+    int ntris = 0;
     std::string last_error;
 };
 
@@ -346,6 +450,7 @@ mpm_status mpm_renderer_create(const mpm_render_params* params, int32_t device, 
     if (err == cudaSuccess) err = cudaMalloc(&r->fin, npix * sizeof(float));
     if (err == cudaSuccess) err = cudaMalloc(&r->rgb, npix * 3 * sizeof(float));
     if (err == cudaSuccess) err = cudaMalloc(&r->bg, npix * 3);
+    if (err == cudaSuccess) err = cudaMalloc(&r->base, npix * 3);
     if (err != cudaSuccess) {
         cudaGetLastError();
         return bad(rfail(nullptr, MPM_ERR_OUT_OF_MEMORY, std::string("renderer allocation: ") + cudaGetErrorString(err)));
@@ -353,7 +458,8 @@ mpm_status mpm_renderer_create(const mpm_render_params* params, int32_t device, 
     std::vector<unsigned char> bg(npix * 3);
     for (size_t i = 0; i < npix; ++i)
         for (int c = 0; c < 3; ++c) bg[i * 3 + c] = unorm8(p.clear_color[c]);
-    if (cudaMemcpy(r->bg, bg.data(), bg.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpy(r->bg, bg.data(), bg.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(r->base, bg.data(), bg.size(), cudaMemcpyHostToDevice) != cudaSuccess)
         return bad(rfail(nullptr, MPM_ERR_CUDA, "background upload"));
     *out = r;
     return MPM_OK;
@@ -362,17 +468,111 @@ mpm_status mpm_renderer_create(const mpm_render_params* params, int32_t device, 
 void mpm_renderer_destroy(mpm_renderer* r) {
     if (!r) return;
     cudaSetDevice(r->device);
-    for (void* p : {(void*)r->zbuf, (void*)r->depth, (void*)r->tmp, (void*)r->fin, (void*)r->rgb, (void*)r->bg})
+    for (void* p : {(void*)r->zbuf, (void*)r->depth, (void*)r->tmp, (void*)r->fin, (void*)r->rgb, (void*)r->bg,
+                    (void*)r->base, (void*)r->odepth, (void*)r->okey, (void*)r->otris, (void*)r->ocolor})
         if (p) cudaFree(p);
     delete r;
 }
 
 const char* mpm_renderer_last_error(const mpm_renderer* r) { return r ? r->last_error.c_str() : ""; }
 
+// Draws the obstacle triangles (if any) over the base image into the
+// background texture and the obstacle depth buffer; without obstacles the
+// background is the base image.
+static mpm_status draw_background(mpm_renderer* r) {
+    const size_t npix = (size_t)r->prm.width * r->prm.height;
+    if (r->ntris == 0) {
+        RK(r, cudaMemcpy(r->bg, r->base, npix * 3, cudaMemcpyDeviceToDevice));
+        return MPM_OK;
+    }
+    RK(r, cudaMemset(r->okey, 0xff, npix * sizeof(unsigned long long)));
+    obstacle_raster_kernel<<<(r->ntris + 127) / 128, 128>>>(r->otris, r->ntris, r->cam, r->okey);
+    obstacle_resolve_kernel<<<(unsigned)((npix + 255) / 256), 256>>>(r->okey, r->ocolor, r->base, (long long)npix, r->bg,
+                                                                     r->odepth);
+    RK(r, cudaGetLastError());
+    RK(r, cudaDeviceSynchronize());
+    return MPM_OK;
+}
+
 mpm_status mpm_renderer_set_background(mpm_renderer* r, const uint8_t* rgb8_host) {
     if (!r || !rgb8_host) return rfail(r, MPM_ERR_INVALID_ARGUMENT, "renderer and image must be non-NULL");
     RK(r, cudaSetDevice(r->device));
-    RK(r, cudaMemcpy(r->bg, rgb8_host, (size_t)r->prm.width * r->prm.height * 3, cudaMemcpyHostToDevice));
+    RK(r, cudaMemcpy(r->base, rgb8_host, (size_t)r->prm.width * r->prm.height * 3, cudaMemcpyHostToDevice));
+    return draw_background(r);
+}
+
+mpm_status mpm_renderer_set_obstacles(mpm_renderer* r, const float* tris_host, int64_t t, const float* rgb_host) {
+    if (!r || t < 0 || (t > 0 && !tris_host) || t > 0x7fffffffLL)
+        return rfail(r, MPM_ERR_INVALID_ARGUMENT, "bad obstacle arguments");
+    RK(r, cudaSetDevice(r->device));
+    for (void** p : {(void**)&r->otris, (void**)&r->ocolor, (void**)&r->okey, (void**)&r->odepth})
+        if (*p) {
+            cudaFree(*p);
+            *p = nullptr;
+        }
+    r->ntris = 0;
+    if (t == 0) return draw_background(r);
+    // Flat colours (dot.frag): the world frame is the model-rotated grid
+    // frame, the eye sits at (SX/2, SY/2, zoom) in it, the light direction is
+    // the normalised world light.
+    const mpm_render_params& p = r->prm;
+    float M[16], T[16];
+    const float cx = p.grid[0] / 2.0f, cy = p.grid[1] / 2.0f, cz = p.grid[2] / 2.0f;
+    translation(M, cx, cy, cz);
+    rotation(T, p.rotation_vertical, 1, 0, 0);
+    mat_mul(M, T, M);
+    rotation(T, p.rotation, 0, 1, 0);
+    mat_mul(M, T, M);
+    translation(T, -cx, -cy, -cz);
+    mat_mul(M, T, M);
+    const float eye[3] = {cx, cy, p.zoom_distance};
+    float L[3] = {p.light_dir[0], p.light_dir[1], p.light_dir[2]};
+    const float ll = std::sqrt(L[0] * L[0] + L[1] * L[1] + L[2] * L[2]);
+    for (float& v : L) v /= ll;
+    const float col[3] = {rgb_host ? rgb_host[0] : 0.5f, rgb_host ? rgb_host[1] : 0.5f, rgb_host ? rgb_host[2] : 0.5f};
+    std::vector<unsigned char> rgb8((size_t)t * 3);
+    for (int64_t i = 0; i < t; ++i) {
+        float w[3][3];
+        for (int k = 0; k < 3; ++k) {
+            const float* v = tris_host + i * 9 + 3 * k;
+            for (int a = 0; a < 3; ++a) w[k][a] = M[a] * v[0] + M[4 + a] * v[1] + M[8 + a] * v[2] + M[12 + a];
+        }
+        const float e1[3] = {w[1][0] - w[0][0], w[1][1] - w[0][1], w[1][2] - w[0][2]};
+        const float e2[3] = {w[2][0] - w[0][0], w[2][1] - w[0][1], w[2][2] - w[0][2]};
+        float n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        const float nl = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (nl > 0.0f)
+            for (float& v : n) v /= nl;
+        const float toward = n[0] * (eye[0] - w[0][0]) + n[1] * (eye[1] - w[0][1]) + n[2] * (eye[2] - w[0][2]);
+        if (toward < 0.0f)
+            for (float& v : n) v = -v;
+        const float diff = std::max(n[0] * L[0] + n[1] * L[1] + n[2] * L[2], 0.0f);
+        for (int c = 0; c < 3; ++c) rgb8[(size_t)i * 3 + c] = unorm8(0.3f * col[c] + diff * col[c]);
+    }
+    const size_t npix = (size_t)p.width * p.height;
+    RK(r, cudaMalloc(&r->otris, (size_t)t * 9 * sizeof(float)));
+    RK(r, cudaMalloc(&r->ocolor, (size_t)t * 3));
+    RK(r, cudaMalloc(&r->okey, npix * sizeof(unsigned long long)));
+    RK(r, cudaMalloc(&r->odepth, npix * sizeof(float)));
+    RK(r, cudaMemcpy(r->otris, tris_host, (size_t)t * 9 * sizeof(float), cudaMemcpyHostToDevice));
+    RK(r, cudaMemcpy(r->ocolor, rgb8.data(), rgb8.size(), cudaMemcpyHostToDevice));
+    r->ntris = (int)t;
+    return draw_background(r);
+}
+
+mpm_status mpm_renderer_get_background(mpm_renderer* r, uint8_t* rgb8_host, float* depth_host) {
+    if (!r) return rfail(r, MPM_ERR_INVALID_ARGUMENT, "renderer is NULL");
+    RK(r, cudaSetDevice(r->device));
+    RK(r, cudaDeviceSynchronize());
+    const size_t npix = (size_t)r->prm.width * r->prm.height;
+    if (rgb8_host) RK(r, cudaMemcpy(rgb8_host, r->bg, npix * 3, cudaMemcpyDeviceToHost));
+    if (depth_host) {
+        if (r->odepth) {
+            RK(r, cudaMemcpy(depth_host, r->odepth, npix * sizeof(float), cudaMemcpyDeviceToHost));
+        } else {
+            for (size_t i = 0; i < npix; ++i) depth_host[i] = 1.0f;
+        }
+    }
     return MPM_OK;
 }
 
@@ -388,8 +588,8 @@ mpm_status mpm_render_points(mpm_renderer* r, const float* xyz_device, int64_t n
     const dim3 blk(32, 8), grd((w + 31) / 32, (h + 7) / 8);
     blur_kernel<<<grd, blk, 0, st>>>(r->depth, r->tmp, w, h, 1, 0, r->prm.filter_size, r->prm.depth_falloff);
     blur_kernel<<<grd, blk, 0, st>>>(r->tmp, r->fin, w, h, 0, 1, r->prm.filter_size, r->prm.depth_falloff);
-    composite_kernel<<<grd, blk, 0, st>>>(r->fin, r->bg, w, h, r->cam.p00, r->cam.p11, r->light[0], r->light[1],
-                                          r->light[2], r->rgb);
+    composite_kernel<<<grd, blk, 0, st>>>(r->fin, r->bg, w, h, r->cam.p00, r->cam.p11, r->cam.p22, r->cam.p32,
+                                          r->light[0], r->light[1], r->light[2], r->odepth, r->rgb);
     RK(r, cudaGetLastError());
     return MPM_OK;
 }

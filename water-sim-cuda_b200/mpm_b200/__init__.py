@@ -206,6 +206,8 @@ def _load() -> ctypes.CDLL:
         "mpm_renderer_destroy": (None, [P]),
         "mpm_renderer_last_error": (ctypes.c_char_p, [P]),
         "mpm_renderer_set_background": (I32, [P, P]),
+        "mpm_renderer_set_obstacles": (I32, [P, P, I64, P]),
+        "mpm_renderer_get_background": (I32, [P, P, P]),
         "mpm_render_points": (I32, [P, P, I64, P]),
         "mpm_render_frame": (I32, [P, P]),
         "mpm_renderer_get_depth": (I32, [P, I32, P]),
@@ -834,6 +836,20 @@ class Renderer:
     def set_background(self, rgb8: np.ndarray):
         a = np.ascontiguousarray(rgb8, np.uint8).reshape(self.height, self.width, 3)
         self._check(lib.mpm_renderer_set_background(self._h, _ptr(a)))
+
+    def set_obstacles(self, triangles: np.ndarray, rgb=None):
+        """The obstacle pass (dot.vert/dot.frag): (t, 9) triangles in grid coordinates."""
+        t = np.ascontiguousarray(triangles, np.float32).reshape(-1, 9)
+        c = None if rgb is None else np.ascontiguousarray(rgb, np.float32).reshape(3)
+        self._check(lib.mpm_renderer_set_obstacles(self._h, _ptr(t) if len(t) else None, len(t),
+                                                   _ptr(c) if c is not None else None))
+
+    def background(self):
+        """(background RGB8 (h, w, 3), obstacle window depth (h, w)), row 0 at the bottom."""
+        b = np.empty((self.height, self.width, 3), np.uint8)
+        d = np.empty((self.height, self.width), np.float32)
+        self._check(lib.mpm_renderer_get_background(self._h, _ptr(b), _ptr(d)))
+        return b, d
 
     def render_device(self, xyz_ptr: int, n: int, stream: int = 0):
         self._check(lib.mpm_render_points(self._h, ctypes.c_void_p(xyz_ptr), int(n), ctypes.c_void_p(stream)))
