@@ -520,6 +520,28 @@ void orc_make_sdf(const orc_params* p, const real* tris, long t, real* sdf, real
     }
 }
 
+/* makeSDF at `count` chosen nodes (grid indices `nodes`): the same per-node
+ * loop as orc_make_sdf, for grids whose full SDF is too costly on the CPU. */
+void orc_make_sdf_nodes(const orc_params* p, const real* tris, long t, const long* nodes, long count, real* sdf,
+                        real* wn_out) {
+    const real four_pi_ref = (real)(4.0f * 3.1415f);
+    long k;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (k = 0; k < count; ++k) {
+        const long idx = nodes[k];
+        const real P[3] = {(real)(idx % p->sx), (real)((idx / p->sx) % p->sy), (real)(idx / ((long)p->sx * p->sy))};
+        real wsum = 0, dmin = (real)1e30f;
+        for (long i = 0; i < t; ++i) {
+            wsum += solid_angle(P, tris + 9 * i);
+            const real d2 = tri_dist2(P, tris + 9 * i);
+            if (d2 < dmin) dmin = d2;
+        }
+        const real wn = wsum / four_pi_ref;
+        sdf[k] = (wn > (real)0.5f ? -1 : 1) * (real)sqrt((double)dmin);
+        if (wn_out) wn_out[k] = wn;
+    }
+}
+
 int orc_real_bytes(void) { return (int)sizeof(real); }
 
 int orc_threads(void) {

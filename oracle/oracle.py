@@ -51,7 +51,8 @@ class Oracle:
             ("orc_sort_perm", V, [P, L, P]), ("orc_p2g", V, [P, P, L, P, P, ctypes.c_int]),
             ("orc_grid_update", V, [P, P, P]), ("orc_g2p", V, [P, P, L, P, P, P]),
             ("orc_substep", V, [P, P, L, P, P, P, P, ctypes.c_int]), ("orc_positions", V, [P, L, P]),
-            ("orc_make_sdf", V, [P, P, L, P, P]), ("orc_real_bytes", ctypes.c_int, []),
+            ("orc_make_sdf", V, [P, P, L, P, P]), ("orc_make_sdf_nodes", V, [P, P, L, P, L, P, P]),
+            ("orc_real_bytes", ctypes.c_int, []),
             ("orc_threads", ctypes.c_int, []), ("orc_set_threads", V, [ctypes.c_int]),
         ]:
             f = getattr(self.lib, name)
@@ -122,6 +123,15 @@ class Oracle:
         sdf = np.empty(cfg.grid_number, self.dtype)
         wn = np.empty(cfg.grid_number, self.dtype)
         self.lib.orc_make_sdf(ctypes.byref(_params(cfg)), _p(t), t.size // 9, _p(sdf), _p(wn))
+        return sdf, wn
+
+    def make_sdf_nodes(self, cfg, tris, nodes):
+        """(sdf, winding number) at the grid nodes `nodes` (flat indices)."""
+        t = np.ascontiguousarray(tris, self.dtype).reshape(-1)
+        idx = np.ascontiguousarray(nodes, np.int64)
+        sdf = np.empty(idx.size, self.dtype)
+        wn = np.empty(idx.size, self.dtype)
+        self.lib.orc_make_sdf_nodes(ctypes.byref(_params(cfg)), _p(t), t.size // 9, _p(idx), idx.size, _p(sdf), _p(wn))
         return sdf, wn
 
     def empty_sdf(self, cfg):

@@ -962,71 +962,125 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
     axis_weights(fx, 1.0f, wx);
     axis_weights(fy, 1.0f, wy);
     axis_weights(fz, 1.0f, wz);
-    // Interpolation sums (g2PTransfer's loop, kernels.cu:214-235), separable
-    // per axis.  With o = (a, b, c) the node offset and x_node - x_p =
-    // (o - 1) - (f - 1):
+    // Interpolation sums (g2PTransfer's loop, kernels.cu:214-235).  The plain,
+    // large and collection modes take them separably per axis: with o =
+    // (a, b, c) the node offset and x_node - x_p = (o - 1) - (f - 1),
     //   v' = sum w v,   C' = 4 (M - v' (f - 1)^T),   M[k][d] = sum w v_k (o_d - 1),
-    // and each row of three nodes along x is reduced first (S0 = sum_a wx v,
-    // S1 = sum_a wx (a - 1) v) before its weight wy wz is applied: about half
-    // the arithmetic of summing node by node.
-    float tv[3] = {0.f, 0.f, 0.f}, M[9], tc[9], tm = 0.f;
+    // each row of three nodes along x reduced first (S0 = sum_a wx v, S1 =
+    // sum_a wx (a - 1) v) before its weight wy wz is applied: a quarter fewer
+    // instructions.  The learned modes sum node by node (the reference's
+    // form), which holds fewer values live next to the MLP's registers: the
+    // row form made the tcgen05 learned G2P spill three times as much and run
+    // 7 % slower.
+    float tv[3] = {0.f, 0.f, 0.f}, tc[9], tm = 0.f;
     // Set when a stencil node lies outside the grid or inside an obstacle:
     // only then can the SDF at the new position be negative (see below).
     uint32_t sdf_risk = 0u;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) M[k] = 0.f;
     const int plane = p.sx * p.sy;
     // Whole stencil inside the grid (almost every particle): no per-node
     // bounds tests.  Nodes outside the grid add nothing.
     const bool inside = p.sx >= 3 && p.sy >= 3 && p.sz >= 3 && (unsigned)bx <= (unsigned)(p.sx - 3) &&
                         (unsigned)by <= (unsigned)(p.sy - 3) && (unsigned)bz <= (unsigned)(p.sz - 3);
+    constexpr bool kRowSums = kMode != kG2PLearned && kMode != kG2PLearnedTc;
+    if constexpr (kRowSums) {
+        float M[9];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
+        for (int k = 0; k < 9; ++k) M[k] = 0.f;
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
-            const int z = bz + c, y = by + b;
-            float4 g[3];
-            if (inside) {
-                const float4* row = vgrid + ((size_t)z * plane + (size_t)y * p.sx + bx);
+        for (int c = 0; c < 3; ++c) {
 #pragma unroll
-                for (int a = 0; a < 3; ++a) g[a] = __ldg(row + a);
-            } else {
-                const bool zy = (unsigned)z < (unsigned)p.sz && (unsigned)y < (unsigned)p.sy;
+            for (int b = 0; b < 3; ++b) {
+                const int z = bz + c, y = by + b;
+                float4 g[3];
+                if (inside) {
+                    const float4* row = vgrid + ((size_t)z * plane + (size_t)y * p.sx + bx);
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    const bool ok = zy && (unsigned)(bx + a) < (unsigned)p.sx;
-                    g[a] = ok ? __ldg(vgrid + ((size_t)z * plane + (size_t)y * p.sx + bx + a))
-                              : make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (!ok) sdf_risk = 1u;
+                    for (int a = 0; a < 3; ++a) g[a] = __ldg(row + a);
+                } else {
+                    const bool zy = (unsigned)z < (unsigned)p.sz && (unsigned)y < (unsigned)p.sy;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const bool ok = zy && (unsigned)(bx + a) < (unsigned)p.sx;
+                        g[a] = ok ? __ldg(vgrid + ((size_t)z * plane + (size_t)y * p.sx + bx + a))
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (!ok) sdf_risk = 1u;
+                    }
                 }
-            }
-            sdf_risk |= (__float_as_uint(g[0].x) | __float_as_uint(g[1].x) | __float_as_uint(g[2].x)) >> 31;
-            const float s0[3] = {wx[0] * g[0].y + wx[1] * g[1].y + wx[2] * g[2].y,
-                                 wx[0] * g[0].z + wx[1] * g[1].z + wx[2] * g[2].z,
-                                 wx[0] * g[0].w + wx[1] * g[1].w + wx[2] * g[2].w};
-            const float s1[3] = {wx[2] * g[2].y - wx[0] * g[0].y, wx[2] * g[2].z - wx[0] * g[0].z,
-                                 wx[2] * g[2].w - wx[0] * g[0].w};
-            const float wyz = wy[b] * wz[c];
+                sdf_risk |= (__float_as_uint(g[0].x) | __float_as_uint(g[1].x) | __float_as_uint(g[2].x)) >> 31;
+                const float s0[3] = {wx[0] * g[0].y + wx[1] * g[1].y + wx[2] * g[2].y,
+                                     wx[0] * g[0].z + wx[1] * g[1].z + wx[2] * g[2].z,
+                                     wx[0] * g[0].w + wx[1] * g[1].w + wx[2] * g[2].w};
+                const float s1[3] = {wx[2] * g[2].y - wx[0] * g[0].y, wx[2] * g[2].z - wx[0] * g[0].z,
+                                     wx[2] * g[2].w - wx[0] * g[0].w};
+                const float wyz = wy[b] * wz[c];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                tv[k] += wyz * s0[k];
-                M[3 * k + 0] += wyz * s1[k];
-                if (b == 0) M[3 * k + 1] -= wyz * s0[k];
-                if (b == 2) M[3 * k + 1] += wyz * s0[k];
-                if (c == 0) M[3 * k + 2] -= wyz * s0[k];
-                if (c == 2) M[3 * k + 2] += wyz * s0[k];
+                for (int k = 0; k < 3; ++k) {
+                    tv[k] += wyz * s0[k];
+                    M[3 * k + 0] += wyz * s1[k];
+                    if (b == 0) M[3 * k + 1] -= wyz * s0[k];
+                    if (b == 2) M[3 * k + 1] += wyz * s0[k];
+                    if (c == 0) M[3 * k + 2] -= wyz * s0[k];
+                    if (c == 2) M[3 * k + 2] += wyz * s0[k];
+                }
+                if constexpr (kMode != kG2PPlain)
+                    tm += wyz * (wx[0] * fabsf(g[0].x) + wx[1] * fabsf(g[1].x) + wx[2] * fabsf(g[2].x));
             }
-            if constexpr (kMode != kG2PPlain)
-                tm += wyz * (wx[0] * fabsf(g[0].x) + wx[1] * fabsf(g[1].x) + wx[2] * fabsf(g[2].x));
         }
-    }
-    {
         const float gx = fx - 1.0f, gy = fy - 1.0f, gz = fz - 1.0f;  // exact
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             tc[3 * k + 0] = 4.0f * (M[3 * k + 0] - tv[k] * gx);
             tc[3 * k + 1] = 4.0f * (M[3 * k + 1] - tv[k] * gy);
             tc[3 * k + 2] = 4.0f * (M[3 * k + 2] - tv[k] * gz);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) tc[k] = 0.f;
+        // One node of the stencil, offsets (a, b, c), `row` = node (base x, y, z).
+        auto gather = [&](int a, int b, int c, const float4* row) {
+            const float dxv = -(fx - (float)a), dyv = -(fy - (float)b), dzv = -(fz - (float)c);
+            const float4 g = __ldg(row + a);
+            sdf_risk |= __float_as_uint(g.x) >> 31;
+            const float w = wx[a] * wy[b] * wz[c];
+            tv[0] += w * g.y;
+            tv[1] += w * g.z;
+            tv[2] += w * g.w;
+            tm += w * fabsf(g.x);
+            const float term = 4.0f * w;
+            tc[0] += term * g.y * dxv;
+            tc[1] += term * g.y * dyv;
+            tc[2] += term * g.y * dzv;
+            tc[3] += term * g.z * dxv;
+            tc[4] += term * g.z * dyv;
+            tc[5] += term * g.z * dzv;
+            tc[6] += term * g.w * dxv;
+            tc[7] += term * g.w * dyv;
+            tc[8] += term * g.w * dzv;
+        };
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int z = bz + c;
+            if (!inside && (unsigned)z >= (unsigned)p.sz) {
+                sdf_risk = 1u;
+                continue;
+            }
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const int y = by + b;
+                if (!inside && (unsigned)y >= (unsigned)p.sy) {
+                    sdf_risk = 1u;
+                    continue;
+                }
+                const float4* row = vgrid + ((size_t)z * plane + (size_t)y * p.sx + bx);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    if (!inside && (unsigned)(bx + a) >= (unsigned)p.sx) {
+                        sdf_risk = 1u;
+                        continue;
+                    }
+                    gather(a, b, c, row);
+                }
+            }
         }
     }
     if constexpr (kMode == kG2PLearned || kMode == kG2PCollect || kMode == kG2PLearnedTc) {
