@@ -16,10 +16,14 @@ def _meshes():
         "torus": ((48, 32, 48), scenes.torus(12.0, 4.0, (24.3, 15.9, 23.8), 24, 12)),
         "box": ((32, 24, 40), scenes.box_mesh((10.5, 6.25, 14.0), (15.5, 12.1, 20.3))),
         "sphere_257tris": ((24, 24, 24), scenes.uv_sphere(7.0, (12.0, 12.0, 12.0), 17, 8)),
+        # edges that are no multiple of the 8 x 8 x 4 node bricks, two shapes
+        # in one list (1,200 triangles, five tiles of the sorted copy)
+        "two_shapes_ragged": ((30, 21, 27), np.concatenate([
+            scenes.torus(7.0, 2.5, (14.3, 10.2, 13.1), 24, 12), scenes.uv_sphere(3.5, (5.1, 5.2, 20.7), 24, 13)])),
     }
 
 
-@pytest.mark.parametrize("name", ["sphere", "torus", "box", "sphere_257tris"])
+@pytest.mark.parametrize("name", ["sphere", "torus", "box", "sphere_257tris", "two_shapes_ragged"])
 def test_sdf_matches_oracle(gpu_ok, mpm, oracle64, name):
     from mpm_b200 import scenes
     size, tris = _meshes()[name]
@@ -61,3 +65,25 @@ def test_sdf_dam_break_torus(gpu_ok, mpm, oracle64):
     err = np.abs(got[62:66].astype(np.float64) - want)[ok]
     assert err.max() <= 1e-4
     assert (want < 0).sum() > 100
+
+
+def test_sdf_scale_scene_sampled(gpu_ok, mpm, oracle64):
+    """The 256^3 scene with its three obstacles (3,276 triangles): the SDF at
+    6,000 random nodes and 6,000 random nodes within 3 cells of a surface
+    against the FP64 oracle at the same nodes."""
+    from mpm_b200 import scenes
+    cfg, st, tris = scenes.scale_scene(1236)
+    with mpm.Engine(cfg) as eng:
+        eng.init(st[:, :1000])
+        eng.init_sdf(tris)
+        sdf = eng.get_sdf()
+    rng = np.random.default_rng(3)
+    near = np.flatnonzero(np.abs(sdf) < 3.0)
+    assert near.size > 6000
+    idx = np.concatenate([rng.choice(sdf.size, 6000, replace=False), rng.choice(near, 6000, replace=False)])
+    want, wn = oracle64.make_sdf_nodes(cfg, tris.astype(np.float64), idx)
+    ok = np.abs(wn - 0.5) >= 1e-3
+    assert ok.mean() > 0.999
+    err = np.abs(sdf[idx].astype(np.float64) - want)[ok]
+    assert err.max() <= 1e-4, f"max SDF error {err.max():.3e} cells"
+    assert (want < 0).any()

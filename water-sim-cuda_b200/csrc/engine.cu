@@ -896,19 +896,30 @@ extern "C" mpm_status mpm_scene_init_sdf(mpm_engine* e, int32_t scene, const flo
         CK(e, cudaStreamSynchronize(e->stream));
         return MPM_OK;
     }
-    // cudaMalloc: 256-byte aligned, as the kernel's 16-byte bulk copies need;
-    // 16 spare bytes cover the last tile's copy rounded up to 16 bytes.
+    // One allocation: the triangles as given, then the sorted copy with its
+    // tile boxes (sdf.cu).  cudaMalloc: 256-byte aligned, as the kernel's
+    // 16-byte bulk copies need; each part starts on a 16-byte boundary and 16
+    // spare bytes cover the last tile's copy rounded up to 16 bytes.
     const size_t bytes = (size_t)t * 9 * sizeof(float);
+    const size_t off = align_up(bytes, 16) + 16;
+    const size_t aux_floats = mpm::sdf_aux_floats((int)t);
+    std::vector<float> aux(aux_floats, 0.0f);
+    mpm::sdf_prepare_host(tris, (int)t, aux.data());
     float* d_tris = nullptr;
-    CK(e, cudaMalloc(&d_tris, align_up(bytes, 16) + 16));
-    cudaError_t err = cudaMemsetAsync(d_tris, 0, align_up(bytes, 16) + 16, e->stream);
+    CK(e, cudaMalloc(&d_tris, off + aux_floats * sizeof(float) + 16));
+    float* d_aux = reinterpret_cast<float*>(reinterpret_cast<char*>(d_tris) + off);
+    cudaError_t err = cudaMemsetAsync(d_tris, 0, off + aux_floats * sizeof(float) + 16, e->stream);
     if (err == cudaSuccess) err = cudaMemcpyAsync(d_tris, tris, bytes, cudaMemcpyHostToDevice, e->stream);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(d_aux, aux.data(), aux_floats * sizeof(float), cudaMemcpyHostToDevice, e->stream);
     if (err == cudaSuccess) {
-        e->kernel_launches += mpm::launch_sdf_build(p, d_tris, (int)t, sdf, e->d_flags + 1, e->stream,
+        e->kernel_launches += mpm::launch_sdf_build(p, d_tris, d_aux, (int)t, sdf, e->d_flags + 1, e->stream,
                                                     e->wait_test & (MPM_WAIT_TEST_SDF_GIVE_UP | MPM_WAIT_TEST_SDF_EXPIRE));
         err = cudaGetLastError();
     }
+    // aux is pageable host memory: the synchronisation below ends its copy.
     const mpm_status s2 = err != cudaSuccess ? cuda_fail(e, err, "sdf build") : sync_and_collect(e);
+    if (err != cudaSuccess) cudaStreamSynchronize(e->stream);
     cudaFree(d_tris);
     return s2;
 }

@@ -139,11 +139,16 @@ int launch_positions_export(const SimParams& p, const float* P, const int32_t* s
 int launch_grid_export(const SimParams& p, const float4* grid, float* planes4, cudaStream_t st);
 
 // ----------------------------------------------------------------- sdf ----
-// tris: 9*t floats on the device, allocation padded by >= 16 bytes.
+// tris: 9*t floats on the device, allocation padded by >= 16 bytes.  aux:
+// sdf_aux_floats(t) floats on the device (16-byte aligned, padded by >= 16
+// bytes) holding what sdf_prepare_host wrote: the triangles sorted by the
+// Morton code of their centroids and a bounding box per 256 of them.
 // wait_test: test hooks of the first triangle tile's wait (kWaitTestGiveUp /
 // kWaitTestExpire, corrector_tc.cuh), acted on after the real completion.
-int launch_sdf_build(const SimParams& p, const float* tris, int t, float* sdf, uint32_t* status, cudaStream_t st,
-                     uint32_t wait_test = 0u);
+size_t sdf_aux_floats(int t);
+void sdf_prepare_host(const float* tris, int t, float* aux);
+int launch_sdf_build(const SimParams& p, const float* tris, const float* aux, int t, float* sdf, uint32_t* status,
+                     cudaStream_t st, uint32_t wait_test = 0u);
 int launch_fill(float* dst, long long count, float value, cudaStream_t st);
 // dst[i] = i for i < n.
 int launch_identity(int32_t* dst, int n, cudaStream_t st);

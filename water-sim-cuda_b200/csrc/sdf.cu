@@ -1,13 +1,29 @@
 // Signed distance field of the obstacle triangles on the simulation grid
 // (makeSDF, kernels.cu:282-300; Engine::initSDF, engine.cu:105-114).
 //
-// One thread per node at integer coordinates.  Every CTA streams the whole
-// triangle list through shared memory in tiles of 256 triangles: one thread
-// issues a bulk async copy (cp.async.bulk, the 1-D TMA path) of the next tile
-// into the second buffer while the CTA evaluates the current one, and
-// completion is tracked by an mbarrier.  Each wait gives up after a fixed
-// time, records kStatusTimeout and drains the copies still in flight before
-// the CTA returns, so a lost completion cannot hang the device.
+// One thread per node at integer coordinates, a CTA per brick of 8 x 8 x 4
+// nodes, in two passes over the triangles:
+//
+//  1. the winding number: every triangle, in the order given (the sign of
+//     the SDF needs all of them).  The CTA streams the list through shared
+//     memory in tiles of 256 triangles: one thread issues a bulk async copy
+//     (cp.async.bulk, the 1-D TMA path) of the next tile into the second
+//     buffer while the CTA evaluates the current one, completion tracked by
+//     an mbarrier.  Each node also keeps the least squared distance to a
+//     triangle's first vertex, a point on the mesh, hence an upper bound of
+//     its distance to the mesh.
+//  2. the distance: the triangles again, in a copy sorted by the Morton code
+//     of their centroids, whose 256-triangle tiles carry bounding boxes.  A
+//     tile whose box lies farther from the brick than the brick's largest
+//     bound cannot hold any node's nearest triangle and is skipped by the
+//     whole CTA; within a loaded tile, a node skips a triangle whose
+//     bounding box lies farther than its distance so far.  The minimum is
+//     taken over the same per-pair values as a pass over every triangle, so
+//     the result is the same.
+//
+// Each wait gives up after a fixed time, records kStatusTimeout and drains
+// the copies still in flight before the CTA returns, so a lost completion
+// cannot hang the device.
 //
 // Per node-triangle pair the kernel adds the signed solid angle
 // (Van Oosterom & Strackee, 1983) and keeps the minimum squared distance to
@@ -15,6 +31,10 @@
 // Collision Detection" 5.1.5), in triangle order like the reference.  The
 // node is inside when the winding number, the solid-angle sum divided by
 // 4 * 3.1415 (the reference's constant, kernels.cu:298), exceeds 0.5.
+#include <algorithm>
+#include <utility>
+#include <vector>
+
 #include "kernels.h"
 
 namespace mpm {
@@ -23,6 +43,8 @@ namespace {
 constexpr int kSdfThreads = 256;
 constexpr int kTriTile = 256;                 // triangles per stage
 constexpr int kTriFloats = 9;
+// Floats rounded up to a 16-byte multiple (bulk copies start 16-byte aligned).
+constexpr size_t align_floats16(size_t n) { return (n + 3) & ~(size_t)3; }
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per wait
 constexpr unsigned long long kSdfTestWaitNs = 20000000ull;  // the test hook's expiring wait: 20 ms
 // Test hooks (the engine's wait test, the values of kWaitTest* in
@@ -136,14 +158,34 @@ __device__ __forceinline__ float tri_dist2(float px, float py, float pz, const f
     return dot3(qx, qy, qz, qx, qy, qz);
 }
 
+constexpr int kBrickX = 8, kBrickY = 8, kBrickZ = 4;  // kSdfThreads nodes per CTA
+static_assert(kBrickX * kBrickY * kBrickZ == kSdfThreads, "one node per thread");
+constexpr int kBoxFloats = 8;  // tile box: min x, y, z, max x, y, z, 2 unused
+
+// Squared distance between two boxes (0 when they overlap).
+__device__ __forceinline__ float box_dist2(float ax0, float ay0, float az0, float ax1, float ay1, float az1,
+                                           const float* b) {
+    const float dx = fmaxf(0.0f, fmaxf(b[0] - ax1, ax0 - b[3]));
+    const float dy = fmaxf(0.0f, fmaxf(b[1] - ay1, ay0 - b[4]));
+    const float dz = fmaxf(0.0f, fmaxf(b[2] - az1, az0 - b[5]));
+    return dx * dx + dy * dy + dz * dz;
+}
+
 __global__ void __launch_bounds__(kSdfThreads) sdf_build_kernel(SimParams p, const float* __restrict__ tris,
-                                                                int t_count, float* __restrict__ sdf,
+                                                                const float* __restrict__ sorted,
+                                                                const float* __restrict__ boxes, int t_count,
+                                                                float* __restrict__ sdf,
                                                                 uint32_t* __restrict__ status, uint32_t wait_test) {
     __shared__ __align__(128) float s_tri[2][kTriTile * kTriFloats];
     __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ float s_red[kSdfThreads / 32];
 
-    const int node = blockIdx.x * kSdfThreads + threadIdx.x;
-    const int x = node % p.sx, y = (node / p.sx) % p.sy, z = node / (p.sx * p.sy);
+    const int nbx = (p.sx + kBrickX - 1) / kBrickX, nby = (p.sy + kBrickY - 1) / kBrickY;
+    const int bxi = blockIdx.x % nbx, byi = (blockIdx.x / nbx) % nby, bzi = blockIdx.x / (nbx * nby);
+    const int t = threadIdx.x;
+    const int x = bxi * kBrickX + t % kBrickX, y = byi * kBrickY + (t / kBrickX) % kBrickY,
+              z = bzi * kBrickZ + t / (kBrickX * kBrickY);
+    const bool valid = x < p.sx && y < p.sy && z < p.sz;
     const float px = x * 1.0f, py = y * 1.0f, pz = z * 1.0f;
     const int ntiles = (t_count + kTriTile - 1) / kTriTile;
 
@@ -154,22 +196,23 @@ __global__ void __launch_bounds__(kSdfThreads) sdf_build_kernel(SimParams p, con
     }
     __syncthreads();
 
-    auto issue = [&](int tile) {
-        const int b = tile & 1;
+    auto issue = [&](const float* src, int tile, int b) {
         const int cnt = min(kTriTile, t_count - tile * kTriTile);
         const uint32_t bytes = (uint32_t)((cnt * kTriFloats * 4 + 15) & ~15);
         proxy_fence_shared();
         mbar_expect_tx(&s_bar[b], bytes);
-        bulk_copy_g2s(s_tri[b], tris + (size_t)tile * kTriTile * kTriFloats, bytes, &s_bar[b]);
+        bulk_copy_g2s(s_tri[b], src + (size_t)tile * kTriTile * kTriFloats, bytes, &s_bar[b]);
     };
 
-    if (threadIdx.x == 0 && ntiles > 0) issue(0);
-    float wsum = 0.0f, dmin2 = 1e30f;
+    // Pass 1: winding number over every triangle in order, and an upper bound
+    // of the distance (first vertices).
+    if (threadIdx.x == 0 && ntiles > 0) issue(tris, 0, 0);
+    float wsum = 0.0f, ub2 = 1e30f;
     bool aborted = false;
     int tile = 0;
     for (; tile < ntiles; ++tile) {
         const int b = tile & 1;
-        if (threadIdx.x == 0 && tile + 1 < ntiles) issue(tile + 1);
+        if (threadIdx.x == 0 && tile + 1 < ntiles) issue(tris, tile + 1, (tile + 1) & 1);
         bool ok = mbar_wait_bounded(&s_bar[b], (uint32_t)((tile >> 1) & 1));
         if (ok && tile == 0 && wait_test) {
             // Test hooks, with tile 0's copy landed: report a give-up, or
@@ -187,10 +230,9 @@ __global__ void __launch_bounds__(kSdfThreads) sdf_build_kernel(SimParams p, con
         const float* st = s_tri[b];
         for (int k = 0; k < cnt; ++k) {
             const float* tr = st + k * kTriFloats;
-            wsum += solid_angle(tr[0] - px, tr[1] - py, tr[2] - pz, tr[3] - px, tr[4] - py, tr[5] - pz,
-                                tr[6] - px, tr[7] - py, tr[8] - pz);
-            const float d2 = tri_dist2(px, py, pz, tr);
-            if (d2 < dmin2) dmin2 = d2;
+            const float ax = tr[0] - px, ay = tr[1] - py, az = tr[2] - pz;
+            wsum += solid_angle(ax, ay, az, tr[3] - px, tr[4] - py, tr[5] - pz, tr[6] - px, tr[7] - py, tr[8] - pz);
+            ub2 = fminf(ub2, ax * ax + ay * ay + az * az);
         }
         __syncthreads();
     }
@@ -204,19 +246,124 @@ __global__ void __launch_bounds__(kSdfThreads) sdf_build_kernel(SimParams p, con
         __syncthreads();
         return;
     }
-    if (node < p.g) {
+    // The brick's bound: no node of it is farther from the mesh than this,
+    // with a margin for the rounding of the bound and of the box distances.
+    float bound = valid ? ub2 : 0.0f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bound = fmaxf(bound, __shfl_xor_sync(0xffffffffu, bound, o));
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = bound;
+    __syncthreads();
+    bound = s_red[0];
+#pragma unroll
+    for (int w = 1; w < kSdfThreads / 32; ++w) bound = fmaxf(bound, s_red[w]);
+    bound = bound * 1.0001f + 1e-6f;
+    const float bx0 = bxi * kBrickX, by0 = byi * kBrickY, bz0 = bzi * kBrickZ;
+    const float bx1 = bx0 + (kBrickX - 1), by1 = by0 + (kBrickY - 1), bz1 = bz0 + (kBrickZ - 1);
+
+    // Pass 2: distance over the sorted tiles that can hold a nearest
+    // triangle, one tile at a time through buffer 0, whose barrier has
+    // completed (ntiles + 1) / 2 phases in pass 1.
+    uint32_t phase = (uint32_t)(((ntiles + 1) / 2) & 1);
+    float dmin2 = 1e30f;
+    for (int k = 0; k < ntiles; ++k) {
+        if (box_dist2(bx0, by0, bz0, bx1, by1, bz1, boxes + (size_t)k * kBoxFloats) > bound) continue;
+        if (threadIdx.x == 0) issue(sorted, k, 0);
+        const bool ok = mbar_wait_bounded(&s_bar[0], phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicOr(status, kStatusTimeout);
+                mbar_wait_bounded(&s_bar[0], phase ^ 1u);  // drain the copy
+            }
+            __syncthreads();
+            return;
+        }
+        const int cnt = min(kTriTile, t_count - k * kTriTile);
+        const float* st = s_tri[0];
+        for (int q = 0; q < cnt; ++q) {
+            const float* tr = st + q * kTriFloats;
+            const float lo[3] = {fminf(tr[0], fminf(tr[3], tr[6])), fminf(tr[1], fminf(tr[4], tr[7])),
+                                 fminf(tr[2], fminf(tr[5], tr[8]))};
+            const float hi[3] = {fmaxf(tr[0], fmaxf(tr[3], tr[6])), fmaxf(tr[1], fmaxf(tr[4], tr[7])),
+                                 fmaxf(tr[2], fmaxf(tr[5], tr[8]))};
+            const float dx = fmaxf(0.0f, fmaxf(lo[0] - px, px - hi[0]));
+            const float dy = fmaxf(0.0f, fmaxf(lo[1] - py, py - hi[1]));
+            const float dz = fmaxf(0.0f, fmaxf(lo[2] - pz, pz - hi[2]));
+            if ((dx * dx + dy * dy + dz * dz) * 0.9999f > dmin2) continue;
+            const float d2 = tri_dist2(px, py, pz, tr);
+            if (d2 < dmin2) dmin2 = d2;
+        }
+        __syncthreads();
+    }
+    if (valid) {
         const float wn = wsum / (4.0f * 3.1415f);
-        sdf[node] = (wn > 0.5f ? -1.0f : 1.0f) * sqrtf(dmin2);
+        sdf[node_index(p, x, y, z)] = (wn > 0.5f ? -1.0f : 1.0f) * sqrtf(dmin2);
     }
 }
 
 }  // namespace
 
-int launch_sdf_build(const SimParams& p, const float* tris, int t, float* sdf, uint32_t* status, cudaStream_t st,
-                     uint32_t wait_test) {
+// Morton code of a point in [0, 1)^3, 10 bits per axis.
+static uint32_t morton10(float x, float y, float z) {
+    auto spread = [](uint32_t v) {
+        v = (v * 0x00010001u) & 0xFF0000FFu;
+        v = (v * 0x00000101u) & 0x0F00F00Fu;
+        v = (v * 0x00000011u) & 0xC30C30C3u;
+        v = (v * 0x00000005u) & 0x49249249u;
+        return v;
+    };
+    auto q = [](float f) { return (uint32_t)std::min(1023.0f, std::max(0.0f, f * 1024.0f)); };
+    return (spread(q(z)) << 2) | (spread(q(y)) << 1) | spread(q(x));
+}
+
+size_t sdf_aux_floats(int t) {
+    const size_t tiles = (size_t)(t + kTriTile - 1) / kTriTile;
+    return align_floats16((size_t)t * kTriFloats) + tiles * kBoxFloats;
+}
+
+void sdf_prepare_host(const float* tris, int t, float* aux) {
+    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+    for (int i = 0; i < t; ++i)
+        for (int k = 0; k < 9; ++k) {
+            lo[k % 3] = std::min(lo[k % 3], tris[i * 9 + k]);
+            hi[k % 3] = std::max(hi[k % 3], tris[i * 9 + k]);
+        }
+    std::vector<std::pair<uint32_t, int>> key((size_t)t);
+    for (int i = 0; i < t; ++i) {
+        float c[3];
+        for (int a = 0; a < 3; ++a) {
+            const float mid = (tris[i * 9 + a] + tris[i * 9 + 3 + a] + tris[i * 9 + 6 + a]) / 3.0f;
+            const float ext = hi[a] - lo[a];
+            c[a] = ext > 0.0f ? (mid - lo[a]) / ext : 0.0f;
+        }
+        key[i] = {morton10(c[0], c[1], c[2]), i};
+    }
+    std::stable_sort(key.begin(), key.end());
+    float* sorted = aux;
+    float* boxes = aux + align_floats16((size_t)t * kTriFloats);
+    for (int i = 0; i < t; ++i) std::copy(tris + (size_t)key[i].second * 9, tris + (size_t)key[i].second * 9 + 9, sorted + (size_t)i * 9);
+    const int tiles = (t + kTriTile - 1) / kTriTile;
+    for (int k = 0; k < tiles; ++k) {
+        float* b = boxes + (size_t)k * kBoxFloats;
+        b[0] = b[1] = b[2] = 1e30f;
+        b[3] = b[4] = b[5] = -1e30f;
+        b[6] = b[7] = 0.0f;
+        for (int i = k * kTriTile; i < std::min(t, (k + 1) * kTriTile); ++i)
+            for (int v = 0; v < 9; ++v) {
+                b[v % 3] = std::min(b[v % 3], sorted[(size_t)i * 9 + v]);
+                b[3 + v % 3] = std::max(b[3 + v % 3], sorted[(size_t)i * 9 + v]);
+            }
+    }
+}
+
+int launch_sdf_build(const SimParams& p, const float* tris, const float* aux, int t, float* sdf, uint32_t* status,
+                     cudaStream_t st, uint32_t wait_test) {
     if (p.g <= 0) return 0;
-    sdf_build_kernel<<<(p.g + kSdfThreads - 1) / kSdfThreads, kSdfThreads, 0, st>>>(p, tris, t, sdf, status,
-                                                                                     wait_test);
+    const int bricks = ((p.sx + kBrickX - 1) / kBrickX) * ((p.sy + kBrickY - 1) / kBrickY) *
+                       ((p.sz + kBrickZ - 1) / kBrickZ);
+    const float* sorted = aux;
+    const float* boxes = aux + align_floats16((size_t)t * kTriFloats);
+    sdf_build_kernel<<<bricks, kSdfThreads, 0, st>>>(p, tris, sorted, boxes, t, sdf, status, wait_test);
     return 1;
 }
 
