@@ -476,7 +476,9 @@ def run_engine(args, rank, world, local):
         e2e_s = dist.max(t1 - t0)
         frames = [1e3 * (b - a) for a, b in zip(marks[1:-1], marks[2:])]
         e2e = {"value": world * n * sub * args.steps / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": int(26 * 4 * n / args.steps), "d2h_bytes_per_step": 12 * n,
+               # mpm_init_particles copies the 21 planes its import reads (not
+               # F's diagonal, VOL or MASS, which the init rules set)
+               "h2d_bytes_per_step": int(21 * 4 * n / args.steps), "d2h_bytes_per_step": 12 * n,
                "timed": "mpm_init_particles(pinned host state) + K x (mpm_step_async(SUBSTEPS) + "
                         "positions read back to pinned memory: mpm_get_positions_async, one frame's copy "
                         "overlapping the next frame's substeps) + the final synchronisation; host wall "

@@ -460,10 +460,24 @@ mpm_status load_states(mpm_engine* e, const float* const* soa26_host, bool init_
     for (int s = 0; s < e->scenes; ++s) {
         const SimParams& p = e->prm[s];
         if (p.n <= 0) continue;
-        const size_t bytes = (size_t)MPM_PARTICLE_PLANES * p.n * sizeof(float);
-        mpm_status st = ensure_staging(e, bytes);
+        const size_t plane = (size_t)p.n * sizeof(float);
+        mpm_status st = ensure_staging(e, (size_t)MPM_PARTICLE_PLANES * plane);
         if (st != MPM_OK) return st;
-        CK(e, cudaMemcpyAsync(e->staging, soa26_host[s], bytes, cudaMemcpyHostToDevice, e->stream));
+        // Only the planes the import reads cross the bus: VOL and MASS are
+        // uniform and live in SimParams, and with the init rules
+        // (initFMatrices) F's diagonal is overwritten with 1 (21 of 26
+        // planes; the import reads the skipped diagonal planes and discards
+        // them).
+        const char* src = reinterpret_cast<const char*>(soa26_host[s]);
+        char* dst = reinterpret_cast<char*>(e->staging);
+        if (init_rules) {
+            const int runs[3][2] = {{0, MPM_F00}, {MPM_F00 + 1, MPM_F00 + 4}, {MPM_F00 + 5, MPM_F00 + 8}};
+            for (const auto& r : runs)
+                CK(e, cudaMemcpyAsync(dst + r[0] * plane, src + r[0] * plane, (size_t)(r[1] - r[0]) * plane,
+                                      cudaMemcpyHostToDevice, e->stream));
+        } else {
+            CK(e, cudaMemcpyAsync(dst, src, (size_t)MPM_VOL * plane, cudaMemcpyHostToDevice, e->stream));
+        }
         e->kernel_launches += mpm::launch_state_import(p, e->staging, e->P[0] + p.poff * mpm::kAFloats,
                                                        e->sigma[0] + p.poff, init_rules, e->stream);
         CK(e, cudaGetLastError());
