@@ -620,6 +620,16 @@ mpm_status mpm_step_learned(mpm_engine* engine, int32_t nlarge, mpm_learned_stat
 #define MPM_FALLBACK_REST_DENSITY 1
 #define MPM_FALLBACK_REST_DENSITY_EXCESS 2
 mpm_status mpm_set_fallback_rule(mpm_engine* engine, int32_t rule);
+/* Where a checked large step (a corrector set, max_density_change >= 0) is
+ * accepted or rejected.  On the device (1, the default): each large step is
+ * one CUDA graph (large step, a one-thread decision kernel, and a conditional
+ * node whose body is the fallback: RATIO plain substeps from the start state,
+ * then the result moved to where an accepted step leaves its own), so a call
+ * of nlarge steps reads back only its counters, once.  On the host (0): the
+ * statistic is read back after every large step and the fallback enqueued
+ * from the host.  Both give the same results; after device-decided steps
+ * mpm_get_sort reports the sort of the current state. */
+mpm_status mpm_set_fallback_on_device(mpm_engine* engine, int32_t on_device);
 /* The three means above (in that order: |1/J - 1|, |rho/rho0/J - 1|,
  * |rho/rho0 - 1|) of the last large step that was checked. */
 mpm_status mpm_learned_statistics(mpm_engine* engine, double* out3);

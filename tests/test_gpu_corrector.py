@@ -259,3 +259,34 @@ def test_learned_step_tcgen05_matches_mma_sync(gpu_ok, mpm):
     a, b = out[True], out[False]
     assert np.abs(a[3:6] - b[3:6]).max() < 2e-3 * max(1.0, float(np.abs(b[3:6]).max()))
     assert np.abs(a[0:3] - b[0:3]).max() < 2e-3
+
+
+@pytest.mark.parametrize("threshold", [0.0, 1e9])
+def test_device_decided_fallback_matches_host(gpu_ok, mpm, threshold):
+    """The checked large step decided on the device (one graph per step: the
+    large step, the decision kernel and a conditional node whose body is the
+    fallback) against the same steps decided on the host, over three large
+    steps: every step rejected (threshold 0) or every one accepted (1e9).
+    Counters, statistics and states agree (to the rounding of the float
+    atomics, whose order differs between runs)."""
+    cfg, st, tris = _small(mpm, obstacle=True, seed=21, randomize=False)
+    w = mlp_ref.random_params(10)
+    out = {}
+    for on_device in (False, True):
+        with mpm.Engine(cfg) as e:
+            e.init(st)
+            e.init_sdf(tris)
+            e.set_corrector(w, ratio=4, max_density_change=threshold)
+            e.set_fallback_on_device(on_device)
+            stats = e.step_learned(2)
+            stats = e.step_learned(1)
+            out[on_device] = (stats, e.learned_statistics(), e.get_buffer(), e.stats()["substeps"], e.get_positions())
+    (sh, lh, bh, nh, ph), (sd, ld, bd, nd, pd) = out[False], out[True]
+    assert sh["large_steps"] == sd["large_steps"] and sh["fallbacks"] == sd["fallbacks"]
+    assert (sd["fallbacks"], sd["large_steps"]) == ((3, 0) if threshold == 0.0 else (0, 3))
+    assert nh == nd == (12 if threshold == 0.0 else 0)
+    for k in lh:
+        assert ld[k] == pytest.approx(lh[k], rel=1e-3, abs=1e-6)
+    assert np.isfinite(bd).all()
+    assert np.abs(bd.astype(np.float64) - bh).max() <= 1e-4 * max(1.0, np.abs(bh).max())
+    assert np.array_equal(pd, bd[0:3].T)

@@ -164,6 +164,16 @@ struct mpm_engine {
     int64_t fallbacks = 0;
     double last_density_change = 0.0;
     int fallback_rule = MPM_FALLBACK_DENSITY_CHANGE;
+    // The checked learned step with its fallback decided on the device: a
+    // graph per parity (large step, decision, conditional fallback body).
+    bool fallback_on_device = true;
+    cudaGraph_t lgraph_src[2] = {nullptr, nullptr};
+    cudaGraphExec_t lgraph[2] = {nullptr, nullptr};
+    int lgraph_kernels[2] = {0, 0};
+    long long* d_lcount = nullptr;  // accepted, rejected large steps (device decision)
+    float* d_llast = nullptr;       // the last decision's three means and its statistic
+    long long lcount_host[2] = {0, 0};  // d_lcount as last read
+    int lbody_kernels = 0;              // kernels of one fallback body
     double last_stats[3] = {0.0, 0.0, 0.0};  // the three means of the last checked large step
 
     // Launch shapes of the substep (mpm_autotune / mpm_set_tuning).
@@ -197,6 +207,18 @@ void free_dev(T*& p) {
     p = nullptr;
 }
 
+// The learned-step graphs depend on the corrector, the rule, the threshold,
+// the launch shapes and the buffers: rebuilt when any of them changes.
+void destroy_learned_graphs(mpm_engine* e) {
+    for (int k = 0; k < 2; ++k) {
+        if (e->lgraph[k]) cudaGraphExecDestroy(e->lgraph[k]);
+        if (e->lgraph_src[k]) cudaGraphDestroy(e->lgraph_src[k]);
+        e->lgraph[k] = nullptr;
+        e->lgraph_src[k] = nullptr;
+        e->lgraph_kernels[k] = 0;
+    }
+}
+
 // Buffers of the learned large step, sized by the particle count; allocated
 // when first needed after an init.
 void free_learned_buffers(mpm_engine* e) {
@@ -206,6 +228,7 @@ void free_learned_buffers(mpm_engine* e) {
 }
 
 void free_particles(mpm_engine* e) {
+    destroy_learned_graphs(e);
     for (int k = 0; k < 2; ++k) {
         free_dev(e->P[k]);
         free_dev(e->sigma[k]);
@@ -251,6 +274,7 @@ mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_by
         // positions read-back on the copy stream included) ends first.
         CK(e, cudaStreamSynchronize(e->stream));
         CK(e, cudaStreamSynchronize(e->copy_stream));
+        destroy_learned_graphs(e);
         for (int k = 0; k < 2; ++k) {
             if (e->graph[k]) cudaGraphExecDestroy(e->graph[k]);
             if (e->graph_src[k]) cudaGraphDestroy(e->graph_src[k]);
@@ -366,6 +390,7 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
 }
 
 mpm_status capture_graphs(mpm_engine* e) {
+    destroy_learned_graphs(e);  // they embed the launch shapes too
     const bool timed = e->timing_cap > 0;
     for (int par = 0; par < 2; ++par) {
         if (e->graph[par]) cudaGraphExecDestroy(e->graph[par]);
@@ -785,6 +810,112 @@ mpm_status plain_substeps(mpm_engine* e, int count) {
     return MPM_OK;
 }
 
+// The fallback of a rejected large step from parity `par`, enqueued on the
+// engine's stream (captured into the conditional body of the learned-step
+// graph): the counter sets emptied and the start state, still intact in
+// P[par], filed into set par (rebin); RATIO plain substeps; then, when RATIO
+// is even, the result moved to parity 1 - par, where an accepted large step
+// leaves its own: the state, its slot-to-particle map, and the counter set
+// the last substep filled (its slot order and cells stay valid, so the next
+// substep orders by it and clears the other set as usual).
+int enqueue_fallback(mpm_engine* e, int par) {
+    cudaStream_t st = e->stream;
+    int launches = 0;
+    launches += mpm::launch_fill(static_cast<float*>(e->bins_mem), (long long)(bins_bytes(e) / sizeof(float)), 0.0f, st);
+    launches += mpm::launch_fill(reinterpret_cast<float*>(e->ctl), 2 * e->scenes + 4, 0.0f, st);
+    launches += mpm::launch_bin_count(e->table, e->n, e->P[par], e->pcell, e->prank, e->bins[par], st);
+    int q = par;
+    for (int r = 0; r < e->ratio; ++r) {
+        launches += enqueue_substep(e, q, MPM_STAGE_SORT, MPM_STAGE_G2P);
+        q ^= 1;
+    }
+    if (q != 1 - par) {
+        uint32_t* sets = static_cast<uint32_t*>(e->bins_mem);
+        launches += mpm::launch_copy_words(e->P[1 - par], e->P[q], e->n * mpm::kAFloats, st);
+        launches += mpm::launch_copy_words(e->sigma[1 - par], e->sigma[q], e->n, st);
+        launches += mpm::launch_copy_words(sets + (size_t)(1 - par) * bins_set_words(e), sets + (size_t)q * bins_set_words(e),
+                                           (long long)bins_set_words(e), st);
+        launches += mpm::launch_copy_words(e->ctl + (1 - par) * e->scenes, e->ctl + q * e->scenes, e->scenes, st);
+    }
+    return launches;
+}
+
+// Captures the checked learned step as one graph per parity: the statistic
+// sums cleared, the large step (ordering, P2G, grid update, learned G2P),
+// the decision kernel, and a conditional node whose body is the fallback,
+// run only when the decision kernel sets its condition.  The step then costs
+// no host round trip, and the state ends at parity 1 - par either way.
+mpm_status capture_learned_graphs(mpm_engine* e) {
+    destroy_learned_graphs(e);
+    if (!e->d_lcount) {
+        CK(e, cudaMalloc(&e->d_lcount, 2 * sizeof(long long)));
+        CK(e, cudaMalloc(&e->d_llast, 4 * sizeof(float)));
+        CK(e, cudaMemsetAsync(e->d_lcount, 0, 2 * sizeof(long long), e->stream));
+        CK(e, cudaMemsetAsync(e->d_llast, 0, 4 * sizeof(float), e->stream));
+        CK(e, cudaStreamSynchronize(e->stream));
+        e->lcount_host[0] = e->lcount_host[1] = 0;
+    }
+    cudaStream_t st = e->stream;
+    const bool tc = e->corrector_kernel == MPM_CORRECTOR_TCGEN05;
+    for (int par = 0; par < 2; ++par) {
+        mpm::LearnArgs la{e->mlp, nullptr, nullptr, e->d_stat, large_blend(e), tc ? e->mlp_tc : nullptr, e->d_flags + 1,
+                          (e->wait_test & (MPM_WAIT_TEST_MMA_GIVE_UP | MPM_WAIT_TEST_MMA_EXPIRE)) >> 2};
+        CK(e, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int launches = mpm::launch_fill(e->d_stat, 3, 0.0f, st);
+        launches += enqueue_large(e, par, &la);
+        cudaError_t err = cudaGetLastError();
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        cudaGraphConditionalHandle handle = 0;
+        cudaGraphNode_t cnode = nullptr;
+        cudaGraph_t body = nullptr;
+        if (err == cudaSuccess) err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd);
+        if (err == cudaSuccess) err = cudaGraphConditionalHandleCreate(&handle, cg, 0, cudaGraphCondAssignDefault);
+        if (err == cudaSuccess) {
+            launches += mpm::launch_learned_decide(e->d_stat, e->n, e->fallback_rule, e->max_density_change, handle,
+                                                   e->d_lcount, e->d_llast, st);
+            err = cudaGetLastError();
+        }
+        if (err == cudaSuccess) err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd);
+        if (err == cudaSuccess) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeIf;
+            cp.conditional.size = 1;
+            err = cudaGraphAddNode(&cnode, cg, deps, nd, &cp);
+            if (err == cudaSuccess) body = cp.conditional.phGraph_out[0];
+        }
+        if (err == cudaSuccess) err = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
+        cudaGraph_t g = nullptr;
+        const cudaError_t end_err = cudaStreamEndCapture(st, &g);
+        if (err == cudaSuccess) err = end_err;
+        if (err != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return cuda_fail(e, err, "learned-step graph capture");
+        }
+        e->lgraph_src[par] = g;
+        // The fallback body, captured into the conditional node's graph.
+        CK(e, cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        const int body_launches = enqueue_fallback(e, par);
+        err = cudaGetLastError();
+        cudaGraph_t b2 = nullptr;
+        const cudaError_t bend = cudaStreamEndCapture(st, &b2);
+        if (err == cudaSuccess) err = bend;
+        if (err != cudaSuccess) {
+            cudaGetLastError();
+            return cuda_fail(e, err, "learned-step fallback capture");
+        }
+        CK(e, cudaGraphInstantiate(&e->lgraph[par], g, 0));
+        e->lgraph_kernels[par] = launches;
+        e->lbody_kernels = body_launches;
+    }
+    return MPM_OK;
+}
+
 mpm_status learned_ready(mpm_engine* e) {
     if (!e->initialized) return record(e, MPM_ERR_NOT_INITIALIZED, "mpm_init_particles has not been called");
     if (e->scenes != 1) return record(e, MPM_ERR_UNSUPPORTED, "the learned large step serves engines of one scene");
@@ -852,6 +983,8 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->mlp_tc);
     free_dev(e->d_params);
     free_dev(e->d_stat);
+    free_dev(e->d_lcount);
+    free_dev(e->d_llast);
     if (e->copy_stream) cudaStreamSynchronize(e->copy_stream);
     for (int k = 0; k < 2; ++k) {
         if (e->pos_ready[k]) cudaEventDestroy(e->pos_ready[k]);
@@ -945,6 +1078,7 @@ extern "C" mpm_status mpm_set_wait_test(mpm_engine* e, uint32_t flags) {
                             MPM_WAIT_TEST_MMA_EXPIRE))
         return record(e, MPM_ERR_INVALID_ARGUMENT, "unknown wait-test flag");
     e->wait_test = flags;
+    destroy_learned_graphs(e);
     return MPM_OK;
 }
 
@@ -1264,6 +1398,7 @@ extern "C" mpm_status mpm_set_corrector(mpm_engine* e, const float* params_host,
     e->mlp_set = params_host != nullptr;
     e->ratio = ratio;
     e->max_density_change = max_density_change;
+    destroy_learned_graphs(e);
     return MPM_OK;
 }
 
@@ -1272,6 +1407,35 @@ extern "C" mpm_status mpm_step_learned(mpm_engine* e, int32_t nlarge, mpm_learne
     if (s != MPM_OK) return s;
     if (nlarge < 0) return record(e, MPM_ERR_INVALID_ARGUMENT, "nlarge < 0");
     if ((s = learned_ready(e)) != MPM_OK) return s;
+    const int32_t requested = nlarge;
+    const bool checked_on_device = e->mlp_set && e->max_density_change >= 0.f && e->fallback_on_device;
+    if (checked_on_device && nlarge > 0) {
+        if (!e->lgraph[0] && (s = capture_learned_graphs(e)) != MPM_OK) return s;
+        for (int k = 0; k < nlarge; ++k) {
+            CK(e, cudaGraphLaunch(e->lgraph[e->parity], e->stream));
+            e->kernel_launches += e->lgraph_kernels[e->parity];
+            e->parity ^= 1;
+        }
+        // One read-back per call: the decisions' counters and the last means.
+        long long cnt[2] = {0, 0};
+        float last[4] = {0.f, 0.f, 0.f, 0.f};
+        CK(e, cudaMemcpyAsync(cnt, e->d_lcount, sizeof(cnt), cudaMemcpyDeviceToHost, e->stream));
+        CK(e, cudaMemcpyAsync(last, e->d_llast, sizeof(last), cudaMemcpyDeviceToHost, e->stream));
+        CK(e, cudaStreamSynchronize(e->stream));
+        const long long acc = cnt[0] - e->lcount_host[0], rej = cnt[1] - e->lcount_host[1];
+        e->lcount_host[0] = cnt[0];
+        e->lcount_host[1] = cnt[1];
+        e->large_steps += acc;
+        e->fallbacks += rej;
+        e->substeps += rej * e->ratio;
+        e->kernel_launches += rej * e->lbody_kernels;
+        for (int q = 0; q < 3; ++q) e->last_stats[q] = last[q];
+        e->last_density_change = last[3];
+        // The state a fallback's last substep started from is overwritten by
+        // the move to parity 1 - par: mpm_get_sort reports the current state.
+        e->sort_src = kNoSort;
+        nlarge = 0;  // done; the host-decided loop below runs no step
+    }
     for (int k = 0; k < nlarge; ++k) {
         const int par = e->parity;
         const bool tc = e->mlp_set && e->corrector_kernel == MPM_CORRECTOR_TCGEN05;
@@ -1307,7 +1471,7 @@ extern "C" mpm_status mpm_step_learned(mpm_engine* e, int32_t nlarge, mpm_learne
             ++e->fallbacks;
         }
     }
-    if (nlarge > 0) e->grid_view = GridView::kVelocity;
+    if (requested > 0) e->grid_view = GridView::kVelocity;
     if ((s = export_positions(e)) != MPM_OK) return s;
     if (stats) {
         stats->large_steps = e->large_steps;
@@ -1683,6 +1847,14 @@ extern "C" mpm_status mpm_set_fallback_rule(mpm_engine* e, int32_t rule) {
         rule != MPM_FALLBACK_REST_DENSITY_EXCESS)
         return record(e, MPM_ERR_INVALID_ARGUMENT, "unknown fallback rule");
     e->fallback_rule = rule;
+    destroy_learned_graphs(e);
+    return MPM_OK;
+}
+
+extern "C" mpm_status mpm_set_fallback_on_device(mpm_engine* e, int32_t on_device) {
+    mpm_status s = enter(e);
+    if (s != MPM_OK) return s;
+    e->fallback_on_device = on_device != 0;
     return MPM_OK;
 }
 
@@ -1700,5 +1872,6 @@ extern "C" mpm_status mpm_set_corrector_kernel(mpm_engine* e, int32_t kind) {
     if (kind != MPM_CORRECTOR_TCGEN05 && kind != MPM_CORRECTOR_MMA_SYNC)
         return record(e, MPM_ERR_INVALID_ARGUMENT, "unknown corrector kernel");
     e->corrector_kernel = kind;
+    destroy_learned_graphs(e);
     return MPM_OK;
 }

@@ -150,6 +150,13 @@ void sdf_prepare_host(const float* tris, int t, float* aux);
 int launch_sdf_build(const SimParams& p, const float* tris, const float* aux, int t, float* sdf, uint32_t* status,
                      cudaStream_t st, uint32_t wait_test = 0u);
 int launch_fill(float* dst, long long count, float value, cudaStream_t st);
+// The learned step's fallback decision (one thread): rule 0 / 1 / 2 =
+// MPM_FALLBACK_DENSITY_CHANGE / REST_DENSITY / REST_DENSITY_EXCESS on the
+// means of stat[0..2] over n particles; sets `fallback` to 1 to reject.
+int launch_learned_decide(const float* stat, long long n, int rule, float threshold,
+                          cudaGraphConditionalHandle fallback, long long* counters, float* last, cudaStream_t st);
+// count 32-bit words from src to dst (device memory, not overlapping).
+int launch_copy_words(void* dst, const void* src, long long count, cudaStream_t st);
 // dst[i] = i for i < n.
 int launch_identity(int32_t* dst, int n, cudaStream_t st);
 

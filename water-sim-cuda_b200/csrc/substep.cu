@@ -18,6 +18,7 @@
 //  - sdf: one float per node.
 #include <algorithm>
 #include <climits>
+#include <cstdint>
 
 #include "kernels.h"
 
@@ -1307,6 +1308,42 @@ __global__ void __launch_bounds__(256) fill_kernel(float* __restrict__ dst, long
         dst[i] = value;
 }
 
+// The learned step's accept / reject decision on the device: the mean of the
+// statistic the rule names (la.stat sums, kernels above) against the
+// threshold; reject (NaN included) sets the graph's conditional, which runs
+// the fallback body.  counters[0] / [1] count accepted and rejected steps;
+// last[0..2] receive the three means, last[3] the compared statistic.
+__global__ void learned_decide_kernel(const float* __restrict__ stat, long long n, int rule, float threshold,
+                                      cudaGraphConditionalHandle fallback, long long* __restrict__ counters,
+                                      float* __restrict__ last) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const float inv = n > 0 ? 1.0f / (float)n : 0.0f;
+    const float m0 = stat[0] * inv, m1 = stat[1] * inv, m2 = stat[2] * inv;
+    const float st = rule == 1 ? m1 : (rule == 2 ? m1 - m2 : m0);
+    const bool reject = !(st <= threshold);
+    cudaGraphSetConditional(fallback, reject ? 1u : 0u);
+    counters[reject ? 1 : 0] += 1;
+    last[0] = m0;
+    last[1] = m1;
+    last[2] = m2;
+    last[3] = st;
+}
+
+// dst[i] = src[i] for i < count 32-bit words (16-byte vectors when both
+// pointers and the count allow).
+__global__ void __launch_bounds__(256) copy_words_kernel(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
+                                                         long long count, bool vec) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (vec) {
+        uint4* d = reinterpret_cast<uint4*>(dst);
+        const uint4* q = reinterpret_cast<const uint4*>(src);
+        for (long long i = i0; i < count / 4; i += stride) d[i] = __ldg(q + i);
+    } else {
+        for (long long i = i0; i < count; i += stride) dst[i] = __ldg(src + i);
+    }
+}
+
 inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
@@ -1446,6 +1483,23 @@ int launch_grid_export(const SimParams& p, const float4* grid, float* planes4, c
 int launch_identity(int32_t* dst, int n, cudaStream_t st) {
     if (n <= 0) return 0;
     identity_kernel<<<blocks_for(n, 256), 256, 0, st>>>(dst, n);
+    return 1;
+}
+
+int launch_learned_decide(const float* stat, long long n, int rule, float threshold,
+                          cudaGraphConditionalHandle fallback, long long* counters, float* last, cudaStream_t st) {
+    learned_decide_kernel<<<1, 32, 0, st>>>(stat, n, rule, threshold, fallback, counters, last);
+    return 1;
+}
+
+int launch_copy_words(void* dst, const void* src, long long count, cudaStream_t st) {
+    if (count <= 0) return 0;
+    const bool vec = count % 4 == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0 &&
+                     (reinterpret_cast<uintptr_t>(src) & 15) == 0;
+    const long long units = vec ? count / 4 : count;
+    const int blocks = (int)std::min<long long>((units + 255) / 256, 148LL * 16);
+    copy_words_kernel<<<blocks, 256, 0, st>>>(static_cast<uint32_t*>(dst), static_cast<const uint32_t*>(src), count,
+                                               vec);
     return 1;
 }
 

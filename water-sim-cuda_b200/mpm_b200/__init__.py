@@ -219,6 +219,7 @@ def _load() -> ctypes.CDLL:
         "mpm_step_learned": (I32, [P, I32, P]),
         "mpm_set_corrector_kernel": (I32, [P, I32]),
         "mpm_set_fallback_rule": (I32, [P, I32]),
+        "mpm_set_fallback_on_device": (I32, [P, I32]),
         "mpm_learned_statistics": (I32, [P, P]),
         "mpm_corrector_create": (I32, [I32, I64, P]),
         "mpm_corrector_destroy": (None, [P]),
@@ -473,6 +474,11 @@ class Engine:
         """The fallback statistic: "density_change" (default), "rest_density" or
         "rest_density_excess" (mpm_set_fallback_rule)."""
         self._check(lib.mpm_set_fallback_rule(self._h, FALLBACK_RULES[rule]))
+
+    def set_fallback_on_device(self, on_device: bool = True):
+        """Decide a checked large step's fallback on the device (a conditional
+        graph node, the default) or on the host (a read-back per step)."""
+        self._check(lib.mpm_set_fallback_on_device(self._h, 1 if on_device else 0))
 
     def learned_statistics(self) -> dict:
         """The three fallback means of the last checked large step."""
