@@ -152,14 +152,18 @@ def _timed(fn):
 
 
 def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_density_change: float = 0.02,
-             checkpoints=(10, 25, 50, 100), perturb: float = 1e-4, rule: str = "density_change") -> dict:
+             checkpoints=(10, 25, 50, 100), perturb: float = 1e-4, rule: str = "density_change",
+             on_device: bool = True, per_step_stats: bool = False) -> dict:
     """Plain (ratio * nlarge substeps) vs learned (nlarge large steps) vs the
     uncorrected large step, from the same state; metrics at each checkpoint
     (in large steps) and at the end.  "perturbed" is the plain run from
     positions moved by N(0, perturb) cells: its distance from the plain run
     is the chaos floor of the scene, what no large step can undercut.
-    rule: the fallback statistic (Engine.set_fallback_rule); the learned run
-    also reports the mean of each statistic over its checked large steps."""
+    rule: the fallback statistic (Engine.set_fallback_rule); on_device: the
+    fallback decided on the device (Engine.set_fallback_on_device); the learned
+    run also reports the mean of each statistic, over every checked large step
+    with per_step_stats (one call per step), else over the last step before
+    each checkpoint."""
     marks = sorted(set([c for c in checkpoints if c <= nlarge] + [nlarge]))
     res = {"ratio": ratio, "large_steps": nlarge, "max_density_change": max_density_change, "rule": rule}
     runs = {}
@@ -172,6 +176,7 @@ def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_densi
             if tag == "learned":
                 e.set_corrector(params, ratio=ratio, max_density_change=max_density_change)
                 e.set_fallback_rule(rule)
+                e.set_fallback_on_device(on_device)
             elif tag == "uncorrected":
                 e.set_corrector(None, ratio=ratio)
             pos, total, prev, stats = {}, 0.0, 0, {}
@@ -180,9 +185,8 @@ def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_densi
                 k = m - prev
                 if tag in ("plain", "perturbed"):
                     _, dt = _timed(lambda: e.step(k * ratio))
-                elif tag == "learned" and max_density_change >= 0:
-                    # One call per large step, to record each step's statistics
-                    # (the step is synchronous when checked either way).
+                elif tag == "learned" and max_density_change >= 0 and per_step_stats:
+                    # One call per large step, to record each step's statistics.
                     dt = 0.0
                     for _ in range(k):
                         stats, d = _timed(lambda: e.step_learned(1))
@@ -191,6 +195,9 @@ def evaluate(cfg, st, tris, params, nlarge: int = 100, ratio: int = 4, max_densi
                             seen[key].append(v)
                 else:
                     stats, dt = _timed(lambda: e.step_learned(k))
+                    if tag == "learned" and max_density_change >= 0:
+                        for key, v in e.learned_statistics().items():
+                            seen[key].append(v)
                 total += dt
                 prev = m
                 pos[m] = e.get_positions().copy()
@@ -247,6 +254,8 @@ def main(argv=None):
     ev.add_argument("--alpha", type=float, default=1.0, help="scale of the applied correction")
     ev.add_argument("--rule", choices=["density_change", "rest_density", "rest_density_excess"],
                     default="density_change", help="the fallback statistic")
+    ev.add_argument("--host-decision", action="store_true", help="decide the fallback on the host")
+    ev.add_argument("--per-step-stats", action="store_true", help="record every large step's statistics")
     pr = sub.add_parser("probe", help="a few learned large steps on a thinned dam break (a small case to profile)")
     pr.add_argument("--params", default=PHYSICAL_PARAMS)
     pr.add_argument("--thin", type=int, default=5, help="keep every THIN-th particle")
@@ -318,7 +327,8 @@ def main(argv=None):
         if a.physical:
             cfg = physical_config(cfg)
         res = evaluate(cfg, st, tris, params, nlarge=a.large_steps, ratio=int(meta.get("ratio", 4)),
-                       max_density_change=a.threshold, rule=a.rule)
+                       max_density_change=a.threshold, rule=a.rule, on_device=not a.host_decision,
+                       per_step_stats=a.per_step_stats)
         res["alpha"] = a.alpha
         print(json.dumps(res))
 
