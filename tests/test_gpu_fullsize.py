@@ -135,11 +135,15 @@ def _check_reference_bounded(cfg, start, got, grid, r_state, r_grid, want, wgrid
     ok = np.isfinite(start).all(0) & ~bad_want & ~bad_got & ~bad_ref
     e_got = _field_errors(got[:, ok], want[:, ok])
     e_ref = _field_errors(r_state[:, ok], want[:, ok])
+    # The grid's velocity is momentum over mass: at nodes that particles barely
+    # reach (mass just above the 1e-9 cut) it takes any value the order of the
+    # float sums gives, so the grid is compared as mass and momentum.
     nodes = np.isfinite(wgrid).all(0) & np.isfinite(grid).all(0) & np.isfinite(r_grid).all(0)
+    mom = lambda g: g[0:1, nodes].astype(np.float64) * g[1:4, nodes]
     g_got = {"mass": float(np.max(np.abs(grid[0, nodes] - wgrid[0, nodes]))),
-             "velocity": float(np.max(np.abs(grid[1:4, nodes] - wgrid[1:4, nodes])))}
+             "momentum": float(np.max(np.abs(mom(grid) - mom(wgrid))))}
     g_ref = {"mass": float(np.max(np.abs(r_grid[0, nodes] - wgrid[0, nodes]))),
-             "velocity": float(np.max(np.abs(r_grid[1:4, nodes] - wgrid[1:4, nodes])))}
+             "momentum": float(np.max(np.abs(mom(r_grid) - mom(wgrid))))}
     print(f"non-finite particles differing from FP64: engine {d_got}, reference {d_ref} "
           f"(of {int(bad_want.sum())} in FP64); particle errors vs FP64: engine {e_got}, reference {e_ref}; "
           f"grid errors: engine {g_got}, reference {g_ref}")
@@ -149,8 +153,8 @@ def _check_reference_bounded(cfg, start, got, grid, r_state, r_grid, want, wgrid
     for name in e_got:
         assert e_got[name] <= max(2.0 * e_ref[name], 1e-5 * scales[name]), \
             f"{name}: engine error {e_got[name]:.3e}, reference {e_ref[name]:.3e}"
-    for name, sl in (("mass", 0), ("velocity", slice(1, 4))):
-        scale = float(np.max(np.abs(wgrid[sl, nodes])))
+    for name in ("mass", "momentum"):
+        scale = float(np.max(np.abs(wgrid[0, nodes] if name == "mass" else mom(wgrid))))
         assert g_got[name] <= max(2.0 * g_ref[name], 1e-5 * scale), \
             f"grid {name}: engine error {g_got[name]:.3e}, reference {g_ref[name]:.3e}"
 
