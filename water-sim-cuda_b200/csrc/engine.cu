@@ -85,7 +85,7 @@ struct mpm_engine {
     int4* crowd = nullptr;                   // P2G's crowded-cell list
     int crowd_cap = 0;
     int32_t* pcell = nullptr;                // global cell of each slot of P[parity]
-    int32_t* prank = nullptr;                // rank within its cell
+    int32_t* ccur = nullptr;                 // slot cursor of every cell (the ordering's scatter)
     int32_t* ref_keys = nullptr;             // mpm_get_sort: keys in original order (one scene)
     int32_t* ref_perm = nullptr;             // mpm_get_sort: stable sort permutation
     void* sort_mem = nullptr;
@@ -242,7 +242,6 @@ void free_particles(mpm_engine* e) {
     free_dev(e->gidx);
     free_dev(e->crowd);
     free_dev(e->pcell);
-    free_dev(e->prank);
     free_dev(e->ref_keys);
     free_dev(e->ref_perm);
     free_dev(e->sort_mem);
@@ -305,7 +304,6 @@ mpm_status alloc_particles(mpm_engine* e, long long n, int max_n, size_t sort_by
     e->crowd_cap = (int)std::min<long long>(cap / 4 + 64, 0x7fffffffLL);
     CK(e, cudaMalloc(&e->crowd, (size_t)e->crowd_cap * sizeof(int4)));
     CK(e, cudaMalloc(&e->pcell, ibytes));
-    CK(e, cudaMalloc(&e->prank, ibytes));
     const size_t sbytes = (size_t)std::max(max_n, 1) * sizeof(int32_t);
     CK(e, cudaMalloc(&e->ref_keys, sbytes));
     CK(e, cudaMalloc(&e->ref_perm, sbytes));
@@ -370,7 +368,7 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
     mark(0);
     if (from <= MPM_STAGE_SORT && upto >= MPM_STAGE_SORT)
         launches += mpm::launch_bin_order(sc, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart, e->cstart,
-                                          e->pcell, e->prank, e->gidx, e->corder, e->d_itemoff, e->d_clroff, work, e->bpart,
+                                          e->pcell, e->ccur, e->gidx, e->corder, e->d_itemoff, e->d_clroff, work, e->bpart,
                                           e->scan_chunks, st);
     mark(1);
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
@@ -384,7 +382,7 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
     mark(3);
     if (from <= MPM_STAGE_G2P && upto >= MPM_STAGE_G2P)
         launches += mpm::launch_g2p(sc, e->prm[0], e->n, e->P[par], e->P[1 - par], e->gidx, e->sigma[par],
-                                    e->sigma[1 - par], e->vgrid, e->sdf, e->pcell, e->prank, e->bins[1 - par],
+                                    e->sigma[1 - par], e->vgrid, e->sdf, e->pcell, e->bins[1 - par],
                                     e->d_flags, st, nullptr, e->tune.g2p_block);
     mark(4);
     return launches;
@@ -511,7 +509,7 @@ mpm_status load_states(mpm_engine* e, const float* const* soa26_host, bool init_
     // Both counter sets empty, then the imported particles filed into set 0.
     CK(e, cudaMemsetAsync(e->bins_mem, 0, bins_bytes(e), e->stream));
     CK(e, cudaMemsetAsync(e->ctl, 0, (2 * e->scenes + 4) * sizeof(uint32_t), e->stream));
-    e->kernel_launches += mpm::launch_bin_count(e->table, e->n, e->P[0], e->pcell, e->prank, e->bins[0], e->stream);
+    e->kernel_launches += mpm::launch_bin_count(e->table, e->n, e->P[0], e->pcell, e->bins[0], e->stream);
     CK(e, cudaGetLastError());
     e->parity = 0;
     e->sort_src = kNoSort;
@@ -718,6 +716,7 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
         (err = cudaMalloc(&e->bstart, (size_t)bins_total * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->bpart, (size_t)count * e->scan_chunks * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->cstart, (size_t)cells_total * sizeof(int32_t))) != cudaSuccess ||
+        (err = cudaMalloc(&e->ccur, (size_t)cells_total * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->corder, (size_t)cells_total)) != cudaSuccess ||
         (err = cudaMalloc(&e->d_prm, count * sizeof(SimParams))) != cudaSuccess ||
         (err = cudaMalloc(&e->d_poff, (count + 1) * sizeof(long long))) != cudaSuccess ||
@@ -815,7 +814,7 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
     const SimParams big = large_params(e, 0);
     int launches = 0;
     launches += mpm::launch_bin_order(e->table, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart,
-                                      e->cstart, e->pcell, e->prank, e->gidx, e->corder, e->d_itemoff, e->d_clroff, work, e->bpart,
+                                      e->cstart, e->pcell, e->ccur, e->gidx, e->corder, e->d_itemoff, e->d_clroff, work, e->bpart,
                                           e->scan_chunks, st);
     launches += mpm::launch_p2g(e->table_large, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par],
                                 e->corder, e->d_itemoff, work, e->accum, e->crowd, e->crowd_cap, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
@@ -823,7 +822,7 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
     launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, st,
                                         e->tune.grid_block);
     launches += mpm::launch_g2p(e->table_large, big, e->n, e->P[par], e->P[1 - par], e->gidx, e->sigma[par],
-                                e->sigma[1 - par], e->vgrid, e->sdf, e->pcell, e->prank, e->bins[1 - par], e->d_flags,
+                                e->sigma[1 - par], e->vgrid, e->sdf, e->pcell, e->bins[1 - par], e->d_flags,
                                 st, learn);
     return launches;
 }
@@ -833,7 +832,7 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
 mpm_status rebin(mpm_engine* e, int par) {
     CK(e, cudaMemsetAsync(e->bins_mem, 0, bins_bytes(e), e->stream));
     CK(e, cudaMemsetAsync(e->ctl, 0, (2 * e->scenes + 4) * sizeof(uint32_t), e->stream));
-    e->kernel_launches += mpm::launch_bin_count(e->table, e->n, e->P[par], e->pcell, e->prank, e->bins[par], e->stream);
+    e->kernel_launches += mpm::launch_bin_count(e->table, e->n, e->P[par], e->pcell, e->bins[par], e->stream);
     CK(e, cudaGetLastError());
     e->parity = par;
     return MPM_OK;
@@ -864,7 +863,7 @@ int enqueue_fallback(mpm_engine* e, int par) {
     int launches = 0;
     launches += mpm::launch_fill(static_cast<float*>(e->bins_mem), (long long)(bins_bytes(e) / sizeof(float)), 0.0f, st);
     launches += mpm::launch_fill(reinterpret_cast<float*>(e->ctl), 2 * e->scenes + 4, 0.0f, st);
-    launches += mpm::launch_bin_count(e->table, e->n, e->P[par], e->pcell, e->prank, e->bins[par], st);
+    launches += mpm::launch_bin_count(e->table, e->n, e->P[par], e->pcell, e->bins[par], st);
     int q = par;
     for (int r = 0; r < e->ratio; ++r) {
         launches += enqueue_substep(e, q, MPM_STAGE_SORT, MPM_STAGE_G2P);
@@ -1012,6 +1011,7 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->sdf);
     free_dev(e->bins_mem);
     free_dev(e->bstart);
+    free_dev(e->ccur);
     free_dev(e->bpart);
     free_dev(e->corder);
     free_dev(e->cstart);

@@ -50,8 +50,8 @@ int launch_radix_sort(const int32_t* keys, int n, const SortScratch& s, int32_t*
 // The substep kernels work on all scenes of a SceneTable at once; particle
 // slots, cells and bins are global (device_math.cuh).  P is the
 // particle-major state, ordered by cell of the binning that produced it.
-// pcell[j]/prank[j] are the global cell of slot j and its rank among the
-// cell's particles.  A counter set holds the cell counts (global cells), the
+// pcell[j] is the global cell of slot j; ccur holds one slot cursor per
+// cell, which the ordering's scatter draws the cell's slots from.  A counter set holds the cell counts (global cells), the
 // bin counts and the per-scene lists of bins that hold particles (global bin
 // entries: nb + 2 per scene), and the per-scene list lengths nlist[scene].
 // Two sets alternate: a substep orders the particles by one and its G2P
@@ -64,8 +64,8 @@ struct BinSet {
 };
 
 // Files the n particles of P (all scenes, slot order) into an empty set.
-int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t* pcell, int32_t* prank,
-                     const BinSet& set, cudaStream_t st);
+int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t* pcell, const BinSet& set,
+                     cudaStream_t st);
 // Order by cell from set `cur`: bstart (global first slots of every bin), cstart
 // (first slot of every cell of a listed bin), corder (P2G's order of each
 // listed bin's cells, one byte per cell, indexed like the cells), gidx[new
@@ -75,7 +75,7 @@ int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t*
 // bins_total: sum over scenes of nb + 1.  bpart: scenes x scan_chunks ints of
 // scratch; scan_chunks = bin_scan_chunks(largest nb + 1).
 int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
-                     int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
+                     int32_t* bstart, int32_t* cstart, const int32_t* pcell, int32_t* ccur, int32_t* gidx,
                      uint8_t* corder, long long* itemoff, long long* clroff, uint32_t* work, int32_t* bpart,
                      int scan_chunks, cudaStream_t st);
 // Chunks of the bin scan for a scene of `bins` scanned bins.
@@ -117,7 +117,7 @@ struct LearnArgs {
 // step of one scene (LearnArgs), else null.
 int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const float* Pin, float* Pout,
                const int32_t* gidx, const int32_t* sig_in, int32_t* sig_out, const float4* vgrid, const float* sdf,
-               int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st,
+               int32_t* pcell, const BinSet& next, uint32_t* health, cudaStream_t st,
                const LearnArgs* learn = nullptr, int block = 256);
 
 // The kernels below take one scene's SimParams and pointers already offset to

@@ -56,24 +56,22 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // Files this lane's particle under global cell `gcell` (global bin `gbin`,
 // bin `bin` of scene `scene`, whose bin entries start at `boff`) of a counter
-// set and returns its rank among the cell's particles: one atomic per
-// distinct cell and per distinct bin of the warp; the first particle of a
-// bin appends the bin to its scene's list.  Every lane of the warp must call
-// it; lanes with gcell < 0 take part without counting.
-__device__ __forceinline__ int file_particle(int gcell, int gbin, int bin, int scene, long long boff,
-                                             const BinSet& set) {
+// set: one reduction per distinct cell of the warp (no value comes back, so
+// no lane waits on it) and one atomic per distinct bin, whose leader appends
+// the bin to its scene's list when it is the bin's first particle.  The
+// particle's place within its cell is drawn later, by the ordering's scatter.
+// Every lane of the warp must call it; lanes with gcell < 0 take part without
+// counting.
+__device__ __forceinline__ void file_particle(int gcell, int gbin, int bin, int scene, long long boff,
+                                              const BinSet& set) {
     const int lane = threadIdx.x & 31;
     const uint32_t peers = __match_any_sync(0xffffffffu, gcell);
-    const int leader = __ffs(peers) - 1;
-    uint32_t base = 0;
-    if (gcell >= 0 && lane == leader) base = atomicAdd(set.ccount + gcell, (uint32_t)__popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader);
+    if (gcell >= 0 && lane == __ffs(peers) - 1) atomicAdd(set.ccount + gcell, (uint32_t)__popc(peers));
     const uint32_t bpeers = __match_any_sync(0xffffffffu, gbin);
     if (gbin >= 0 && lane == __ffs(bpeers) - 1) {
         if (atomicAdd(set.bcount + gbin, (uint32_t)__popc(bpeers)) == 0u)
             set.blist[boff + atomicAdd(set.nlist + scene, 1u)] = bin;
     }
-    return (int)base + __popc(peers & lanemask_lt());
 }
 
 // Scene lookup for the per-particle and per-node kernels.  With one scene
@@ -537,8 +535,7 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_crowd_kernel(SceneTabl
 // -------------------------------------------------------------- binning ----
 // Files the particles of an imported state (slot order) into a counter set.
 __global__ void __launch_bounds__(256) bin_count_kernel(SceneTable sc, long long n, const float* __restrict__ P,
-                                                        int32_t* __restrict__ pcell, int32_t* __restrict__ prank,
-                                                        BinSet set) {
+                                                        int32_t* __restrict__ pcell, BinSet set) {
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const bool valid = j < n;
     int gcell = -1, gbin = -1, bin = -1, scene = 0;
@@ -552,11 +549,8 @@ __global__ void __launch_bounds__(256) bin_count_kernel(SceneTable sc, long long
         gbin = (int)p.boff + bin;
         boff = p.boff;
     }
-    const int r = file_particle(gcell, gbin, bin, scene, boff, set);
-    if (valid) {
-        pcell[j] = gcell;
-        prank[j] = r;
-    }
+    file_particle(gcell, gbin, bin, scene, boff, set);
+    if (valid) pcell[j] = gcell;
 }
 
 // Bin starts in two launches over (scene, chunk of kScanChunk bins) CTAs, no
@@ -742,11 +736,13 @@ __device__ __forceinline__ void cell_order(uint4 c, uint8_t* __restrict__ order)
 }
 
 // One warp per listed bin of each scene: cstart of its 128 cells = bstart of
-// the bin + the exclusive scan of their counts.  Then clears the cell
+// the bin + the exclusive scan of their counts (also written to ccur, the
+// cursors the scatter draws slots from).  Then clears the cell
 // counters of the other set for the bins on that set's lists (the cells it
 // last filled).
 __global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet set, const int32_t* __restrict__ bstart,
-                                                        int32_t* __restrict__ cstart, uint8_t* __restrict__ corder,
+                                                        int32_t* __restrict__ cstart, int32_t* __restrict__ ccur,
+                                                        uint8_t* __restrict__ corder,
                                                         BinSet clear, const long long* __restrict__ itemoff,
                                                         const long long* __restrict__ clroff) {
     const int lane = threadIdx.x & 31;
@@ -774,6 +770,7 @@ __global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet se
         st.z = st.y + (int)c.y;
         st.w = st.z + (int)c.z;
         *reinterpret_cast<int4*>(cstart + c0) = st;
+        *reinterpret_cast<int4*>(ccur + c0) = st;  // the scatter's cursors start at the cells' first slots
         cell_order(c, corder + (size_t)coff + (size_t)bin * kBinCells);
     }
     const long long nclear = clroff[sc.count];
@@ -786,18 +783,24 @@ __global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet se
     }
 }
 
-// gidx[cstart[cell[j]] + rank[j]] = j: the order by cell.  Thread 0 also
-// resets the other set's lists, which cell_scan_kernel has just cleared.
+// gidx[slot] = j: the order by cell, each particle taking the next slot of
+// its cell from the cursor ccur[cell] (one atomic per distinct cell of a warp;
+// the lanes sharing a cell take consecutive slots in lane order).  Thread 0
+// also resets the other set's lists, which cell_scan_kernel has just cleared.
 __global__ void __launch_bounds__(256) bin_scatter_kernel(long long n, int scenes, const int32_t* __restrict__ pcell,
-                                                          const int32_t* __restrict__ prank,
-                                                          const int32_t* __restrict__ cstart,
-                                                          int32_t* __restrict__ gidx,
+                                                          int32_t* __restrict__ ccur, int32_t* __restrict__ gidx,
                                                           uint32_t* __restrict__ clear_nlist) {
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (j == 0)
         for (int s2 = 0; s2 < scenes; ++s2) clear_nlist[s2] = 0u;
-    if (j >= n) return;
-    gidx[__ldg(cstart + __ldg(pcell + j)) + __ldg(prank + j)] = (int32_t)j;
+    const int cell = j < n ? __ldg(pcell + j) : -1;
+    const int lane = threadIdx.x & 31;
+    const uint32_t peers = __match_any_sync(0xffffffffu, cell);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (cell >= 0 && lane == leader) base = atomicAdd(ccur + cell, __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (cell >= 0) gidx[base + __popc(peers & lanemask_lt())] = (int32_t)j;
 }
 
 // ---------------------------------------------------------- grid update ----
@@ -886,7 +889,7 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
                                                   float* __restrict__ Pout, const int32_t* __restrict__ gidx,
                                                   const int32_t* __restrict__ sig_in, int32_t* __restrict__ sig_out,
                                                   const float4* __restrict__ vgrid_all, const float* __restrict__ sdf_all,
-                                                  int32_t* __restrict__ pcell, int32_t* __restrict__ prank, BinSet next,
+                                                  int32_t* __restrict__ pcell, BinSet next,
                                                   uint32_t* __restrict__ health, LearnArgs la) {
     __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
     __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
@@ -1188,7 +1191,7 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
         gcell = (int)p.coff + cell_of(p, nx, ny, nz, &bin);
         gbin = (int)p.boff + bin;
     }
-    const int rank = file_particle(gcell, gbin, bin, scene, p.boff, next);
+    file_particle(gcell, gbin, bin, scene, p.boff, next);
     if (!valid) continue;  // only the last passes of the last block have idle lanes
     float4* o = reinterpret_cast<float4*>(Pout + (size_t)j * kAFloats);
     o[0] = make_float4(nx, ny, nz, NF[0]);
@@ -1199,7 +1202,6 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
     o[5] = make_float4(tc[5], tc[6], tc[7], tc[8]);
     sig_out[j] = __ldg(sig_in + src);
     pcell[j] = gcell;
-    prank[j] = rank;
     if constexpr (kMode == kG2PCollect) {
         float* vo = la.vel + (size_t)__ldg(sig_in + src) * 3;
         vo[0] = tv[0], vo[1] = tv[1], vo[2] = tv[2];
@@ -1348,17 +1350,17 @@ inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t* pcell, int32_t* prank,
-                     const BinSet& set, cudaStream_t st) {
+int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t* pcell, const BinSet& set,
+                     cudaStream_t st) {
     if (n <= 0) return 0;
-    bin_count_kernel<<<blocks_for(n, 256), 256, 0, st>>>(sc, n, P, pcell, prank, set);
+    bin_count_kernel<<<blocks_for(n, 256), 256, 0, st>>>(sc, n, P, pcell, set);
     return 1;
 }
 
 int bin_scan_chunks(long long bins) { return (int)std::max(1LL, (bins + kScanChunk - 1) / kScanChunk); }
 
 int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
-                     int32_t* bstart, int32_t* cstart, const int32_t* pcell, const int32_t* prank, int32_t* gidx,
+                     int32_t* bstart, int32_t* cstart, const int32_t* pcell, int32_t* ccur, int32_t* gidx,
                      uint8_t* corder, long long* itemoff, long long* clroff, uint32_t* work, int32_t* bpart,
                      int scan_chunks, cudaStream_t st) {
     if (n <= 0) return 0;
@@ -1367,8 +1369,8 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
     bin_scan_kernel<<<scan_grid, kScanThreads, 0, st>>>(sc, cur.bcount, other.bcount, bpart, bstart, work, cur.nlist,
                                                        other.nlist, itemoff, clroff);
     const int ctas = (int)std::max(1LL, std::min((long long)blocks_for(bins_total * 32, 128), 148LL * 8));
-    cell_scan_kernel<<<ctas, 128, 0, st>>>(sc, cur, bstart, cstart, corder, other, itemoff, clroff);
-    bin_scatter_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, sc.count, pcell, prank, cstart, gidx, other.nlist);
+    cell_scan_kernel<<<ctas, 128, 0, st>>>(sc, cur, bstart, cstart, ccur, corder, other, itemoff, clroff);
+    bin_scatter_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, sc.count, pcell, ccur, gidx, other.nlist);
     return 4;
 }
 
@@ -1408,14 +1410,14 @@ int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_to
 
 int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const float* Pin, float* Pout,
                const int32_t* gidx, const int32_t* sig_in, int32_t* sig_out, const float4* vgrid, const float* sdf,
-               int32_t* pcell, int32_t* prank, const BinSet& next, uint32_t* health, cudaStream_t st,
+               int32_t* pcell, const BinSet& next, uint32_t* health, cudaStream_t st,
                const LearnArgs* learn, int block) {
     if (n <= 0) return 0;
     const LearnArgs la = learn ? *learn : LearnArgs{};
     const unsigned grid = blocks_for(n, 256);
     if (learn && sc.count == 1 && la.mlp_tc) {
         g2p_kernel<false, kG2PLearnedTc><<<grid, 256, sizeof(MlpTcSmem), st>>>(
-            sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, prank, next, health, la);
+            sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, next, health, la);
         return 1;
     }
     // Plain G2P: 128- or 256-thread CTAs, or 512 = the register-wide 256-thread
@@ -1424,28 +1426,28 @@ int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const flo
     const int pb = wide ? 256 : ((block == 128 || block == 256) ? block : 256);
     if (learn && sc.count == 1 && la.mlp)
         g2p_kernel<false, kG2PLearned><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
-                                                             pcell, prank, next, health, la);
+                                                             pcell, next, health, la);
     else if (learn && sc.count == 1 && la.feat)
         g2p_kernel<false, kG2PCollect><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
-                                                             pcell, prank, next, health, la);
+                                                             pcell, next, health, la);
     else if (learn && sc.count == 1)
         g2p_kernel<false, kG2PLarge><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
-                                                           pcell, prank, next, health, la);
+                                                           pcell, next, health, la);
     else if (sc.count == 1 && wide)
         g2p_kernel<false, kG2PPlain, true><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in,
-                                                                             sig_out, vgrid, sdf, pcell, prank, next,
+                                                                             sig_out, vgrid, sdf, pcell, next,
                                                                              health, la);
     else if (sc.count == 1)
         g2p_kernel<false, kG2PPlain><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out,
-                                                                       vgrid, sdf, pcell, prank, next, health, la);
+                                                                       vgrid, sdf, pcell, next, health, la);
     else if (wide)
         g2p_kernel<true, kG2PPlain, true><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in,
-                                                                            sig_out, vgrid, sdf, pcell, prank, next,
+                                                                            sig_out, vgrid, sdf, pcell, next,
                                                                             health, la);
     else {
         constexpr int k = g2p_per_thread(true, kG2PPlain, false);
         g2p_kernel<true, kG2PPlain><<<blocks_for(n, (long long)pb * k), pb, k * 3 * pb * sizeof(float4), st>>>(
-            sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, prank, next, health, la);
+            sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, next, health, la);
     }
     return 1;
 }
