@@ -54,6 +54,13 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Programmatic dependent launch: the substep's kernels are launched with
+// programmatic stream serialisation (launch_dep), so that a kernel's CTAs are
+// scheduled while its predecessor drains; each such kernel waits here, before
+// touching memory, until its predecessor has completed and its writes are
+// visible (griddepcontrol.wait; a no-op for an ordinary launch).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Files this lane's particle under global cell `gcell` (global bin `gbin`,
 // bin `bin` of scene `scene`, whose bin entries start at `boff`) of a counter
 // set: one reduction per distinct cell of the warp (no value comes back, so
@@ -302,6 +309,7 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
                                                                   uint32_t* __restrict__ work,
                                                                   float4* __restrict__ accum_all, int4* __restrict__ crowd,
                                                                   int crowd_cap, uint32_t* __restrict__ status, int cap) {
+    pdl_wait();
     __shared__ __align__(16) float4 s_ring[kRing][6][32];
     __shared__ float4 s_foot[kFootNodes];
     __shared__ int32_t s_gidx[kGidxStage];
@@ -446,6 +454,7 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_crowd_kernel(SceneTabl
                                                                         uint32_t* __restrict__ work,
                                                                         float4* __restrict__ accum_all,
                                                                         uint32_t* __restrict__ status) {
+    pdl_wait();
     __shared__ __align__(16) float4 s_ring[kRing][6][32];
     const int lane = threadIdx.x;
     const int total = (int)min(*reinterpret_cast<volatile const uint32_t*>(work + 2), (uint32_t)crowd_cap);
@@ -584,6 +593,7 @@ __device__ __forceinline__ int scan_block_sum(int v, int* s_red) {
 
 __global__ void __launch_bounds__(kScanThreads) bin_sum_kernel(SceneTable sc, const uint32_t* __restrict__ bcount_all,
                                                                int32_t* __restrict__ bpart) {
+    pdl_wait();
     __shared__ int s_red[kScanWarps];
     const int scene = blockIdx.x, chunk = blockIdx.y;
     const int nbins = sc.prm[scene].nb + 1;
@@ -610,6 +620,7 @@ __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(SceneTable sc, c
                                                                 const uint32_t* __restrict__ clear_nlist,
                                                                 long long* __restrict__ itemoff,
                                                                 long long* __restrict__ clroff) {
+    pdl_wait();
     __shared__ int s_val[kScanChunk];
     __shared__ int s_red[kScanWarps];
     __shared__ int s_warp[kScanWarps];
@@ -745,6 +756,7 @@ __global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet se
                                                         uint8_t* __restrict__ corder,
                                                         BinSet clear, const long long* __restrict__ itemoff,
                                                         const long long* __restrict__ clroff) {
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -790,6 +802,7 @@ __global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet se
 __global__ void __launch_bounds__(256) bin_scatter_kernel(long long n, int scenes, const int32_t* __restrict__ pcell,
                                                           int32_t* __restrict__ ccur, int32_t* __restrict__ gidx,
                                                           uint32_t* __restrict__ clear_nlist) {
+    pdl_wait();
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (j == 0)
         for (int s2 = 0; s2 < scenes; ++s2) clear_nlist[s2] = 0u;
@@ -813,6 +826,7 @@ template <bool kBatch>
 __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimParams p0, long long g_total,
                                                           float4* __restrict__ accum, float4* __restrict__ vgrid,
                                                           const float* __restrict__ sdf_all) {
+    pdl_wait();
     __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
     __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
     __shared__ int s_range[2];
@@ -891,6 +905,7 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
                                                   const float4* __restrict__ vgrid_all, const float* __restrict__ sdf_all,
                                                   int32_t* __restrict__ pcell, BinSet next,
                                                   uint32_t* __restrict__ health, LearnArgs la) {
+    pdl_wait();
     __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
     __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
     __shared__ int s_range[2];
@@ -1348,6 +1363,23 @@ __global__ void __launch_bounds__(256) copy_words_kernel(uint32_t* __restrict__ 
 
 inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
 
+// Launches a substep kernel (one that starts with pdl_wait) with programmatic
+// stream serialisation.
+template <typename... P, typename... A>
+void launch_dep(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<P>(args)...);
+}
+
 }  // namespace
 
 int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t* pcell, const BinSet& set,
@@ -1365,12 +1397,12 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
                      int scan_chunks, cudaStream_t st) {
     if (n <= 0) return 0;
     const dim3 scan_grid((unsigned)sc.count, (unsigned)scan_chunks);
-    bin_sum_kernel<<<scan_grid, kScanThreads, 0, st>>>(sc, cur.bcount, bpart);
-    bin_scan_kernel<<<scan_grid, kScanThreads, 0, st>>>(sc, cur.bcount, other.bcount, bpart, bstart, work, cur.nlist,
+    launch_dep(bin_sum_kernel, scan_grid, kScanThreads, 0, st, sc, cur.bcount, bpart);
+    launch_dep(bin_scan_kernel, scan_grid, kScanThreads, 0, st, sc, cur.bcount, other.bcount, bpart, bstart, work, cur.nlist,
                                                        other.nlist, itemoff, clroff);
     const int ctas = (int)std::max(1LL, std::min((long long)blocks_for(bins_total * 32, 128), 148LL * 8));
-    cell_scan_kernel<<<ctas, 128, 0, st>>>(sc, cur, bstart, cstart, ccur, corder, other, itemoff, clroff);
-    bin_scatter_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, sc.count, pcell, ccur, gidx, other.nlist);
+    launch_dep(cell_scan_kernel, ctas, 128, 0, st, sc, cur, bstart, cstart, ccur, corder, other, itemoff, clroff);
+    launch_dep(bin_scatter_kernel, blocks_for(n, 256), 256, 0, st, n, sc.count, pcell, ccur, gidx, other.nlist);
     return 4;
 }
 
@@ -1391,9 +1423,9 @@ int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const fl
     const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : kP2GWarpsPerSM;
     const int cap = cell_cap > 0 ? cell_cap : 0;
     const int warps = (int)std::min(bins_total * kBinZ, 148LL * per_sm);
-    p2g_kernel<<<warps, 32, 0, st>>>(sc, P, gidx, cstart, cur, corder, itemoff, work, accum, crowd, crowd_cap, status,
+    launch_dep(p2g_kernel, warps, 32, 0, st, sc, P, gidx, cstart, cur, corder, itemoff, work, accum, crowd, crowd_cap, status,
                                      cap);
-    p2g_crowd_kernel<<<148 * kP2GWarpsPerSM, 32, 0, st>>>(sc, P, gidx, crowd, crowd_cap, work, accum, status);
+    launch_dep(p2g_crowd_kernel, 148 * kP2GWarpsPerSM, 32, 0, st, sc, P, gidx, crowd, crowd_cap, work, accum, status);
     return 2;
 }
 
@@ -1402,9 +1434,9 @@ int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_to
     if (g_total <= 0) return 0;
     const int b = (block == 128 || block == 256) ? block : 256;
     if (sc.count == 1)
-        grid_update_kernel<false><<<blocks_for(g_total, b), b, 0, st>>>(sc, p0, g_total, accum, vgrid, sdf);
+        launch_dep(grid_update_kernel<false>, blocks_for(g_total, b), b, 0, st, sc, p0, g_total, accum, vgrid, sdf);
     else
-        grid_update_kernel<true><<<blocks_for(g_total, b), b, 0, st>>>(sc, p0, g_total, accum, vgrid, sdf);
+        launch_dep(grid_update_kernel<true>, blocks_for(g_total, b), b, 0, st, sc, p0, g_total, accum, vgrid, sdf);
     return 1;
 }
 
@@ -1416,7 +1448,7 @@ int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const flo
     const LearnArgs la = learn ? *learn : LearnArgs{};
     const unsigned grid = blocks_for(n, 256);
     if (learn && sc.count == 1 && la.mlp_tc) {
-        g2p_kernel<false, kG2PLearnedTc><<<grid, 256, sizeof(MlpTcSmem), st>>>(
+        launch_dep(g2p_kernel<false, kG2PLearnedTc>, grid, 256, sizeof(MlpTcSmem), st,
             sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, next, health, la);
         return 1;
     }
@@ -1425,28 +1457,28 @@ int launch_g2p(const SceneTable& sc, const SimParams& p0, long long n, const flo
     const bool wide = block == 512;
     const int pb = wide ? 256 : ((block == 128 || block == 256) ? block : 256);
     if (learn && sc.count == 1 && la.mlp)
-        g2p_kernel<false, kG2PLearned><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+        launch_dep(g2p_kernel<false, kG2PLearned>, grid, 256, 0, st, sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
                                                              pcell, next, health, la);
     else if (learn && sc.count == 1 && la.feat)
-        g2p_kernel<false, kG2PCollect><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+        launch_dep(g2p_kernel<false, kG2PCollect>, grid, 256, 0, st, sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
                                                              pcell, next, health, la);
     else if (learn && sc.count == 1)
-        g2p_kernel<false, kG2PLarge><<<grid, 256, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
+        launch_dep(g2p_kernel<false, kG2PLarge>, grid, 256, 0, st, sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf,
                                                            pcell, next, health, la);
     else if (sc.count == 1 && wide)
-        g2p_kernel<false, kG2PPlain, true><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in,
+        launch_dep(g2p_kernel<false, kG2PPlain, true>, blocks_for(n, pb), pb, 0, st, sc, p0, n, Pin, Pout, gidx, sig_in,
                                                                              sig_out, vgrid, sdf, pcell, next,
                                                                              health, la);
     else if (sc.count == 1)
-        g2p_kernel<false, kG2PPlain><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in, sig_out,
+        launch_dep(g2p_kernel<false, kG2PPlain>, blocks_for(n, pb), pb, 0, st, sc, p0, n, Pin, Pout, gidx, sig_in, sig_out,
                                                                        vgrid, sdf, pcell, next, health, la);
     else if (wide)
-        g2p_kernel<true, kG2PPlain, true><<<blocks_for(n, pb), pb, 0, st>>>(sc, p0, n, Pin, Pout, gidx, sig_in,
+        launch_dep(g2p_kernel<true, kG2PPlain, true>, blocks_for(n, pb), pb, 0, st, sc, p0, n, Pin, Pout, gidx, sig_in,
                                                                             sig_out, vgrid, sdf, pcell, next,
                                                                             health, la);
     else {
         constexpr int k = g2p_per_thread(true, kG2PPlain, false);
-        g2p_kernel<true, kG2PPlain><<<blocks_for(n, (long long)pb * k), pb, k * 3 * pb * sizeof(float4), st>>>(
+        launch_dep(g2p_kernel<true, kG2PPlain>, blocks_for(n, (long long)pb * k), pb, k * 3 * pb * sizeof(float4), st,
             sc, p0, n, Pin, Pout, gidx, sig_in, sig_out, vgrid, sdf, pcell, next, health, la);
     }
     return 1;
