@@ -797,23 +797,39 @@ __global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet se
 
 // gidx[slot] = j: the order by cell, each particle taking the next slot of
 // its cell from the cursor ccur[cell] (one atomic per distinct cell of a warp;
-// the lanes sharing a cell take consecutive slots in lane order).  Thread 0
-// also resets the other set's lists, which cell_scan_kernel has just cleared.
+// the lanes sharing a cell take consecutive slots in lane order).  A thread
+// files kScatterPer particles (block b: particles b * kScatterPer * blockDim
+// .. + kScatterPer * blockDim, one blockDim-wide slice per pass), so that the
+// cursor atomics of its passes are in flight together.  Thread 0 also resets
+// the other set's lists, which cell_scan_kernel has just cleared.
+constexpr int kScatterPer = 4;
+
 __global__ void __launch_bounds__(256) bin_scatter_kernel(long long n, int scenes, const int32_t* __restrict__ pcell,
                                                           int32_t* __restrict__ ccur, int32_t* __restrict__ gidx,
                                                           uint32_t* __restrict__ clear_nlist) {
     pdl_wait();
-    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (j == 0)
+    const long long j0 = blockIdx.x * (long long)blockDim.x * kScatterPer + threadIdx.x;
+    if (j0 == 0)
         for (int s2 = 0; s2 < scenes; ++s2) clear_nlist[s2] = 0u;
-    const int cell = j < n ? __ldg(pcell + j) : -1;
     const int lane = threadIdx.x & 31;
-    const uint32_t peers = __match_any_sync(0xffffffffu, cell);
-    const int leader = __ffs(peers) - 1;
-    int base = 0;
-    if (cell >= 0 && lane == leader) base = atomicAdd(ccur + cell, __popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (cell >= 0) gidx[base + __popc(peers & lanemask_lt())] = (int32_t)j;
+    int cell[kScatterPer], base[kScatterPer];
+    uint32_t peers[kScatterPer];
+#pragma unroll
+    for (int k = 0; k < kScatterPer; ++k) {
+        const long long j = j0 + (long long)k * blockDim.x;
+        cell[k] = j < n ? __ldg(pcell + j) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < kScatterPer; ++k) {
+        peers[k] = __match_any_sync(0xffffffffu, cell[k]);
+        base[k] = 0;
+        if (cell[k] >= 0 && lane == __ffs(peers[k]) - 1) base[k] = atomicAdd(ccur + cell[k], __popc(peers[k]));
+    }
+#pragma unroll
+    for (int k = 0; k < kScatterPer; ++k) {
+        const int b = __shfl_sync(0xffffffffu, base[k], __ffs(peers[k]) - 1);
+        if (cell[k] >= 0) gidx[b + __popc(peers[k] & lanemask_lt())] = (int32_t)(j0 + (long long)k * blockDim.x);
+    }
 }
 
 // ---------------------------------------------------------- grid update ----
@@ -1402,7 +1418,7 @@ int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, co
                                                        other.nlist, itemoff, clroff);
     const int ctas = (int)std::max(1LL, std::min((long long)blocks_for(bins_total * 32, 128), 148LL * 8));
     launch_dep(cell_scan_kernel, ctas, 128, 0, st, sc, cur, bstart, cstart, ccur, corder, other, itemoff, clroff);
-    launch_dep(bin_scatter_kernel, blocks_for(n, 256), 256, 0, st, n, sc.count, pcell, ccur, gidx, other.nlist);
+    launch_dep(bin_scatter_kernel, blocks_for(n, 256 * kScatterPer), 256, 0, st, n, sc.count, pcell, ccur, gidx, other.nlist);
     return 4;
 }
 
