@@ -107,6 +107,8 @@ struct mpm_engine {
     // {list lengths of set 0 (S), of set 1 (S), P2G work, G2P work, crowded-cell
     // list length, crowded-cell entries taken}.
     void* bins_mem = nullptr;
+    void* tiles_mem = nullptr;  // grid-update tile marks: stamp, mark[bins_total], dirty[bins_total]
+    mpm::TileMarks tiles{};
     mpm::BinSet bins[2] = {};
     int32_t* bstart = nullptr;
     int32_t* cstart = nullptr;
@@ -325,6 +327,7 @@ size_t bins_set_words(const mpm_engine* e) {
     return align_up((size_t)e->cells_total + 2 * (size_t)e->bins_total, 64);
 }
 size_t bins_bytes(const mpm_engine* e) { return 2 * bins_set_words(e) * sizeof(uint32_t); }
+size_t tiles_bytes(const mpm_engine* e) { return (size_t)(1 + e->bins_total) * sizeof(uint32_t) + (size_t)e->bins_total; }
 
 void carve_bins(mpm_engine* e) {
     uint32_t* base = static_cast<uint32_t*>(e->bins_mem);
@@ -354,6 +357,12 @@ mpm_status upload_table(mpm_engine* e) {
     return MPM_OK;
 }
 
+// The tile marks when the grid update works on touched tiles only
+// (grid_block 0, one scene), else none: every node is updated.
+mpm::TileMarks active_tiles(const mpm_engine* e) {
+    return (e->scenes == 1 && e->tune.grid_block == 0) ? e->tiles : mpm::TileMarks{};
+}
+
 // Enqueues stages `from`..`upto` (MPM_STAGE_*) of one substep from parity
 // `par`, for all scenes.  With `marks` (only while capturing a graph), records
 // marks[0..4] as event-record nodes before the ordering and after each stage.
@@ -369,7 +378,7 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
     if (from <= MPM_STAGE_SORT && upto >= MPM_STAGE_SORT)
         launches += mpm::launch_bin_order(sc, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart, e->cstart,
                                           e->pcell, e->ccur, e->gidx, e->corder, e->d_itemoff, e->d_clroff, work, e->bpart,
-                                          e->scan_chunks, st);
+                                          e->scan_chunks, active_tiles(e), st);
     mark(1);
     if (from <= MPM_STAGE_P2G && upto >= MPM_STAGE_P2G)
         launches += mpm::launch_p2g(sc, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par], e->corder, e->d_itemoff,
@@ -377,7 +386,7 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
                                     e->tune.p2g_cell_cap);
     mark(2);
     if (from <= MPM_STAGE_GRID && upto >= MPM_STAGE_GRID)
-        launches += mpm::launch_grid_update(sc, e->prm[0], e->g_total, e->accum, e->vgrid, e->sdf, st,
+        launches += mpm::launch_grid_update(sc, e->prm[0], e->g_total, e->accum, e->vgrid, e->sdf, active_tiles(e), st,
                                             e->tune.grid_block);
     mark(3);
     if (from <= MPM_STAGE_G2P && upto >= MPM_STAGE_G2P)
@@ -390,6 +399,9 @@ int enqueue_substep(mpm_engine* e, int par, int from, int upto, const cudaEvent_
 
 mpm_status capture_graphs(mpm_engine* e) {
     destroy_learned_graphs(e);  // they embed the launch shapes too
+    // Touched tiles only: after updates of every node any tile may hold
+    // velocities, so the first tile update resets every tile not marked.
+    if (active_tiles(e).mark) CK(e, cudaMemsetAsync(e->tiles.dirty, 1, (size_t)e->bins_total, e->stream));
     const bool timed = e->timing_cap > 0;
     for (int par = 0; par < 2; ++par) {
         if (e->graph[par]) cudaGraphExecDestroy(e->graph[par]);
@@ -516,6 +528,7 @@ mpm_status load_states(mpm_engine* e, const float* const* soa26_host, bool init_
     e->partial_stage = 0;
     CK(e, cudaMemsetAsync(e->accum, 0, (size_t)e->g_total * sizeof(float4), e->stream));
     CK(e, cudaMemsetAsync(e->vgrid, 0, (size_t)e->g_total * sizeof(float4), e->stream));
+    CK(e, cudaMemsetAsync(e->tiles.dirty, 0, (size_t)e->bins_total, e->stream));  // the velocity grid is zero
     CK(e, cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(uint32_t), e->stream));
     e->accum_dirty = false;
     e->grid_view = GridView::kVelocity;
@@ -713,6 +726,7 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
         (err = cudaMalloc(&e->d_flags, 2 * sizeof(uint32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->ctl, (2 * count + 4) * sizeof(uint32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->bins_mem, bins_bytes(e))) != cudaSuccess ||
+        (err = cudaMalloc(&e->tiles_mem, tiles_bytes(e))) != cudaSuccess ||
         (err = cudaMalloc(&e->bstart, (size_t)bins_total * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->bpart, (size_t)count * e->scan_chunks * sizeof(int32_t))) != cudaSuccess ||
         (err = cudaMalloc(&e->cstart, (size_t)cells_total * sizeof(int32_t))) != cudaSuccess ||
@@ -725,13 +739,21 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
         (err = cudaMalloc(&e->d_clroff, (count + 1) * sizeof(long long))) != cudaSuccess)
         return fail(cuda_fail(e, err, "cudaMalloc(grid)"));
     carve_bins(e);
+    e->tiles.stamp = static_cast<uint32_t*>(e->tiles_mem);
+    e->tiles.mark = e->tiles.stamp + 1;
+    e->tiles.dirty = reinterpret_cast<uint8_t*>(e->tiles.mark + e->bins_total);
     keep_accum_in_l2(e, device);
     e->table.prm = e->d_prm;
     e->table.poff = e->d_poff;
     e->table.goff = e->d_goff;
     e->table.count = count;
+    // A grid of 2^23 nodes or more (256^3) is mostly empty in the workloads
+    // measured; there the touched-tile update is 2.7x faster than the update
+    // of every node, while on 128^3 it ties and on 64^3 it is slower.
+    if (count == 1 && g_total >= (1LL << 23)) e->tune.grid_block = 0;
     cudaMemsetAsync(e->accum, 0, (size_t)g_total * sizeof(float4), e->stream);
     cudaMemsetAsync(e->vgrid, 0, (size_t)g_total * sizeof(float4), e->stream);
+    cudaMemsetAsync(e->tiles_mem, 0, tiles_bytes(e), e->stream);
     cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(uint32_t), e->stream);
     // An empty triangle list leaves sqrt(1e30) everywhere (kernels.cu:289,299).
     e->kernel_launches += mpm::launch_fill(e->sdf, g_total, sqrtf(1e30f), e->stream);
@@ -815,11 +837,11 @@ int enqueue_large(mpm_engine* e, int par, const mpm::LearnArgs* learn) {
     int launches = 0;
     launches += mpm::launch_bin_order(e->table, e->n, e->bins_scan, e->bins[par], e->bins[1 - par], e->bstart,
                                       e->cstart, e->pcell, e->ccur, e->gidx, e->corder, e->d_itemoff, e->d_clroff, work, e->bpart,
-                                          e->scan_chunks, st);
+                                          e->scan_chunks, active_tiles(e), st);
     launches += mpm::launch_p2g(e->table_large, e->n, e->bins_scan, e->P[par], e->gidx, e->cstart, e->bins[par],
                                 e->corder, e->d_itemoff, work, e->accum, e->crowd, e->crowd_cap, e->d_flags + 1, st, e->tune.p2g_ctas_per_sm,
                                 e->tune.p2g_cell_cap);
-    launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, st,
+    launches += mpm::launch_grid_update(e->table_large, big, e->g_total, e->accum, e->vgrid, e->sdf, active_tiles(e), st,
                                         e->tune.grid_block);
     launches += mpm::launch_g2p(e->table_large, big, e->n, e->P[par], e->P[1 - par], e->gidx, e->sigma[par],
                                 e->sigma[1 - par], e->vgrid, e->sdf, e->pcell, e->bins[1 - par], e->d_flags,
@@ -1010,6 +1032,7 @@ extern "C" void mpm_destroy(mpm_engine* e) {
     free_dev(e->vgrid);
     free_dev(e->sdf);
     free_dev(e->bins_mem);
+    free_dev(e->tiles_mem);
     free_dev(e->bstart);
     free_dev(e->ccur);
     free_dev(e->bpart);
@@ -1778,7 +1801,7 @@ namespace {
 bool valid_tuning(const mpm_tuning& t) {
     return t.p2g_ctas_per_sm >= 1 && t.p2g_ctas_per_sm <= mpm::p2g_max_ctas_per_sm() &&
            (t.g2p_block == 128 || t.g2p_block == 256 || t.g2p_block == 512) &&
-           (t.grid_block == 128 || t.grid_block == 256) &&
+           (t.grid_block == 0 || t.grid_block == 128 || t.grid_block == 256) &&
            (t.p2g_cell_cap == 0 || (t.p2g_cell_cap >= 4 && t.p2g_cell_cap <= 64));
 }
 
@@ -1805,6 +1828,8 @@ extern "C" mpm_status mpm_set_tuning(mpm_engine* e, const mpm_tuning* t) {
     mpm_status s = enter(e);
     if (s != MPM_OK) return s;
     if (!t || !valid_tuning(*t)) return record(e, MPM_ERR_INVALID_ARGUMENT, "tuning out of range");
+    if (t->grid_block == 0 && e->scenes != 1)
+        return record(e, MPM_ERR_INVALID_ARGUMENT, "grid_block 0 (touched tiles) needs an engine of one scene");
     e->tune.p2g_ctas_per_sm = t->p2g_ctas_per_sm;
     e->tune.g2p_block = t->g2p_block;
     e->tune.grid_block = t->grid_block;
@@ -1862,8 +1887,9 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
     // item from the counts it sees, which follows the state as it evolves,
     // while a fixed value timed on one state can cost far more later.
     tbest = 1e30f;
-    for (int k : {128, 256}) {
+    for (int k : {128, 256, 0}) {
         if (s != MPM_OK) break;
+        if (k == 0 && e->scenes != 1) break;
         e->tune.grid_block = k;
         if ((s = median_time(MPM_STAGE_GRID, &ms)) != MPM_OK) break;
         if (ms < tbest) tbest = ms, best.grid_block = k, best.grid_ms = ms;

@@ -63,6 +63,19 @@ struct BinSet {
     uint32_t* nlist;
 };
 
+// Node tiles of the grid update, one per bin: tile (bx, by, bz) of a scene
+// holds the nodes x in [8 bx - 2, 8 bx + 6), y in [4 by - 2, 4 by + 2), z in
+// [4 bz - 2, 4 bz + 2), so that the 10 x 6 x 6 nodes a bin's particles reach
+// lie in tiles bx..bx+1 x by..by+1 x bz..bz+1.  stamp[0] counts orderings;
+// mark[global bin] = the stamp of the last ordering whose listed bins reach
+// the tile; dirty[global bin] = 1 while the tile's velocity nodes may hold
+// values other than zero.
+struct TileMarks {
+    uint32_t* stamp;
+    uint32_t* mark;
+    uint8_t* dirty;
+};
+
 // Files the n particles of P (all scenes, slot order) into an empty set.
 int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t* pcell, const BinSet& set,
                      cudaStream_t st);
@@ -71,13 +84,15 @@ int launch_bin_count(const SceneTable& sc, long long n, const float* P, int32_t*
 // listed bin's cells, one byte per cell, indexed like the cells), gidx[new
 // slot] = old slot, itemoff (the P2G work items of each scene: kBinZ per
 // listed bin, prefix, S + 1 entries) and clroff (the same prefix of `other`'s
-// listed bins, one per bin); clears `other` and the work counters work[0..1].
+// listed bins, one per bin); clears `other` and the work counters work[0..1];
+// with tiles.mark set, advances tiles.stamp and marks the tiles the listed
+// bins of `cur` reach.
 // bins_total: sum over scenes of nb + 1.  bpart: scenes x scan_chunks ints of
 // scratch; scan_chunks = bin_scan_chunks(largest nb + 1).
 int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
                      int32_t* bstart, int32_t* cstart, const int32_t* pcell, int32_t* ccur, int32_t* gidx,
                      uint8_t* corder, long long* itemoff, long long* clroff, uint32_t* work, int32_t* bpart,
-                     int scan_chunks, cudaStream_t st);
+                     int scan_chunks, const TileMarks& tiles, cudaStream_t st);
 // Chunks of the bin scan for a scene of `bins` scanned bins.
 int bin_scan_chunks(long long bins);
 // P2G over the items of `cur`; gidx maps slots of the new order to P.  Two
@@ -93,8 +108,11 @@ int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const fl
 // Most P2G CTAs that fit on one SM.
 int p2g_max_ctas_per_sm();
 // p0: the parameters of scene 0, used directly when the table holds one scene.
+// With tiles.mark set (one scene only): only the tiles marked by this
+// substep's ordering are updated, and tiles updated before but not marked now
+// are reset to zero; else every node.
 int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
-                       const float* sdf, cudaStream_t st, int block = 256);
+                       const float* sdf, const TileMarks& tiles, cudaStream_t st, int block = 256);
 // Large-step G2P (one scene): particles advect with v_old + blend (v_new -
 // v_old).  With mlp set: the corrector's correction is added to each
 // particle's velocity and stat[0] += sum over particles of |1 / det(I + dt C)

@@ -619,7 +619,8 @@ __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(SceneTable sc, c
                                                                 const uint32_t* __restrict__ cur_nlist,
                                                                 const uint32_t* __restrict__ clear_nlist,
                                                                 long long* __restrict__ itemoff,
-                                                                long long* __restrict__ clroff) {
+                                                                long long* __restrict__ clroff,
+                                                                uint32_t* __restrict__ tstamp) {
     pdl_wait();
     __shared__ int s_val[kScanChunk];
     __shared__ int s_red[kScanWarps];
@@ -631,6 +632,7 @@ __global__ void __launch_bounds__(kScanThreads) bin_scan_kernel(SceneTable sc, c
         work[1] = 0u;  // G2P items
         work[2] = 0u;  // crowded-cell list length
         work[3] = 0u;  // crowded-cell entries taken
+        if (tstamp) *tstamp += 1u;  // this ordering's tile stamp
         // Per-scene prefixes: P2G items (kBinZ per listed bin of the current
         // set) and the listed bins of the set to clear.
         long long run = 0, runc = 0;
@@ -755,9 +757,12 @@ __global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet se
                                                         int32_t* __restrict__ cstart, int32_t* __restrict__ ccur,
                                                         uint8_t* __restrict__ corder,
                                                         BinSet clear, const long long* __restrict__ itemoff,
-                                                        const long long* __restrict__ clroff) {
+                                                        const long long* __restrict__ clroff,
+                                                        const uint32_t* __restrict__ tstamp,
+                                                        uint32_t* __restrict__ tmark) {
     pdl_wait();
     const int lane = threadIdx.x & 31;
+    const uint32_t stamp = tmark ? *tstamp : 0u;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     // Listed bins of all scenes, one after another (itemoff counts kBinZ items per bin).
@@ -784,6 +789,14 @@ __global__ void __launch_bounds__(128) cell_scan_kernel(SceneTable sc, BinSet se
         *reinterpret_cast<int4*>(cstart + c0) = st;
         *reinterpret_cast<int4*>(ccur + c0) = st;  // the scatter's cursors start at the cells' first slots
         cell_order(c, corder + (size_t)coff + (size_t)bin * kBinCells);
+        // The grid-update tiles this bin's particles reach: tiles bin + (dx,
+        // dy, dz), d in {0, 1}^3, lane d.
+        const SimParams& ps = sc.prm[scene];
+        if (tmark && lane < 8 && bin < ps.nb) {
+            const int tx = bin % ps.nbx + (lane & 1), ty = (bin / ps.nbx) % ps.nby + ((lane >> 1) & 1),
+                      tz = bin / (ps.nbx * ps.nby) + (lane >> 2);
+            if (tx < ps.nbx && ty < ps.nby && tz < ps.nbz) tmark[boff + ((long long)tz * ps.nby + ty) * ps.nbx + tx] = stamp;
+        }
     }
     const long long nclear = clroff[sc.count];
     for (long long it = gw; it < nclear; it += nw) {
@@ -838,26 +851,12 @@ __global__ void __launch_bounds__(256) bin_scatter_kernel(long long n, int scene
 // zeroes accum for the next P2G.  The wall tests use the reference's
 // unsigned arithmetic (SimConfig fields are uint32_t): x < PADDING and
 // x > SIZE-1-PADDING with wrap-around.
-template <bool kBatch>
-__global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimParams p0, long long g_total,
-                                                          float4* __restrict__ accum, float4* __restrict__ vgrid,
-                                                          const float* __restrict__ sdf_all) {
-    pdl_wait();
-    __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
-    __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
-    __shared__ int s_range[2];
-    const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const SceneLookup<kBatch> look(sc, sc.goff, s_prm, s_first, s_range, blockIdx.x * (long long)blockDim.x,
-                                   min((blockIdx.x + 1) * (long long)blockDim.x, g_total));
-    if (gi >= g_total) return;
-    const SimParams& p = kBatch ? look.params(look.scene(gi)) : p0;
-    const int idx = (int)(gi - p.goff);
-    const float* sdf = sdf_all + p.goff;
-    const float4 a = accum[gi];
+// One node at (x, y, z): (mass, v) for the velocity grid from its
+// accumulated (mass, momentum) `a`; `inside`: the node's SDF is negative.
+__device__ __forceinline__ float4 update_node(const SimParams& p, int x, int y, int z, float4 a, bool inside,
+                                             const float* __restrict__ sdf) {
     float4 out = make_float4(a.x, 0.f, 0.f, 0.f);
-    const bool inside = __ldg(sdf + idx) < 0.0f;
     if (a.x > 1e-9f) {
-        const int x = idx % p.sx, y = (idx / p.sx) % p.sy, z = idx / (p.sx * p.sy);
         float vx = a.y / a.x;
         float vy = a.z / a.x - p.gravity * p.dt;
         float vz = a.w / a.x;
@@ -881,8 +880,78 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
     }
     // Sign bit of the mass: the node's SDF is negative (G2P's obstacle test).
     if (inside) out.x = -out.x;
-    vgrid[gi] = out;
+    return out;
+}
+
+// Every node of every scene, one thread per node.
+template <bool kBatch>
+__global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimParams p0, long long g_total,
+                                                          float4* __restrict__ accum, float4* __restrict__ vgrid,
+                                                          const float* __restrict__ sdf_all) {
+    pdl_wait();
+    __shared__ SimParams s_prm[kBatch ? kTableScenes : 1];
+    __shared__ long long s_first[kBatch ? kTableScenes + 1 : 1];
+    __shared__ int s_range[2];
+    const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const SceneLookup<kBatch> look(sc, sc.goff, s_prm, s_first, s_range, blockIdx.x * (long long)blockDim.x,
+                                   min((blockIdx.x + 1) * (long long)blockDim.x, g_total));
+    if (gi >= g_total) return;
+    const SimParams& p = kBatch ? look.params(look.scene(gi)) : p0;
+    const int idx = (int)(gi - p.goff);
+    const float* sdf = sdf_all + p.goff;
+    const float4 a = accum[gi];
+    const bool inside = __ldg(sdf + idx) < 0.0f;
+    const int x = idx % p.sx, y = (idx / p.sx) % p.sy, z = idx / (p.sx * p.sy);
+    vgrid[gi] = update_node(p, x, y, z, a, inside, sdf);
     if (a.x != 0.f || a.y != 0.f || a.z != 0.f || a.w != 0.f) accum[gi] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// One scene, one warp per node tile (TileMarks): lane l takes the nodes
+// (x0 + l % 8, y0 + l / 8, z0 + c), c = 0..3.  A tile marked by this
+// substep's ordering is updated like grid_update_kernel; a tile updated
+// before but not marked now holds no accumulated mass any more and is reset to
+// zero; every other tile is already zero and is skipped.  Every node the
+// substep's particles reach lies in a marked tile, and G2P reads no other.
+__global__ void __launch_bounds__(256) grid_tiles_kernel(SimParams p, TileMarks tiles, float4* __restrict__ accum,
+                                                         float4* __restrict__ vgrid, const float* __restrict__ sdf) {
+    pdl_wait();
+    const int t = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= p.nb) return;  // warp-uniform
+    const bool act = tiles.mark[p.boff + t] == *tiles.stamp;
+    const bool dirty = tiles.dirty[p.boff + t] != 0;
+    if (!act && !dirty) return;
+    __syncwarp();  // every lane has read the flag lane 0 rewrites below
+    const int x = (t % p.nbx) * kBinX - 2 + (lane & 7);
+    const int y = ((t / p.nbx) % p.nby) * kBinY - 2 + (lane >> 3);
+    const int z0 = (t / (p.nbx * p.nby)) * kBinZ - 2;
+    const bool xy = (unsigned)x < (unsigned)p.sx && (unsigned)y < (unsigned)p.sy;
+    if (act) {
+        float4 a[kBinZ];
+        bool inside[kBinZ];
+#pragma unroll
+        for (int c = 0; c < kBinZ; ++c) {
+            const bool ok = xy && (unsigned)(z0 + c) < (unsigned)p.sz;
+            const int i = ok ? node_index(p, x, y, z0 + c) : 0;
+            a[c] = ok ? accum[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            inside[c] = ok && __ldg(sdf + i) < 0.0f;
+        }
+#pragma unroll
+        for (int c = 0; c < kBinZ; ++c) {
+            if (!xy || (unsigned)(z0 + c) >= (unsigned)p.sz) continue;
+            const int i = node_index(p, x, y, z0 + c);
+            vgrid[i] = update_node(p, x, y, z0 + c, a[c], inside[c], sdf);
+            if (a[c].x != 0.f || a[c].y != 0.f || a[c].z != 0.f || a[c].w != 0.f)
+                accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < kBinZ; ++c)
+            if (xy && (unsigned)(z0 + c) < (unsigned)p.sz)
+                vgrid[node_index(p, x, y, z0 + c)] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncwarp();
+    if (lane == 0 && act != dirty) tiles.dirty[p.boff + t] = act ? 1 : 0;
 }
 
 // ------------------------------------------------------------------ G2P ----
@@ -1410,14 +1479,15 @@ int bin_scan_chunks(long long bins) { return (int)std::max(1LL, (bins + kScanChu
 int launch_bin_order(const SceneTable& sc, long long n, long long bins_total, const BinSet& cur, const BinSet& other,
                      int32_t* bstart, int32_t* cstart, const int32_t* pcell, int32_t* ccur, int32_t* gidx,
                      uint8_t* corder, long long* itemoff, long long* clroff, uint32_t* work, int32_t* bpart,
-                     int scan_chunks, cudaStream_t st) {
+                     int scan_chunks, const TileMarks& tiles, cudaStream_t st) {
     if (n <= 0) return 0;
     const dim3 scan_grid((unsigned)sc.count, (unsigned)scan_chunks);
     launch_dep(bin_sum_kernel, scan_grid, kScanThreads, 0, st, sc, cur.bcount, bpart);
     launch_dep(bin_scan_kernel, scan_grid, kScanThreads, 0, st, sc, cur.bcount, other.bcount, bpart, bstart, work, cur.nlist,
-                                                       other.nlist, itemoff, clroff);
+                                                       other.nlist, itemoff, clroff, tiles.stamp);
     const int ctas = (int)std::max(1LL, std::min((long long)blocks_for(bins_total * 32, 128), 148LL * 8));
-    launch_dep(cell_scan_kernel, ctas, 128, 0, st, sc, cur, bstart, cstart, ccur, corder, other, itemoff, clroff);
+    launch_dep(cell_scan_kernel, ctas, 128, 0, st, sc, cur, bstart, cstart, ccur, corder, other, itemoff, clroff,
+               tiles.stamp, tiles.mark);
     launch_dep(bin_scatter_kernel, blocks_for(n, 256 * kScatterPer), 256, 0, st, n, sc.count, pcell, ccur, gidx, other.nlist);
     return 4;
 }
@@ -1446,9 +1516,13 @@ int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const fl
 }
 
 int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
-                       const float* sdf, cudaStream_t st, int block) {
+                       const float* sdf, const TileMarks& tiles, cudaStream_t st, int block) {
     if (g_total <= 0) return 0;
     const int b = (block == 128 || block == 256) ? block : 256;
+    if (sc.count == 1 && tiles.mark) {
+        launch_dep(grid_tiles_kernel, blocks_for(p0.nb, 8), 256, 0, st, p0, tiles, accum, vgrid, sdf);
+        return 1;
+    }
     if (sc.count == 1)
         launch_dep(grid_update_kernel<false>, blocks_for(g_total, b), b, 0, st, sc, p0, g_total, accum, vgrid, sdf);
     else
