@@ -550,9 +550,9 @@ typedef struct mpm_tuning {
     int32_t g2p_block;        /* 128 or 256 (default 256); 512 = 256-thread CTAs free to use up to
                                * 255 registers (more loads in flight, fewer warps) */
     int32_t grid_block;       /* 128 or 256: the update visits every node in CTAs of that size;
-                               * 0 (engines of one scene): only the node tiles this substep's
-                               * particles reach, plus a reset of tiles they left (default
-                               * for one scene of 2^23 nodes or more, else 256) */
+                               * 0: only the node tiles this substep's particles reach, plus a
+                               * reset of tiles they left (default for one scene of 2^23 nodes
+                               * or more, else 256) */
     float p2g_ms, g2p_ms, grid_ms;  /* stage times of the chosen shapes (mpm_autotune) */
     int32_t p2g_cell_cap;     /* 4 .. 64: particles of a cell one lane sums before the
                                * rest goes, in chunks, to all warps; 0 (default): chosen

@@ -68,9 +68,31 @@ def test_tiles_left_behind_are_reset(gpu_ok, mpm):
     assert_state_close(s_t, s_e, mid)
 
 
-def test_tile_mode_needs_one_scene(gpu_ok, mpm):
+def test_batch_one_substep_tiles(gpu_ok, mpm, oracle64):
+    """Touched tiles in a batch: every scene (one of them empty) after one
+    substep against the FP64 oracle on that scene alone."""
     from mpm_b200 import scenes
-    cfgs = [scenes.small_scene(500, (16, 16, 16), seed=s, obstacle=False)[0] for s in (1, 2)]
-    with mpm.Batch(cfgs) as b:
-        with pytest.raises(mpm.MpmError):
-            b.set_tuning(grid_block=0)
+    sc = [scenes.small_scene(3000, (32, 32, 32), seed=41),
+          scenes.small_scene(5000, (48, 24, 40), seed=42),
+          scenes.small_scene(10, (16, 16, 16), seed=43, obstacle=False)]
+    cfg, st, tris = scenes.small_scene(100, (20, 20, 20), seed=45, obstacle=False)
+    sc.append((cfg, st[:, :0], tris))
+    with mpm.Batch([c for c, _, _ in sc]) as b:
+        b.init_all([s for _, s, _ in sc])
+        for k, (_, _, t) in enumerate(sc):
+            if len(t):
+                b.init_scene_sdf(k, t)
+        b.set_tuning(grid_block=0)
+        sdfs = [b.scene_sdf(k) for k in range(len(sc))]
+        b.step(1)
+        got = [b.scene_buffer(k) for k in range(len(sc))]
+        grids = [b.scene_grid(k) for k in range(len(sc))]
+    for k, (c, st, _) in enumerate(sc):
+        if st.shape[1] == 0:
+            assert not grids[k].any()
+            continue
+        st0 = oracle64.init_particles(c, st)
+        want, wgrid, _, _ = oracle64.substep(c, st0, sdfs[k].astype(np.float64))
+        assert_state_close(got[k], want, st0)
+        assert_normwise(f"scene {k} grid mass", grids[k][0], wgrid[0])
+        assert_normwise(f"scene {k} grid velocity", grids[k][1:4], wgrid[1:4])

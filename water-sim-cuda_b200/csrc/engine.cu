@@ -358,10 +358,8 @@ mpm_status upload_table(mpm_engine* e) {
 }
 
 // The tile marks when the grid update works on touched tiles only
-// (grid_block 0, one scene), else none: every node is updated.
-mpm::TileMarks active_tiles(const mpm_engine* e) {
-    return (e->scenes == 1 && e->tune.grid_block == 0) ? e->tiles : mpm::TileMarks{};
-}
+// (grid_block 0), else none: every node is updated.
+mpm::TileMarks active_tiles(const mpm_engine* e) { return e->tune.grid_block == 0 ? e->tiles : mpm::TileMarks{}; }
 
 // Enqueues stages `from`..`upto` (MPM_STAGE_*) of one substep from parity
 // `par`, for all scenes.  With `marks` (only while capturing a graph), records
@@ -742,6 +740,7 @@ mpm_status create_engine(const mpm_config* cfgs, int32_t count, int32_t device, 
     e->tiles.stamp = static_cast<uint32_t*>(e->tiles_mem);
     e->tiles.mark = e->tiles.stamp + 1;
     e->tiles.dirty = reinterpret_cast<uint8_t*>(e->tiles.mark + e->bins_total);
+    e->tiles.count = e->bins_total;
     keep_accum_in_l2(e, device);
     e->table.prm = e->d_prm;
     e->table.poff = e->d_poff;
@@ -1828,8 +1827,6 @@ extern "C" mpm_status mpm_set_tuning(mpm_engine* e, const mpm_tuning* t) {
     mpm_status s = enter(e);
     if (s != MPM_OK) return s;
     if (!t || !valid_tuning(*t)) return record(e, MPM_ERR_INVALID_ARGUMENT, "tuning out of range");
-    if (t->grid_block == 0 && e->scenes != 1)
-        return record(e, MPM_ERR_INVALID_ARGUMENT, "grid_block 0 (touched tiles) needs an engine of one scene");
     e->tune.p2g_ctas_per_sm = t->p2g_ctas_per_sm;
     e->tune.g2p_block = t->g2p_block;
     e->tune.grid_block = t->grid_block;
@@ -1889,7 +1886,6 @@ extern "C" mpm_status mpm_autotune(mpm_engine* e, int32_t repeats, mpm_tuning* o
     tbest = 1e30f;
     for (int k : {128, 256, 0}) {
         if (s != MPM_OK) break;
-        if (k == 0 && e->scenes != 1) break;
         e->tune.grid_block = k;
         if ((s = median_time(MPM_STAGE_GRID, &ms)) != MPM_OK) break;
         if (ms < tbest) tbest = ms, best.grid_block = k, best.grid_ms = ms;

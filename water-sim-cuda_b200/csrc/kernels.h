@@ -74,6 +74,7 @@ struct TileMarks {
     uint32_t* stamp;
     uint32_t* mark;
     uint8_t* dirty;
+    long long count;  // global bin entries (nb + 2 per scene)
 };
 
 // Files the n particles of P (all scenes, slot order) into an empty set.
@@ -108,9 +109,9 @@ int launch_p2g(const SceneTable& sc, long long n, long long bins_total, const fl
 // Most P2G CTAs that fit on one SM.
 int p2g_max_ctas_per_sm();
 // p0: the parameters of scene 0, used directly when the table holds one scene.
-// With tiles.mark set (one scene only): only the tiles marked by this
-// substep's ordering are updated, and tiles updated before but not marked now
-// are reset to zero; else every node.
+// With tiles.mark set: only the tiles marked by this substep's ordering are
+// updated, and tiles updated before but not marked now are reset to zero;
+// else every node.
 int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_total, float4* accum, float4* vgrid,
                        const float* sdf, const TileMarks& tiles, cudaStream_t st, int block = 256);
 // Large-step G2P (one scene): particles advect with v_old + blend (v_new -

@@ -906,20 +906,39 @@ __global__ void __launch_bounds__(256) grid_update_kernel(SceneTable sc, SimPara
     if (a.x != 0.f || a.y != 0.f || a.z != 0.f || a.w != 0.f) accum[gi] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-// One scene, one warp per node tile (TileMarks): lane l takes the nodes
+// One warp per node tile (TileMarks; global bin entries, the scene found by
+// binary search over the scenes' first entries): lane l takes the nodes
 // (x0 + l % 8, y0 + l / 8, z0 + c), c = 0..3.  A tile marked by this
 // substep's ordering is updated like grid_update_kernel; a tile updated
 // before but not marked now holds no accumulated mass any more and is reset to
 // zero; every other tile is already zero and is skipped.  Every node the
 // substep's particles reach lies in a marked tile, and G2P reads no other.
-__global__ void __launch_bounds__(256) grid_tiles_kernel(SimParams p, TileMarks tiles, float4* __restrict__ accum,
-                                                         float4* __restrict__ vgrid, const float* __restrict__ sdf) {
+template <bool kBatch>
+__global__ void __launch_bounds__(256) grid_tiles_kernel(SceneTable sc, SimParams p0, TileMarks tiles,
+                                                         float4* __restrict__ accum_all, float4* __restrict__ vgrid_all,
+                                                         const float* __restrict__ sdf_all) {
     pdl_wait();
-    const int t = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const long long gt = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (t >= p.nb) return;  // warp-uniform
-    const bool act = tiles.mark[p.boff + t] == *tiles.stamp;
-    const bool dirty = tiles.dirty[p.boff + t] != 0;
+    if (gt >= tiles.count) return;  // warp-uniform
+    int scene = 0;
+    if constexpr (kBatch) {
+        int lo = 0, hi = sc.count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&sc.prm[mid].boff) <= gt) lo = mid;
+            else hi = mid - 1;
+        }
+        scene = lo;
+    }
+    const SimParams& p = kBatch ? sc.prm[scene] : p0;
+    const int t = (int)(gt - p.boff);
+    if (t >= p.nb) return;  // the overflow bin's entries hold no tile
+    float4* accum = accum_all + p.goff;
+    float4* vgrid = vgrid_all + p.goff;
+    const float* sdf = sdf_all + p.goff;
+    const bool act = tiles.mark[gt] == *tiles.stamp;
+    const bool dirty = tiles.dirty[gt] != 0;
     if (!act && !dirty) return;
     __syncwarp();  // every lane has read the flag lane 0 rewrites below
     const int x = (t % p.nbx) * kBinX - 2 + (lane & 7);
@@ -951,7 +970,7 @@ __global__ void __launch_bounds__(256) grid_tiles_kernel(SimParams p, TileMarks 
                 vgrid[node_index(p, x, y, z0 + c)] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncwarp();
-    if (lane == 0 && act != dirty) tiles.dirty[p.boff + t] = act ? 1 : 0;
+    if (lane == 0 && act != dirty) tiles.dirty[gt] = act ? 1 : 0;
 }
 
 // ------------------------------------------------------------------ G2P ----
@@ -1519,8 +1538,13 @@ int launch_grid_update(const SceneTable& sc, const SimParams& p0, long long g_to
                        const float* sdf, const TileMarks& tiles, cudaStream_t st, int block) {
     if (g_total <= 0) return 0;
     const int b = (block == 128 || block == 256) ? block : 256;
-    if (sc.count == 1 && tiles.mark) {
-        launch_dep(grid_tiles_kernel, blocks_for(p0.nb, 8), 256, 0, st, p0, tiles, accum, vgrid, sdf);
+    if (tiles.mark) {
+        if (sc.count == 1)
+            launch_dep(grid_tiles_kernel<false>, blocks_for(tiles.count, 8), 256, 0, st, sc, p0, tiles, accum, vgrid,
+                       sdf);
+        else
+            launch_dep(grid_tiles_kernel<true>, blocks_for(tiles.count, 8), 256, 0, st, sc, p0, tiles, accum, vgrid,
+                       sdf);
         return 1;
     }
     if (sc.count == 1)
