@@ -1,7 +1,9 @@
 """Per-particle parity at the benchmark scenes' full sizes.
 
-One substep of the sphere drop (113k particles, 64^3) and of the 2M dam break
-(1,989,120 particles, 128^3, torus obstacle) runs in the engine and in the
+One substep of the sphere drop (113k particles, 64^3), of the 2M dam break
+(1,989,120 particles, 128^3, torus obstacle) and of the 256^3 scene (6,856,623
+particles, three obstacles; its grid update runs over touched tiles only, the
+default at this size) runs in the engine and in the
 reference's own engine (engine.cu/kernels.cu compiled from its sources into
 oracle/_ref) from the same state, and the FP64 oracle restates the same
 substep: keys and sort permutation bit-exact between the two engines; state
@@ -48,6 +50,8 @@ def _scene(workload):
     from mpm_b200 import scenes
     if workload == "sphere_drop":
         return scenes.sphere_drop(1234)
+    if workload == "scale_256":
+        return scenes.scale_scene(1236)
     return scenes.dam_break(1235)
 
 
@@ -160,7 +164,7 @@ def _check_reference_bounded(cfg, start, got, grid, r_state, r_grid, want, wgrid
 
 
 @needs_ref
-@pytest.mark.parametrize("workload", ["sphere_drop", "dam_break_2M"])
+@pytest.mark.parametrize("workload", ["sphere_drop", "dam_break_2M", "scale_256"])
 def test_full_scene_substep_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_path, workload):
     cfg, st, tris = _scene(workload)
     ref.create(cfg, st, tris, str(tmp_path / "config.txt"))
@@ -180,7 +184,14 @@ def test_full_scene_substep_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_path, w
     assert np.abs(sdf.astype(np.float64) - r_sdf).max() <= 1e-4, "SDF differs from the reference's makeSDF"
     want, wgrid, okeys, operm = oracle64.substep(cfg, r_start.astype(np.float64), r_sdf.astype(np.float64))
     assert np.array_equal(okeys, r_keys) and np.array_equal(operm, r_perm)
-    _check(cfg, r_start, state, grid, r_state, r_grid, want, wgrid)
+    if workload == "scale_256":
+        # Positions up to 250 cells carry float spacings of 1.5e-5, and the
+        # affine terms round on that scale, while the velocities after one
+        # substep from rest are only gravity times DT (0.03): the reference's
+        # own FP32 result misses 1e-5 of that scale (4.9e-7), so it sets the bar.
+        _check_reference_bounded(cfg, r_start, state, grid, r_state, r_grid, want, wgrid)
+    else:
+        _check(cfg, r_start, state, grid, r_state, r_grid, want, wgrid)
 
 
 @needs_ref
