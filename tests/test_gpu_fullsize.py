@@ -15,6 +15,9 @@ loaded into the reference engine as it is (no initFMatrices); there the FP32
 results are ill-conditioned and the engine is held to the reference's own
 distance from FP64.
 
+The 64-scene batch (5,895,642 particles) takes one substep in one batched
+engine, and each scene is checked against the FP64 oracle run on it alone.
+
 Reference: Engine::step (engine.cu:54-70), p2GTransferScatter
 (kernels.cu:6-142), gridUpdate (kernels.cu:144-196), g2PTransfer
 (kernels.cu:199-280), setKeys + thrust::sort_by_key (kernels.cu:361-371,
@@ -243,3 +246,53 @@ def test_dam_break_crowded_state_vs_reference(gpu_ok, mpm, oracle64, ref, tmp_pa
     # of the rescue are ill-conditioned in FP32: the reference's own result
     # sets the bar.
     _check_reference_bounded(cfg, late, state, grid, r_state, r_grid, want, wgrid)
+
+
+@needs_ref
+def test_batched_64_substep_vs_oracle(gpu_ok, mpm, oracle64, oracle32, ref, tmp_path):
+    """The 64-scene batch (5.9M particles, grids 32-96 per axis, 0-2 obstacles
+    each) after one substep in one batched engine: every scene against the FP64
+    oracle run on that scene alone.  Particles pushed out of an obstacle (the
+    ill-conditioned normal of calculateNormal, common.cuh:169-182) are held to
+    an FP32 result's own distance from FP64: the reference engine's on the
+    scenes it can run (node count a multiple of 256: its grid kernels have no
+    bounds check, kernels.cu:146-150, 311-318), else the FP32 oracle's."""
+    from mpm_b200 import scenes
+    sc = scenes.batched_scenes(64, 1237)
+    with mpm.Batch([c for c, _, _ in sc]) as b:
+        b.init_all([s for _, s, _ in sc])
+        for k, (_, _, t) in enumerate(sc):
+            if len(t):
+                b.init_scene_sdf(k, t)
+        starts = [b.scene_buffer(k) for k in range(len(sc))]
+        sdfs = [b.scene_sdf(k) for k in range(len(sc))]
+        b.step(1)
+        got = [b.scene_buffer(k) for k in range(len(sc))]
+        grids = [b.scene_grid(k) for k in range(len(sc))]
+    by = {"reference": 0, "FP32 oracle": 0}
+    for k, (cfg, st, tris) in enumerate(sc):
+        start = starts[k]
+        want, wgrid, _, _ = oracle64.substep(cfg, start.astype(np.float64), sdfs[k].astype(np.float64))
+        pushed = _pushed(cfg, start, want)
+        keep = ~pushed
+        assert_state_close(got[k][:, keep], want[:, keep], start[:, keep])
+        assert_normwise(f"scene {k} grid mass", grids[k][0], wgrid[0])
+        assert_normwise(f"scene {k} grid velocity", grids[k][1:4], wgrid[1:4])
+        if not pushed.any():
+            continue
+        if cfg.grid_number % 256 == 0:
+            ref.create(cfg, st, tris, str(tmp_path / f"config{k}.txt"))
+            assert np.array_equal(ref.state(), start), f"scene {k}: initial state differs from the reference"
+            ref.step(1)
+            other, source = ref.state(), "reference"
+        else:
+            other, source = oracle32.substep(cfg, start, sdfs[k])[0], "FP32 oracle"
+        by[source] += int(pushed.sum())
+        e_got = _field_errors(got[k][:, pushed], want[:, pushed])
+        e_other = _field_errors(np.asarray(other)[:, pushed], want[:, pushed])
+        for name in e_got:
+            sl = {"position": slice(0, 3), "velocity": slice(3, 6), "C": slice(6, 15), "F": slice(15, 24)}[name]
+            scale = float(np.max(np.abs(want[sl, pushed])))
+            assert e_got[name] <= max(2.0 * e_other[name], 1e-5 * scale), \
+                f"scene {k} {name} of pushed particles: engine {e_got[name]:.3e}, {source} {e_other[name]:.3e}"
+    print(f"batched_64: {sum(s.shape[1] for _, s, _ in sc)} particles; pushed particles bounded by {by}")
