@@ -147,7 +147,9 @@ struct SceneLookup {
 // take work items from a counter; a listed bin (8 x 4 x 4 base cells) has
 // kBinZ items, and item g takes positions 32 g .. 32 g + 31 of the bin's cell
 // order (cell_order: occupied cells by count class, largest first), so the
-// lanes of a warp hold cells of similar counts and no empty ones.  Lane =
+// lanes of a warp hold cells of similar counts and no empty ones.  The
+// counter hands out every bin's item 0 before any item 1, and so on, so the
+// longest items start first.  Lane =
 // cell: all particles of a cell scatter to the same 27 nodes, so the lane sums
 // them in registers, reading them through a ring of kRing particles fetched
 // ahead with 16-byte cp.async copies (the gather through gidx costs no
@@ -321,11 +323,14 @@ __global__ void __launch_bounds__(32, kP2GWarpsPerSM) p2g_kernel(SceneTable sc, 
         if (lane == 0) item = (int)atomicAdd(work, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= nitems) return;
-        // Items: kBinZ per listed bin, scene after scene.
+        // Items: kBinZ per listed bin, scene after scene, group-major within a scene.
         const int scene = sc.count == 1 ? 0 : scene_of(itemoff, sc.count, item);
         const SimParams p = sc.prm[scene];
+        // Group-major: every listed bin's group 0 (its most crowded cells) comes
+        // before any group 1, and so on, so that the long items start first.
         const int local = item - (int)__ldg(itemoff + scene);
-        const int bin = __ldg(set.blist + p.boff + local / kBinZ), group = local % kBinZ;
+        const int nl = (int)((__ldg(itemoff + scene + 1) - __ldg(itemoff + scene)) / kBinZ);
+        const int bin = __ldg(set.blist + p.boff + local % nl), group = local / nl;
         if (bin >= p.nb) continue;  // the overflow bin reaches no node
         float4* accum = accum_all + p.goff;
         const int bxi = bin % p.nbx, byi = (bin / p.nbx) % p.nby, bzi = bin / (p.nbx * p.nby);
