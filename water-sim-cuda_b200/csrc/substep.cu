@@ -1075,7 +1075,13 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
         q1 = valid ? r[blockDim.x] : make_float4(0.f, 0.f, 0.f, 0.f);
         q2 = valid ? r[2 * blockDim.x] : make_float4(0.f, 0.f, 0.f, 0.f);
     } else {
-        q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+        // Records are 96 bytes from a cudaMalloc'd base, so each starts on a
+        // 32-byte boundary: one 32-byte load (sm_100 ld.global.v8) for the
+        // position and F00..F04, one 16-byte load for F05..F08.
+        asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=f"(q0.x), "=f"(q0.y), "=f"(q0.z), "=f"(q0.w), "=f"(q1.x), "=f"(q1.y), "=f"(q1.z), "=f"(q1.w)
+            : "l"(q));
+        q2 = __ldg(q + 2);
     }
     float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);
     if constexpr (kMode != kG2PPlain) qv = __ldg(q + 3);  // old velocity
@@ -1318,12 +1324,18 @@ __global__ void __launch_bounds__(256, kWide ? 1 : (kMode == 1 ? 2 : ((kBatch ||
     file_particle(gcell, gbin, bin, scene, p.boff, next);
     if (!valid) continue;  // only the last passes of the last block have idle lanes
     float4* o = reinterpret_cast<float4*>(Pout + (size_t)j * kAFloats);
-    o[0] = make_float4(nx, ny, nz, NF[0]);
-    o[1] = make_float4(NF[1], NF[2], NF[3], NF[4]);
-    o[2] = make_float4(NF[5], NF[6], NF[7], NF[8]);
-    o[3] = make_float4(tv[0], tv[1], tv[2], tc[0]);
-    o[4] = make_float4(tc[1], tc[2], tc[3], tc[4]);
-    o[5] = make_float4(tc[5], tc[6], tc[7], tc[8]);
+    {
+        // Three 32-byte stores (st.global.v8) of the 96-byte record: half the
+        // store instructions of 16-byte vectors.
+        const float w[24] = {nx, ny, nz, NF[0], NF[1], NF[2], NF[3], NF[4], NF[5], NF[6], NF[7], NF[8],
+                             tv[0], tv[1], tv[2], tc[0], tc[1], tc[2], tc[3], tc[4], tc[5], tc[6], tc[7], tc[8]};
+#pragma unroll
+        for (int h = 0; h < 3; ++h)
+            asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(o + 2 * h),
+                         "f"(w[8 * h + 0]), "f"(w[8 * h + 1]), "f"(w[8 * h + 2]), "f"(w[8 * h + 3]),
+                         "f"(w[8 * h + 4]), "f"(w[8 * h + 5]), "f"(w[8 * h + 6]), "f"(w[8 * h + 7])
+                         : "memory");
+    }
     sig_out[j] = __ldg(sig_in + src);
     pcell[j] = gcell;
     if constexpr (kMode == kG2PCollect) {
